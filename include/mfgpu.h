@@ -1,0 +1,144 @@
+/*
+ * mfgpu.h — C ABI of the B200 multifrontal factor / localized-update / solve
+ * path for box/separator-ordered 2D 5-point and 3D 7-point variable-coefficient
+ * Laplacians.
+ *
+ * Every entry point takes plain pointers and sizes.  Each one replaces a public
+ * member of the reference's TreeFactor2D::MF2D<double> / TreeFactor3D::MF3D<double>
+ * (victorminden/updating-multifrontal, include/DE/mf.hpp); the citation is
+ * given beside each declaration.  Errors are reported as status codes; the
+ * C++ drop-in headers turn them back into the reference's exceptions.
+ *
+ * A handle owns its device memory (CSR matrix, symbolic tables, factor,
+ * update matrices) and one CUDA stream; the factorization stays resident on
+ * the GPU between calls.  One handle must be used by one host thread at a
+ * time.  There is no CPU fallback: without a usable CUDA device every
+ * compute call fails with MFGPU_ERR_CUDA.
+ */
+#ifndef MFGPU_H
+#define MFGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mfgpu_handle mfgpu_handle;
+typedef struct mfgpu_symbolic mfgpu_symbolic;
+
+enum mfgpu_status {
+  MFGPU_OK = 0,
+  MFGPU_ERR_ARG = 1,        /* bad argument (sizes, null pointers, pattern)  */
+  MFGPU_ERR_DEPTH = 2,      /* tree depth <= 1 (reference: runtime_error)    */
+  MFGPU_ERR_LEAF = 3,       /* leaf-width arithmetic failed (runtime_error)  */
+  MFGPU_ERR_OOM = 4,        /* device allocation failed                      */
+  MFGPU_ERR_CUDA = 5,       /* CUDA runtime error or no device               */
+  MFGPU_ERR_PIVOT = 6,      /* non-positive pivot: matrix not SPD            */
+  MFGPU_ERR_TIMEOUT = 7,    /* a bounded device wait gave up                 */
+  MFGPU_ERR_STATE = 8,      /* call out of order (e.g. solve before factor)  */
+  MFGPU_ERR_NOT_CONVERGED = 9 /* mixed precision: refinement did not reach tol */
+};
+
+enum mfgpu_precision {
+  MFGPU_FP64 = 0,   /* drop-in path: FP64 factor and solve                    */
+  MFGPU_MIXED = 1   /* FP32/tensor-core factor, FP64 residual + refinement    */
+};
+
+typedef struct mfgpu_options {
+  int precision;        /* mfgpu_precision, default MFGPU_FP64                  */
+  int device;           /* CUDA device ordinal, default 0                       */
+  double refine_tol;    /* mixed: target ||b-Ax||/||b||, default 1e-10          */
+  int refine_maxit;     /* mixed: refinement iteration cap, default 50          */
+  int reserved[7];
+} mfgpu_options;
+
+typedef struct mfgpu_info {
+  int dim, levels, n_fronts, n_seps;
+  int64_t ndof, nnz;
+  int leaf_box[3];              /* leaf box widths (boxWidth{X,Y,Z}Bottom_)   */
+  int max_front;                /* largest n + m                              */
+  double factor_flops;          /* sum over fronts of n^3/3 + n^2 m + n m^2   */
+  int64_t front_bytes, sep_bytes, device_bytes;
+} mfgpu_info;
+
+typedef struct mfgpu_stats {
+  double seconds;         /* device time of the last factor/update/solve call */
+  double flops;           /* algorithmic flops of that call (Cholesky form)   */
+  int fronts;             /* fronts (boxes) refactored by the last factor/update */
+  int iterations;         /* refinement iterations of the last mixed solve    */
+  double residual;        /* last mixed solve: max_j ||b_j - A x_j|| / ||b_j|| */
+} mfgpu_stats;
+
+void mfgpu_default_options(mfgpu_options* opts);
+const char* mfgpu_status_string(int status);
+
+/* MF2D(const Sparse&, Nx, Ny, width, maxSideLength) — include/DE/mf.hpp:74;
+ * MF3D(const Sparse&, Nx, Ny, Nz, width, maxSideLength) — include/DE/mf.hpp:180.
+ * dim = 2 ignores nz.  The CSR (row_ptr[n+1], col_ind[nnz], val[nnz]) is copied.
+ * Only width = 1 (5-/7-point stencils) is supported on the GPU path. */
+int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side_length, int n,
+                 const int* row_ptr, const int* col_ind, const double* val,
+                 const mfgpu_options* opts, mfgpu_handle** out);
+
+/* void Factor() — include/DE/mf.hpp:84, src/DE/mf2d.cpp:449-500. */
+int mfgpu_factor(mfgpu_handle* h);
+
+/* void Update(const Sparse& A, std::set<int> modifiedDOFs) — include/DE/mf.hpp:86,
+ * src/DE/mf2d.cpp:150-181.  `val` holds the new values on the unchanged pattern
+ * (nnz entries); only fronts on root paths of leaves holding modified DOFs are
+ * refactored. */
+int mfgpu_update(mfgpu_handle* h, const double* val, int64_t nnz, const int* modified_dofs,
+                 int n_modified);
+
+/* Vec Solve(const Vec& b) — include/DE/mf.hpp:81, src/DE/mf2d.cpp:976-1054.
+ * Host buffers: b and x are n x nrhs column-major with leading dimension ld. */
+int mfgpu_solve(mfgpu_handle* h, const double* b, double* x, int nrhs, int64_t ld);
+
+/* Vec Apply(const Vec& x) — include/DE/mf.hpp:78, src/DE/mf2d.cpp:904-974. */
+int mfgpu_apply(mfgpu_handle* h, const double* x, double* b, int nrhs, int64_t ld);
+
+/* Device-pointer forms of Solve / Apply (no reference counterpart: the
+ * reference is host-only); b/x live in device memory. */
+int mfgpu_solve_device(mfgpu_handle* h, const double* d_b, double* d_x, int nrhs, int64_t ld);
+int mfgpu_apply_device(mfgpu_handle* h, const double* d_x, double* d_b, int nrhs, int64_t ld);
+
+/* Use an external CUDA stream (cudaStream_t) for all later work; NULL restores
+ * the handle's own stream. */
+int mfgpu_set_stream(mfgpu_handle* h, void* cuda_stream);
+int mfgpu_get_info(const mfgpu_handle* h, mfgpu_info* info);
+int mfgpu_last_stats(const mfgpu_handle* h, mfgpu_stats* stats);
+const char* mfgpu_last_error(const mfgpu_handle* h);
+void mfgpu_destroy(mfgpu_handle* h);
+
+/* Host-only symbolic schedule (no device needed): the reference's per-level
+ * DOF lists (Box::intDOFs / bdDOFs and Edge/Face::DOFs, include/DE/mf.hpp:45-62)
+ * and the assembly tasks that implement ScatterReplace_/ScatterAdd_/
+ * AddNew*Interactions_ (src/DE/mf2d.cpp:755-901). */
+int mfgpu_symbolic_create(int dim, int nx, int ny, int nz, int width, int max_side_length,
+                          mfgpu_symbolic** out);
+void mfgpu_symbolic_destroy(mfgpu_symbolic* s);
+const char* mfgpu_symbolic_error(void);
+/* levels, n_fronts, n_seps, ndof */
+int mfgpu_symbolic_sizes(const mfgpu_symbolic* s, int* levels, int* n_fronts, int* n_seps,
+                         int64_t* ndof);
+/* front f (global id, root first, level by level): level, box, n, m, pointer to
+ * its n+m DOFs (pivots then boundary) valid until destroy. */
+int mfgpu_symbolic_front(const mfgpu_symbolic* s, int f, int* level, int* box, int* n, int* m,
+                         const int** dofs);
+/* separator k (global id, level 1 first): level, index in level, size, DOFs,
+ * and the two adjacent fronts with the separator's row inside each. */
+int mfgpu_symbolic_sep(const mfgpu_symbolic* s, int k, int* level, int* idx, int* size,
+                       const int** dofs, int boxes[2], int rows[2]);
+/* Assembly tasks.  which = 0: front tasks, 1: separator base tasks, 2:
+ * separator accumulation tasks.  Returns the count; `tasks` points at an
+ * array of 56-byte records laid out as in the C++ struct mfgpu::Task. */
+int64_t mfgpu_symbolic_tasks(const mfgpu_symbolic* s, int which, const void** tasks);
+/* Arena layout of front f / separator k: element offset and leading dimension. */
+int mfgpu_symbolic_layout(const mfgpu_symbolic* s, int front_or_sep, int id, int64_t* off,
+                          int* ld);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MFGPU_H */

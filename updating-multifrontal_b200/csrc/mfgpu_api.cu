@@ -1,0 +1,724 @@
+// C ABI (include/mfgpu.h): handle lifetime, level-by-level orchestration of the
+// factor / localized update / solve / apply on one CUDA stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/mfgpu.h"
+#include "device.cuh"
+#include "schedule.hpp"
+
+using mfgpu::DevError;
+using mfgpu::FrontDev;
+using mfgpu::Schedule;
+using mfgpu::SepDev;
+using mfgpu::Task;
+
+namespace {
+
+struct CudaError : std::runtime_error {
+  int status;
+  CudaError(const std::string& m, int s) : std::runtime_error(m), status(s) {}
+};
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    int st = (e == cudaErrorMemoryAllocation) ? MFGPU_ERR_OOM : MFGPU_ERR_CUDA;
+    throw CudaError(std::string(what) + ": " + cudaGetErrorString(e), st);
+  }
+}
+
+template <class T>
+T* dalloc(size_t count, const char* what) {
+  void* p = nullptr;
+  if (count == 0) count = 1;
+  ck(cudaMalloc(&p, count * sizeof(T)), what);
+  return static_cast<T*>(p);
+}
+
+int64_t tilesOf(const Task& t) {
+  const int64_t a = (t.rows + mfgpu::kTaskTile - 1) / mfgpu::kTaskTile;
+  const int64_t b = (t.cols + mfgpu::kTaskTile - 1) / mfgpu::kTaskTile;
+  return a * b;
+}
+
+// A group of tasks executed by one launch.
+struct Group {
+  int64_t task0 = 0, ntasks = 0, pref0 = 0, ntiles = 0;
+};
+
+// Everything one factorization pass needs: per level the fronts and separators
+// to (re)compute and their task groups, all in one device buffer.
+struct Plan {
+  struct Level {
+    int64_t f0 = 0, nf = 0, s0 = 0, ns = 0;  // offsets into the id list
+    int maxN = 0, maxn = 0;
+    Group ftask, sbase, sadd0, sadd1;
+  };
+  std::vector<Level> lv;
+  std::vector<Task> tasks;
+  std::vector<int64_t> pref;
+  std::vector<int> ids;
+  int nfronts = 0;
+  double flops = 0;
+  // device copies
+  Task* d_tasks = nullptr;
+  int64_t* d_pref = nullptr;
+  int* d_ids = nullptr;
+  size_t cap_tasks = 0, cap_pref = 0, cap_ids = 0;
+
+  void release() {
+    cudaFree(d_tasks);
+    cudaFree(d_pref);
+    cudaFree(d_ids);
+    d_tasks = nullptr;
+    d_pref = nullptr;
+    d_ids = nullptr;
+    cap_tasks = cap_pref = cap_ids = 0;
+  }
+
+  Group addGroup(const std::vector<Task>& src, const std::vector<int64_t>& ptr,
+                 const std::vector<int>& owners, int pick /* -1 all, 0/1 add task k */) {
+    Group g;
+    g.task0 = (int64_t)tasks.size();
+    g.pref0 = (int64_t)pref.size();
+    int64_t acc = 0;
+    pref.push_back(0);
+    for (int o : owners) {
+      int64_t a, b;
+      if (pick < 0) {
+        a = ptr[o];
+        b = ptr[o + 1];
+      } else {
+        a = 2 * (int64_t)o + pick;
+        b = a + 1;
+      }
+      for (int64_t t = a; t < b; t++) {
+        tasks.push_back(src[t]);
+        acc += tilesOf(src[t]);
+        pref.push_back(acc);
+      }
+    }
+    g.ntasks = (int64_t)tasks.size() - g.task0;
+    g.ntiles = acc;
+    if (g.ntasks == 0) pref.pop_back();
+    return g;
+  }
+
+  void upload(cudaStream_t st) {
+    auto grow = [](auto*& p, size_t& cap, size_t need, const char* what) {
+      if (need <= cap) return;
+      cudaFree(p);
+      p = nullptr;
+      using T = std::remove_reference_t<decltype(*p)>;
+      size_t c = std::max(need, cap * 2);
+      p = dalloc<T>(c, what);
+      cap = c;
+    };
+    grow(d_tasks, cap_tasks, tasks.size(), "alloc plan tasks");
+    grow(d_pref, cap_pref, pref.size(), "alloc plan prefixes");
+    grow(d_ids, cap_ids, ids.size(), "alloc plan ids");
+    if (!tasks.empty())
+      ck(cudaMemcpyAsync(d_tasks, tasks.data(), tasks.size() * sizeof(Task), cudaMemcpyHostToDevice, st),
+         "upload tasks");
+    if (!pref.empty())
+      ck(cudaMemcpyAsync(d_pref, pref.data(), pref.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st),
+         "upload prefixes");
+    if (!ids.empty())
+      ck(cudaMemcpyAsync(d_ids, ids.data(), ids.size() * sizeof(int), cudaMemcpyHostToDevice, st),
+         "upload ids");
+    // host vectors must outlive the async copies
+    ck(cudaStreamSynchronize(st), "plan upload");
+  }
+};
+
+}  // namespace
+
+struct mfgpu_handle {
+  std::unique_ptr<Schedule> S;
+  mfgpu_options opt{};
+  int device = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  std::string err;
+  mfgpu_stats stats{};
+  bool factored = false;
+  int n = 0;
+  int64_t nnz = 0;
+  std::vector<int> h_rowptr, h_colind;
+
+  double* d_F = nullptr;
+  double* d_Sep = nullptr;
+  double* d_val = nullptr;
+  int* d_rp = nullptr;
+  int* d_ci = nullptr;
+  int* d_dofs = nullptr;
+  FrontDev* d_fr = nullptr;
+  SepDev* d_sp = nullptr;
+  int64_t* d_woff = nullptr;
+  DevError* d_err = nullptr;
+  double* d_W = nullptr;
+  size_t capW = 0;
+  double* d_X = nullptr;
+  double* d_T = nullptr;
+  size_t capX = 0;
+  int* d_all = nullptr;      // every front id then every separator id, level order
+  int64_t woffTotal = 0;     // sum over fronts of 2N
+  Plan full, upd;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int64_t device_bytes = 0;
+
+  ~mfgpu_handle() {
+    if (stream) cudaStreamSynchronize(stream);
+    full.release();
+    upd.release();
+    cudaFree(d_F);
+    cudaFree(d_Sep);
+    cudaFree(d_val);
+    cudaFree(d_rp);
+    cudaFree(d_ci);
+    cudaFree(d_dofs);
+    cudaFree(d_fr);
+    cudaFree(d_sp);
+    cudaFree(d_woff);
+    cudaFree(d_err);
+    cudaFree(d_W);
+    cudaFree(d_X);
+    cudaFree(d_T);
+    cudaFree(d_all);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (own) cudaStreamDestroy(own);
+  }
+
+  // Build a plan for the given dirty fronts (global ids); separators adjacent
+  // to a dirty front at their level are recomputed.
+  void buildPlan(Plan& P, const std::vector<char>& dirtyFront) {
+    const Schedule& s = *S;
+    P.lv.assign(s.levels, Plan::Level());
+    P.tasks.clear();
+    P.pref.clear();
+    P.ids.clear();
+    P.nfronts = 0;
+    P.flops = 0;
+    for (int ell = s.levels - 1; ell >= 0; ell--) {
+      Plan::Level& L = P.lv[ell];
+      std::vector<int> fl, sl;
+      for (int b = 0; b < s.lv[ell].nbox; b++) {
+        int f = s.lv[ell].front0 + b;
+        if (dirtyFront[f]) fl.push_back(f);
+      }
+      for (int e = 0; e < s.lv[ell].nsep; e++) {
+        int k = s.lv[ell].sep0 + e;
+        const mfgpu::Sep& sp = s.seps[k];
+        if (dirtyFront[sp.box[0]] || dirtyFront[sp.box[1]]) sl.push_back(k);
+      }
+      L.f0 = (int64_t)P.ids.size();
+      L.nf = (int64_t)fl.size();
+      P.ids.insert(P.ids.end(), fl.begin(), fl.end());
+      L.s0 = (int64_t)P.ids.size();
+      L.ns = (int64_t)sl.size();
+      P.ids.insert(P.ids.end(), sl.begin(), sl.end());
+      for (int f : fl) {
+        L.maxN = std::max(L.maxN, s.fronts[f].N);
+        L.maxn = std::max(L.maxn, s.fronts[f].n);
+        P.flops += s.front_flops(s.fronts[f]);
+      }
+      P.nfronts += (int)fl.size();
+      L.ftask = P.addGroup(s.front_tasks, s.front_task_ptr, fl, -1);
+      L.sbase = P.addGroup(s.sep_tasks, s.sep_task_ptr, sl, -1);
+      L.sadd0 = P.addGroup(s.sep_add_tasks, s.sep_task_ptr, sl, 0);
+      L.sadd1 = P.addGroup(s.sep_add_tasks, s.sep_task_ptr, sl, 1);
+    }
+  }
+
+  void runGroup(const Plan& P, const Group& g) {
+    if (g.ntasks == 0 || g.ntiles == 0) return;
+    mfgpu::launch_tasks(P.d_tasks + g.task0, P.d_pref + g.pref0, (int)g.ntasks, g.ntiles, d_F, d_Sep,
+                        d_rp, d_ci, d_val, d_dofs, stream);
+  }
+
+  // Run a factorization plan: per level, separator base assembly, front
+  // assembly, partial Cholesky, separator accumulation (src/DE/mf2d.cpp:449-753).
+  void runPlan(const Plan& P) {
+    const Schedule& s = *S;
+    ck(cudaMemsetAsync(d_err, 0, sizeof(DevError), stream), "clear error word");
+    for (int ell = s.levels - 1; ell >= 0; ell--) {
+      const Plan::Level& L = P.lv[ell];
+      runGroup(P, L.sbase);
+      runGroup(P, L.ftask);
+      if (L.nf > 0) {
+        for (int k = 0; k < L.maxn; k += mfgpu::kPanel)
+          mfgpu::launch_panel_step(P.d_ids + L.f0, (int)L.nf, d_fr, d_F, k, L.maxN, d_err, stream);
+      }
+      runGroup(P, L.sadd0);
+      runGroup(P, L.sadd1);
+    }
+    ck(cudaGetLastError(), "factor launch");
+  }
+
+  void checkDevError() {
+    DevError e;
+    ck(cudaMemcpyAsync(&e, d_err, sizeof(e), cudaMemcpyDeviceToHost, stream), "read error word");
+    ck(cudaStreamSynchronize(stream), "factor");
+    if (e.code == 1) {
+      const mfgpu::Front& f = S->fronts[e.front];
+      char buf[256];
+      snprintf(buf, sizeof buf,
+               "non-positive pivot in front %d (level %d, box %d) at pivot column %d: the matrix "
+               "is not symmetric positive definite",
+               e.front, f.level, f.box, e.col);
+      throw CudaError(buf, MFGPU_ERR_PIVOT);
+    }
+  }
+
+  void ensureWork(int nrhs) {
+    size_t needW = (size_t)woffTotal * nrhs;
+    if (needW > capW) {
+      cudaFree(d_W);
+      d_W = nullptr;
+      d_W = dalloc<double>(needW, "alloc solve workspace");
+      capW = needW;
+    }
+    size_t needX = (size_t)n * nrhs;
+    if (needX > capX) {
+      cudaFree(d_X);
+      cudaFree(d_T);
+      d_X = d_T = nullptr;
+      d_X = dalloc<double>(needX, "alloc rhs buffer");
+      d_T = dalloc<double>(needX, "alloc apply buffer");
+      capX = needX;
+    }
+  }
+
+  // Solve in place on device data X (n x nrhs, ld = ldx), nrhs <= 16.
+  void solveChunk(double* X, int64_t ldx, int nrhs) {
+    const Schedule& s = *S;
+    for (int ell = s.levels - 1; ell >= 1; ell--) {
+      const int f0 = s.lv[ell].front0, s0 = s.lv[ell].sep0;
+      mfgpu::launch_solve_fwd(d_all + f0, s.lv[ell].nbox, d_fr, d_F, d_dofs, X, ldx, nrhs, d_W,
+                              d_woff, stream);
+      mfgpu::launch_sep_gather(d_all + s.fronts.size() + s0, s.lv[ell].nsep, d_sp, d_dofs, X, ldx,
+                               nrhs, d_W, d_woff, d_fr, stream);
+    }
+    mfgpu::launch_root_solve(0, d_fr, d_F, d_dofs, X, ldx, nrhs, d_W, d_woff, stream);
+    for (int ell = 1; ell < s.levels; ell++) {
+      mfgpu::launch_solve_bwd(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, d_F, d_dofs, X, ldx,
+                              nrhs, d_W, d_woff, stream);
+    }
+    ck(cudaGetLastError(), "solve launch");
+  }
+
+  void applyChunk(double* X, int64_t ldx, int nrhs) {
+    const Schedule& s = *S;
+    for (int ell = s.levels - 1; ell >= 1; ell--)
+      mfgpu::launch_apply_up(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, d_F, d_dofs, X, ldx,
+                             nrhs, d_W, d_woff, d_T, stream);
+    mfgpu::launch_root_apply(0, d_fr, d_F, d_dofs, X, ldx, nrhs, d_W, d_woff, stream);
+    for (int ell = 1; ell < s.levels; ell++) {
+      mfgpu::launch_apply_down(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, d_F, d_dofs, ldx,
+                               nrhs, d_W, d_woff, d_T, stream);
+      mfgpu::launch_sep_gather(d_all + s.fronts.size() + s.lv[ell].sep0, s.lv[ell].nsep, d_sp, d_dofs,
+                               X, ldx, nrhs, d_W, d_woff, d_fr, stream);
+    }
+    ck(cudaGetLastError(), "apply launch");
+  }
+};
+
+namespace {
+
+int fail(mfgpu_handle* h, int status, const std::string& msg) {
+  if (h) h->err = msg;
+  return status;
+}
+
+template <class F>
+int guarded(mfgpu_handle* h, F&& fn) {
+  if (!h) return MFGPU_ERR_ARG;
+  try {
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(h, MFGPU_ERR_CUDA, "cudaSetDevice failed");
+    fn();
+    h->err.clear();
+    return MFGPU_OK;
+  } catch (const CudaError& e) {
+    return fail(h, e.status, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(h, MFGPU_ERR_OOM, "host allocation failed");
+  } catch (const std::invalid_argument& e) {
+    return fail(h, MFGPU_ERR_ARG, e.what());
+  } catch (const std::exception& e) {
+    return fail(h, MFGPU_ERR_CUDA, e.what());
+  }
+}
+
+thread_local std::string g_create_error;
+thread_local std::string g_sym_error;
+
+}  // namespace
+
+extern "C" {
+
+void mfgpu_default_options(mfgpu_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->precision = MFGPU_FP64;
+  o->device = 0;
+  o->refine_tol = 1e-10;
+  o->refine_maxit = 50;
+}
+
+const char* mfgpu_status_string(int s) {
+  switch (s) {
+    case MFGPU_OK: return "ok";
+    case MFGPU_ERR_ARG: return "invalid argument";
+    case MFGPU_ERR_DEPTH: return "recursion depth is 1 level";
+    case MFGPU_ERR_LEAF: return "leaf box arithmetic failed";
+    case MFGPU_ERR_OOM: return "out of device memory";
+    case MFGPU_ERR_CUDA: return "CUDA error";
+    case MFGPU_ERR_PIVOT: return "non-positive pivot (matrix not SPD)";
+    case MFGPU_ERR_TIMEOUT: return "device wait timed out";
+    case MFGPU_ERR_STATE: return "call out of order";
+    case MFGPU_ERR_NOT_CONVERGED: return "refinement did not converge";
+  }
+  return "unknown status";
+}
+
+int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n,
+                 const int* row_ptr, const int* col_ind, const double* val,
+                 const mfgpu_options* opts, mfgpu_handle** out) {
+  if (!out) return MFGPU_ERR_ARG;
+  *out = nullptr;
+  g_create_error.clear();
+  if (!row_ptr || !col_ind || !val) {
+    g_create_error = "null CSR pointer";
+    return MFGPU_ERR_ARG;
+  }
+  if (width != 1) {
+    g_create_error = "only separator width 1 (5-/7-point stencils) is supported";
+    return MFGPU_ERR_ARG;
+  }
+  std::unique_ptr<mfgpu_handle> h(new (std::nothrow) mfgpu_handle());
+  if (!h) return MFGPU_ERR_OOM;
+  mfgpu_default_options(&h->opt);
+  if (opts) h->opt = *opts;
+  h->device = h->opt.device;
+  try {
+    h->S.reset(new Schedule(dim, nx, ny, nz, width, max_side));
+  } catch (const std::invalid_argument& e) {
+    g_create_error = e.what();
+    return MFGPU_ERR_ARG;
+  } catch (const std::runtime_error& e) {
+    g_create_error = e.what();
+    return std::string(e.what()).find("recursion depth") != std::string::npos ? MFGPU_ERR_DEPTH
+                                                                                : MFGPU_ERR_LEAF;
+  }
+  const Schedule& s = *h->S;
+  if ((int64_t)n != s.ndof || row_ptr[0] != 0) {
+    g_create_error = "matrix dimension does not match the grid";
+    return MFGPU_ERR_ARG;
+  }
+  h->n = n;
+  h->nnz = row_ptr[n];
+  h->h_rowptr.assign(row_ptr, row_ptr + n + 1);
+  h->h_colind.assign(col_ind, col_ind + h->nnz);
+  int st = guarded(h.get(), [&]() {
+    mfgpu_handle& H = *h;
+    ck(cudaStreamCreateWithFlags(&H.own, cudaStreamNonBlocking), "create stream");
+    H.stream = H.own;
+    ck(cudaEventCreate(&H.ev0), "event");
+    ck(cudaEventCreate(&H.ev1), "event");
+    H.d_F = dalloc<double>(s.front_elems, "alloc front arena");
+    H.d_Sep = dalloc<double>(s.sep_elems, "alloc separator arena");
+    H.d_val = dalloc<double>(H.nnz, "alloc CSR values");
+    H.d_rp = dalloc<int>(n + 1, "alloc CSR rows");
+    H.d_ci = dalloc<int>(H.nnz, "alloc CSR cols");
+    H.d_dofs = dalloc<int>(s.dofs.size(), "alloc DOF table");
+    std::vector<FrontDev> fr(s.fronts.size());
+    std::vector<int64_t> woff(s.fronts.size() + 1, 0);
+    for (size_t i = 0; i < s.fronts.size(); i++) {
+      const mfgpu::Front& f = s.fronts[i];
+      fr[i] = FrontDev{f.off, f.dof_off, f.n, f.m, f.N, f.ld};
+      woff[i + 1] = woff[i] + 2 * (int64_t)f.N;
+    }
+    H.woffTotal = woff.back();
+    std::vector<SepDev> sp(s.seps.size());
+    for (size_t i = 0; i < s.seps.size(); i++) {
+      const mfgpu::Sep& e = s.seps[i];
+      sp[i] = SepDev{e.dof_off, e.s, e.box[0], e.box[1], e.bdpos[0], e.bdpos[1], 0};
+    }
+    std::vector<int> all;
+    for (size_t i = 0; i < s.fronts.size(); i++) all.push_back((int)i);
+    for (size_t i = 0; i < s.seps.size(); i++) all.push_back((int)i);
+    H.d_fr = dalloc<FrontDev>(fr.size(), "alloc fronts");
+    H.d_sp = dalloc<SepDev>(std::max<size_t>(1, sp.size()), "alloc seps");
+    H.d_woff = dalloc<int64_t>(woff.size(), "alloc woff");
+    H.d_err = dalloc<DevError>(1, "alloc error word");
+    H.d_all = dalloc<int>(all.size(), "alloc id list");
+    ck(cudaMemcpy(H.d_val, val, H.nnz * sizeof(double), cudaMemcpyHostToDevice), "upload val");
+    ck(cudaMemcpy(H.d_rp, row_ptr, (n + 1) * sizeof(int), cudaMemcpyHostToDevice), "upload rows");
+    ck(cudaMemcpy(H.d_ci, col_ind, H.nnz * sizeof(int), cudaMemcpyHostToDevice), "upload cols");
+    ck(cudaMemcpy(H.d_dofs, s.dofs.data(), s.dofs.size() * sizeof(int), cudaMemcpyHostToDevice),
+       "upload dofs");
+    ck(cudaMemcpy(H.d_fr, fr.data(), fr.size() * sizeof(FrontDev), cudaMemcpyHostToDevice), "upload fronts");
+    if (!sp.empty())
+      ck(cudaMemcpy(H.d_sp, sp.data(), sp.size() * sizeof(SepDev), cudaMemcpyHostToDevice), "upload seps");
+    ck(cudaMemcpy(H.d_woff, woff.data(), woff.size() * sizeof(int64_t), cudaMemcpyHostToDevice), "upload woff");
+    ck(cudaMemcpy(H.d_all, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice), "upload ids");
+    std::vector<char> dirty(s.fronts.size(), 1);
+    H.buildPlan(H.full, dirty);
+    H.full.upload(H.stream);
+    H.device_bytes = (int64_t)(s.front_elems + s.sep_elems + H.nnz) * 8 + (H.nnz + n + 1) * 4 +
+                     (int64_t)s.dofs.size() * 4;
+  });
+  if (st != MFGPU_OK) {
+    g_create_error = h->err;
+    return st;
+  }
+  *out = h.release();
+  return MFGPU_OK;
+}
+
+int mfgpu_factor(mfgpu_handle* h) {
+  return guarded(h, [&]() {
+    ck(cudaEventRecord(h->ev0, h->stream), "event");
+    h->runPlan(h->full);
+    ck(cudaEventRecord(h->ev1, h->stream), "event");
+    h->checkDevError();
+    float ms = 0;
+    ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "elapsed");
+    h->stats.seconds = ms * 1e-3;
+    h->stats.flops = h->full.flops;
+    h->stats.fronts = h->full.nfronts;
+    h->factored = true;
+  });
+}
+
+int mfgpu_update(mfgpu_handle* h, const double* val, int64_t nnz, const int* mod, int nmod) {
+  if (!h) return MFGPU_ERR_ARG;
+  if (!h->factored) return fail(h, MFGPU_ERR_STATE, "Update() before Factor()");
+  if (!val || nnz != h->nnz || (nmod > 0 && !mod) || nmod < 0)
+    return fail(h, MFGPU_ERR_ARG, "Update(): values must match the factored pattern");
+  for (int i = 0; i < nmod; i++)
+    if (mod[i] < 0 || mod[i] >= h->n) return fail(h, MFGPU_ERR_ARG, "modified DOF out of range");
+  return guarded(h, [&]() {
+    const Schedule& s = *h->S;
+    // dirty leaves (mf2d.cpp:163-174), then their root paths
+    std::vector<char> dirty(s.fronts.size(), 0);
+    for (int i = 0; i < nmod; i++) {
+      int f = s.leaf_of_dof(mod[i]);
+      while (f >= 0 && !dirty[f]) {
+        dirty[f] = 1;
+        f = s.fronts[f].parent;
+      }
+    }
+    dirty[0] = 1;   // the root is always refactored (mf2d.cpp:633-657)
+    h->buildPlan(h->upd, dirty);
+    ck(cudaEventRecord(h->ev0, h->stream), "event");
+    ck(cudaMemcpyAsync(h->d_val, val, nnz * sizeof(double), cudaMemcpyHostToDevice, h->stream),
+       "upload values");
+    h->upd.upload(h->stream);
+    h->runPlan(h->upd);
+    ck(cudaEventRecord(h->ev1, h->stream), "event");
+    h->checkDevError();
+    float ms = 0;
+    ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "elapsed");
+    h->stats.seconds = ms * 1e-3;
+    h->stats.flops = h->upd.flops;
+    h->stats.fronts = h->upd.nfronts;
+  });
+}
+
+static int solveOrApply(mfgpu_handle* h, const double* in, double* out, int nrhs, int64_t ld,
+                        bool device, bool apply) {
+  if (!h) return MFGPU_ERR_ARG;
+  if (!h->factored) return fail(h, MFGPU_ERR_STATE, "Solve()/Apply() before Factor()");
+  if (!in || !out || nrhs < 0 || ld < h->n) return fail(h, MFGPU_ERR_ARG, "bad vector arguments");
+  if (nrhs == 0) return MFGPU_OK;
+  return guarded(h, [&]() {
+    const int chunk = 16;
+    ck(cudaEventRecord(h->ev0, h->stream), "event");
+    for (int c0 = 0; c0 < nrhs; c0 += chunk) {
+      const int nc = std::min(chunk, nrhs - c0);
+      h->ensureWork(nc);
+      double* X = h->d_X;
+      for (int c = 0; c < nc; c++)
+        ck(cudaMemcpyAsync(X + (int64_t)c * h->n, in + (int64_t)(c0 + c) * ld, h->n * sizeof(double),
+                           device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream),
+           "copy rhs in");
+      if (apply) h->applyChunk(X, h->n, nc);
+      else h->solveChunk(X, h->n, nc);
+      for (int c = 0; c < nc; c++)
+        ck(cudaMemcpyAsync(out + (int64_t)(c0 + c) * ld, X + (int64_t)c * h->n, h->n * sizeof(double),
+                           device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream),
+           "copy result out");
+      if (!device) ck(cudaStreamSynchronize(h->stream), "solve");
+    }
+    ck(cudaEventRecord(h->ev1, h->stream), "event");
+    ck(cudaEventSynchronize(h->ev1), "solve");
+    float ms = 0;
+    ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "elapsed");
+    h->stats.seconds = ms * 1e-3;
+    double fl = 0;
+    for (const mfgpu::Front& f : h->S->fronts) fl += 2.0 * ((double)f.n * f.n + 2.0 * f.n * f.m);
+    h->stats.flops = fl * nrhs;
+  });
+}
+
+int mfgpu_solve(mfgpu_handle* h, const double* b, double* x, int nrhs, int64_t ld) {
+  return solveOrApply(h, b, x, nrhs, ld, false, false);
+}
+int mfgpu_apply(mfgpu_handle* h, const double* x, double* b, int nrhs, int64_t ld) {
+  return solveOrApply(h, x, b, nrhs, ld, false, true);
+}
+int mfgpu_solve_device(mfgpu_handle* h, const double* b, double* x, int nrhs, int64_t ld) {
+  return solveOrApply(h, b, x, nrhs, ld, true, false);
+}
+int mfgpu_apply_device(mfgpu_handle* h, const double* x, double* b, int nrhs, int64_t ld) {
+  return solveOrApply(h, x, b, nrhs, ld, true, true);
+}
+
+int mfgpu_set_stream(mfgpu_handle* h, void* st) {
+  if (!h) return MFGPU_ERR_ARG;
+  return guarded(h, [&]() {
+    ck(cudaStreamSynchronize(h->stream), "sync old stream");
+    h->stream = st ? static_cast<cudaStream_t>(st) : h->own;
+  });
+}
+
+int mfgpu_get_info(const mfgpu_handle* h, mfgpu_info* info) {
+  if (!h || !info) return MFGPU_ERR_ARG;
+  const Schedule& s = *h->S;
+  std::memset(info, 0, sizeof(*info));
+  info->dim = s.dim;
+  info->levels = s.levels;
+  info->n_fronts = (int)s.fronts.size();
+  info->n_seps = (int)s.seps.size();
+  info->ndof = s.ndof;
+  info->nnz = h->nnz;
+  for (int a = 0; a < 3; a++) info->leaf_box[a] = s.bw[a];
+  for (const mfgpu::Front& f : s.fronts) info->max_front = std::max(info->max_front, f.N);
+  info->factor_flops = s.total_flops();
+  info->front_bytes = s.front_elems * 8;
+  info->sep_bytes = s.sep_elems * 8;
+  info->device_bytes = h->device_bytes;
+  return MFGPU_OK;
+}
+
+int mfgpu_last_stats(const mfgpu_handle* h, mfgpu_stats* st) {
+  if (!h || !st) return MFGPU_ERR_ARG;
+  *st = h->stats;
+  return MFGPU_OK;
+}
+
+const char* mfgpu_last_error(const mfgpu_handle* h) {
+  if (!h) return g_create_error.c_str();
+  return h->err.c_str();
+}
+
+void mfgpu_destroy(mfgpu_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  delete h;
+}
+
+// ---- host-only symbolic access ----
+struct mfgpu_symbolic {
+  std::unique_ptr<Schedule> S;
+};
+
+int mfgpu_symbolic_create(int dim, int nx, int ny, int nz, int width, int max_side,
+                          mfgpu_symbolic** out) {
+  if (!out) return MFGPU_ERR_ARG;
+  *out = nullptr;
+  g_sym_error.clear();
+  try {
+    std::unique_ptr<mfgpu_symbolic> s(new mfgpu_symbolic());
+    s->S.reset(new Schedule(dim, nx, ny, nz, width, max_side));
+    *out = s.release();
+    return MFGPU_OK;
+  } catch (const std::invalid_argument& e) {
+    g_sym_error = e.what();
+    return MFGPU_ERR_ARG;
+  } catch (const std::runtime_error& e) {
+    g_sym_error = e.what();
+    return std::string(e.what()).find("recursion depth") != std::string::npos ? MFGPU_ERR_DEPTH
+                                                                                : MFGPU_ERR_LEAF;
+  } catch (const std::bad_alloc&) {
+    return MFGPU_ERR_OOM;
+  }
+}
+
+void mfgpu_symbolic_destroy(mfgpu_symbolic* s) { delete s; }
+const char* mfgpu_symbolic_error(void) { return g_sym_error.c_str(); }
+
+int mfgpu_symbolic_sizes(const mfgpu_symbolic* s, int* levels, int* nf, int* ns, int64_t* ndof) {
+  if (!s) return MFGPU_ERR_ARG;
+  if (levels) *levels = s->S->levels;
+  if (nf) *nf = (int)s->S->fronts.size();
+  if (ns) *ns = (int)s->S->seps.size();
+  if (ndof) *ndof = s->S->ndof;
+  return MFGPU_OK;
+}
+
+int mfgpu_symbolic_front(const mfgpu_symbolic* s, int f, int* level, int* box, int* n, int* m,
+                         const int** dofs) {
+  if (!s || f < 0 || f >= (int)s->S->fronts.size()) return MFGPU_ERR_ARG;
+  const mfgpu::Front& F = s->S->fronts[f];
+  if (level) *level = F.level;
+  if (box) *box = F.box;
+  if (n) *n = F.n;
+  if (m) *m = F.m;
+  if (dofs) *dofs = s->S->dofs.data() + F.dof_off;
+  return MFGPU_OK;
+}
+
+int mfgpu_symbolic_sep(const mfgpu_symbolic* s, int k, int* level, int* idx, int* size,
+                       const int** dofs, int boxes[2], int rows[2]) {
+  if (!s || k < 0 || k >= (int)s->S->seps.size()) return MFGPU_ERR_ARG;
+  const mfgpu::Sep& e = s->S->seps[k];
+  if (level) *level = e.level;
+  if (idx) *idx = e.idx;
+  if (size) *size = e.s;
+  if (dofs) *dofs = s->S->dofs.data() + e.dof_off;
+  if (boxes) {
+    boxes[0] = e.box[0];
+    boxes[1] = e.box[1];
+  }
+  if (rows) {
+    rows[0] = e.bdpos[0];
+    rows[1] = e.bdpos[1];
+  }
+  return MFGPU_OK;
+}
+
+int64_t mfgpu_symbolic_tasks(const mfgpu_symbolic* s, int which, const void** tasks) {
+  if (!s) return -1;
+  const std::vector<Task>* v = which == 0 ? &s->S->front_tasks
+                               : which == 1 ? &s->S->sep_tasks
+                                            : &s->S->sep_add_tasks;
+  if (tasks) *tasks = v->data();
+  return (int64_t)v->size();
+}
+
+int mfgpu_symbolic_layout(const mfgpu_symbolic* s, int front_or_sep, int id, int64_t* off, int* ld) {
+  if (!s) return MFGPU_ERR_ARG;
+  if (front_or_sep == 0) {
+    if (id < 0 || id >= (int)s->S->fronts.size()) return MFGPU_ERR_ARG;
+    if (off) *off = s->S->fronts[id].off;
+    if (ld) *ld = s->S->fronts[id].ld;
+  } else {
+    if (id < 0 || id >= (int)s->S->seps.size()) return MFGPU_ERR_ARG;
+    if (off) *off = s->S->seps[id].off;
+    if (ld) *ld = s->S->seps[id].ld;
+  }
+  return MFGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,201 @@
+"""B200 multifrontal factor / localized update / solve (Python binding).
+
+`MF2D` / `MF3D` mirror the reference's TreeFactor2D::MF2D<double> and
+TreeFactor3D::MF3D<double> (include/DE/mf.hpp:67-80, 173-188): a constructor
+taking the CSR matrix, grid sizes, separator width and leaf parameter, then
+Factor(), Update(A, modifiedDOFs), Solve(b) and Apply(x).  Errors follow the
+reference: a too-shallow tree or broken leaf arithmetic raise RuntimeError
+(the reference throws std::runtime_error, src/DE/mf2d.cpp:42,64); a matrix
+that is not symmetric positive definite raises RuntimeError from Factor();
+bad arguments raise ValueError.  All compute runs in libmfgpu.so on the GPU;
+there is no CPU path.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import MFGPU_FP64, MFGPU_MIXED, TASK_DTYPE
+from .stencil import CSR, build_laplacian
+
+__all__ = ["MF2D", "MF3D", "Symbolic", "CSR", "build_laplacian", "MFGPU_FP64", "MFGPU_MIXED",
+           "MFError"]
+
+
+class MFError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{_lib.status_string(status)}: {msg}")
+        self.status = status
+
+
+def _raise(status, msg):
+    if status in (_lib.MFGPU_ERR_DEPTH, _lib.MFGPU_ERR_LEAF):
+        raise RuntimeError(msg)
+    if status == _lib.MFGPU_ERR_ARG:
+        raise ValueError(msg)
+    raise MFError(status, msg)
+
+
+class _MFBase:
+    _dim = None
+
+    def __init__(self, A, N, width=1, max_side_length=4, precision=MFGPU_FP64, device=0,
+                 refine_tol=1e-10, refine_maxit=50):
+        lib = _lib.load()
+        if not isinstance(A, CSR):
+            A = CSR(A.indptr, A.indices, A.data, A.shape[0])
+        self.A = A
+        self.N = tuple(int(x) for x in N)
+        opts = _lib.default_options(precision, device, refine_tol, refine_maxit)
+        h = C.c_void_p()
+        Nz = self.N[2] if self._dim == 3 else 1
+        st = lib.mfgpu_create(self._dim, self.N[0], self.N[1], Nz, int(width), int(max_side_length),
+                              int(A.n), _lib._ptr(A.row_ptr), _lib._ptr(A.col_ind), _lib._ptr(A.val),
+                              C.byref(opts), C.byref(h))
+        if st != _lib.MFGPU_OK:
+            _raise(st, lib.mfgpu_last_error(None).decode())
+        self._h = h
+        self._lib = lib
+
+    def _check(self, st):
+        if st != _lib.MFGPU_OK:
+            _raise(st, self._lib.mfgpu_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.mfgpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- the reference's public members ------------------------------------
+    def Factor(self):
+        self._check(self._lib.mfgpu_factor(self._h))
+
+    def Update(self, A, modifiedDOFs):
+        if not isinstance(A, CSR):
+            A = CSR(A.indptr, A.indices, A.data, A.shape[0])
+        mod = np.ascontiguousarray(sorted(set(int(d) for d in modifiedDOFs)), np.int32)
+        self._check(self._lib.mfgpu_update(self._h, _lib._ptr(A.val), A.nnz, _lib._ptr(mod),
+                                           len(mod)))
+        self.A = A
+
+    def _vec_op(self, v, fn):
+        v = np.asarray(v, np.float64)
+        one = v.ndim == 1
+        X = np.asfortranarray(v.reshape(-1, 1) if one else v)
+        if X.shape[0] != self.A.n:
+            raise ValueError("vector length does not match the matrix")
+        out = np.empty_like(X, order="F")
+        self._check(fn(self._h, X.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p),
+                       X.shape[1], X.shape[0]))
+        return out[:, 0] if one else out
+
+    def Solve(self, b):
+        """x = A^{-1} b for b of shape (n,) or (n, nrhs)."""
+        return self._vec_op(b, self._lib.mfgpu_solve)
+
+    def Apply(self, x):
+        """b = (factored A) x for x of shape (n,) or (n, nrhs)."""
+        return self._vec_op(x, self._lib.mfgpu_apply)
+
+    # -- extras ----------------------------------------------------------
+    def solve_device(self, b_ptr, x_ptr, nrhs, ld):
+        self._check(self._lib.mfgpu_solve_device(self._h, C.c_void_p(b_ptr), C.c_void_p(x_ptr),
+                                                 nrhs, ld))
+
+    def apply_device(self, x_ptr, b_ptr, nrhs, ld):
+        self._check(self._lib.mfgpu_apply_device(self._h, C.c_void_p(x_ptr), C.c_void_p(b_ptr),
+                                                 nrhs, ld))
+
+    def set_stream(self, stream_ptr):
+        self._check(self._lib.mfgpu_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def info(self):
+        inf = _lib.Info()
+        self._check(self._lib.mfgpu_get_info(self._h, C.byref(inf)))
+        return {f: (list(getattr(inf, f)) if f == "leaf_box" else getattr(inf, f))
+                for f, _ in _lib.Info._fields_}
+
+    def stats(self):
+        s = _lib.Stats()
+        self._check(self._lib.mfgpu_last_stats(self._h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in _lib.Stats._fields_}
+
+
+class MF2D(_MFBase):
+    """MF2D(A, Nx, Ny, width=1, maxSideLength=4)."""
+    _dim = 2
+
+    def __init__(self, A, Nx, Ny, width=1, maxSideLength=4, **kw):
+        super().__init__(A, (Nx, Ny), width, maxSideLength, **kw)
+
+
+class MF3D(_MFBase):
+    """MF3D(A, Nx, Ny, Nz, width=1, maxSideLength=4)."""
+    _dim = 3
+
+    def __init__(self, A, Nx, Ny, Nz, width=1, maxSideLength=4, **kw):
+        super().__init__(A, (Nx, Ny, Nz), width, maxSideLength, **kw)
+
+
+class Symbolic:
+    """Host-only view of the schedule: DOF lists and assembly tasks."""
+
+    def __init__(self, dim, N, width=1, max_side_length=4):
+        lib = _lib.load()
+        h = C.c_void_p()
+        Nz = N[2] if dim == 3 else 1
+        st = lib.mfgpu_symbolic_create(dim, N[0], N[1], Nz, width, max_side_length, C.byref(h))
+        if st != _lib.MFGPU_OK:
+            _raise(st, lib.mfgpu_symbolic_error().decode())
+        self._h, self._lib = h, lib
+        lv, nf, ns, nd = C.c_int(), C.c_int(), C.c_int(), C.c_int64()
+        lib.mfgpu_symbolic_sizes(h, C.byref(lv), C.byref(nf), C.byref(ns), C.byref(nd))
+        self.levels, self.n_fronts, self.n_seps, self.ndof = lv.value, nf.value, ns.value, nd.value
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.mfgpu_symbolic_destroy(self._h)
+            self._h = None
+
+    def front(self, f):
+        lv, bx, n, m = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        p = C.POINTER(C.c_int)()
+        st = self._lib.mfgpu_symbolic_front(self._h, f, C.byref(lv), C.byref(bx), C.byref(n),
+                                            C.byref(m), C.byref(p))
+        if st:
+            raise IndexError(f)
+        d = np.ctypeslib.as_array(p, shape=(n.value + m.value,)).copy() if n.value + m.value else \
+            np.zeros(0, np.int32)
+        off, ld = C.c_int64(), C.c_int()
+        self._lib.mfgpu_symbolic_layout(self._h, 0, f, C.byref(off), C.byref(ld))
+        return dict(level=lv.value, box=bx.value, n=n.value, m=m.value, dofs=d, off=off.value,
+                    ld=ld.value)
+
+    def sep(self, k):
+        lv, ix, sz = C.c_int(), C.c_int(), C.c_int()
+        p = C.POINTER(C.c_int)()
+        boxes = (C.c_int * 2)()
+        rows = (C.c_int * 2)()
+        st = self._lib.mfgpu_symbolic_sep(self._h, k, C.byref(lv), C.byref(ix), C.byref(sz),
+                                          C.byref(p), boxes, rows)
+        if st:
+            raise IndexError(k)
+        d = np.ctypeslib.as_array(p, shape=(sz.value,)).copy() if sz.value else np.zeros(0, np.int32)
+        off, ld = C.c_int64(), C.c_int()
+        self._lib.mfgpu_symbolic_layout(self._h, 1, k, C.byref(off), C.byref(ld))
+        return dict(level=lv.value, idx=ix.value, size=sz.value, dofs=d, boxes=list(boxes),
+                    rows=list(rows), off=off.value, ld=ld.value)
+
+    def tasks(self, which):
+        p = C.c_void_p()
+        n = self._lib.mfgpu_symbolic_tasks(self._h, which, C.byref(p))
+        if n <= 0:
+            return np.zeros(0, TASK_DTYPE)
+        buf = (C.c_char * (n * TASK_DTYPE.itemsize)).from_address(p.value)
+        return np.frombuffer(bytes(buf), dtype=TASK_DTYPE)
