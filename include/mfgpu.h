@@ -91,6 +91,17 @@ int mfgpu_factor(mfgpu_handle* h);
 int mfgpu_update(mfgpu_handle* h, const double* val, int64_t nnz, const int* modified_dofs,
                  int n_modified);
 
+/* Device-pointer form of Update (no reference counterpart): d_val in device
+ * memory, modified_dofs on the host. */
+int mfgpu_update_device(mfgpu_handle* h, const double* d_val, int64_t nnz,
+                        const int* modified_dofs, int n_modified);
+
+/* Replace all matrix values (same pattern) and refactor every front: the
+ * reference's Update(A, every DOF) (src/DE/mf2d.cpp:150-181 with all leaves
+ * marked), without building the modified-DOF set. */
+int mfgpu_refactor(mfgpu_handle* h, const double* val, int64_t nnz);
+int mfgpu_refactor_device(mfgpu_handle* h, const double* d_val, int64_t nnz);
+
 /* Vec Solve(const Vec& b) — include/DE/mf.hpp:81, src/DE/mf2d.cpp:976-1054.
  * Host buffers: b and x are n x nrhs column-major with leading dimension ld. */
 int mfgpu_solve(mfgpu_handle* h, const double* b, double* x, int nrhs, int64_t ld);
@@ -106,6 +117,28 @@ int mfgpu_apply_device(mfgpu_handle* h, const double* d_x, double* d_b, int nrhs
 /* Use an external CUDA stream (cudaStream_t) for all later work; NULL restores
  * the handle's own stream. */
 int mfgpu_set_stream(mfgpu_handle* h, void* cuda_stream);
+
+/* Per-kernel-class device timing (no reference counterpart; the reference's
+ * HASCPP11TIMING millisecond counters, src/DE/mf2d.cpp:15-18, 464-499, are the
+ * closest).  When enabled, every launch group is bracketed by CUDA events on
+ * the handle's stream; reads return cumulative launches, milliseconds and the
+ * algorithmic flops / bytes of the work those launches did. */
+enum mfgpu_kernel_class {
+  MFGPU_KC_ASSEMBLE = 0,  /* front / separator assembly and accumulation     */
+  MFGPU_KC_POTRF = 1,     /* diagonal-block Cholesky of each panel           */
+  MFGPU_KC_TRSM = 2,      /* panel triangular solves                         */
+  MFGPU_KC_SYRK = 3,      /* trailing symmetric updates (Schur complements)  */
+  MFGPU_KC_SOLVE = 4,     /* forward / backward sweeps                       */
+  MFGPU_KC_APPLY = 5,     /* factored-operator application                   */
+  MFGPU_KC_COUNT = 6
+};
+int mfgpu_profile_enable(mfgpu_handle* h, int on);
+int mfgpu_profile_reset(mfgpu_handle* h);
+int mfgpu_profile_read(const mfgpu_handle* h, int kernel_class, int64_t* launches, double* ms,
+                       double* flops, double* bytes);
+/* Kernels launched by this library since it was loaded (all handles). */
+long long mfgpu_kernel_launches(void);
+
 int mfgpu_get_info(const mfgpu_handle* h, mfgpu_info* info);
 int mfgpu_last_stats(const mfgpu_handle* h, mfgpu_stats* stats);
 const char* mfgpu_last_error(const mfgpu_handle* h);
@@ -134,6 +167,11 @@ int mfgpu_symbolic_sep(const mfgpu_symbolic* s, int k, int* level, int* idx, int
  * separator accumulation tasks.  Returns the count; `tasks` points at an
  * array of 56-byte records laid out as in the C++ struct mfgpu::Task. */
 int64_t mfgpu_symbolic_tasks(const mfgpu_symbolic* s, int which, const void** tasks);
+/* Fronts a localized update with these modified DOFs refactors (the leaf-marking
+ * rule of src/DE/mf2d.cpp:163-174 followed by root paths): dirty[f] = 1 for
+ * each, *flops = their Cholesky-form flops.  Returns the count, -1 on error. */
+int64_t mfgpu_symbolic_dirty(const mfgpu_symbolic* s, const int* modified_dofs, int n_modified,
+                             unsigned char* dirty, double* flops);
 /* Arena layout of front f / separator k: element offset and leading dimension. */
 int mfgpu_symbolic_layout(const mfgpu_symbolic* s, int front_or_sep, int id, int64_t* off,
                           int* ld);

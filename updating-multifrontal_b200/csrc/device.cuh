@@ -41,9 +41,18 @@ void launch_tasks(const Task* tasks, const int64_t* tstart, int ntasks, int64_t 
                   double* fronts, double* seps, const int* rp, const int* ci, const double* va,
                   const int* dofs, cudaStream_t st);
 
-// One panel step of the partial Cholesky for every front in flist.
-void launch_panel_step(const int* flist, int nf, const FrontDev* fr, double* F, int k,
-                       int max_rows, DevError* err, cudaStream_t st);
+// One panel step k of the partial Cholesky for every front in flist: the
+// diagonal block factorization, the triangular solve of the rows below it
+// (max_rows bounds N - k over the list) and the trailing symmetric update.
+void launch_potrf(const int* flist, int nf, const FrontDev* fr, double* F, int k, DevError* err,
+                  cudaStream_t st);
+void launch_trsm(const int* flist, int nf, const FrontDev* fr, double* F, int k, int max_rows,
+                 cudaStream_t st);
+void launch_syrk(const int* flist, int nf, const FrontDev* fr, double* F, int k, int max_rows,
+                 cudaStream_t st);
+
+// Number of kernels this library has launched since it was loaded.
+long long launches_total();
 
 // Solve / apply sweeps (nrhs <= 16 per call).  W holds 2*N*nrhs doubles per
 // front at offset woff[f]*nrhs (woff = exclusive prefix of 2*N).

@@ -9,11 +9,14 @@
 //   rows/cols [n,N)^2        hold the update matrix: Schur complement
 //                            S = -L21 L21^T on the separator diagonal blocks,
 //                            A11 + S elsewhere (the reference's A11post).
+#include <atomic>
 #include <cstdio>
 
 #include "device.cuh"
 
 namespace mfgpu {
+
+std::atomic<long long> g_launches{0};
 
 namespace {
 
@@ -483,51 +486,77 @@ void launch_tasks(const Task* tasks, const int64_t* tstart, int ntasks, int64_t 
   const int64_t gy = (ntiles + gx - 1) / gx;
   k_tasks<<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(tasks, tstart, ntasks, fronts,
                                                                       seps, rp, ci, va, dofs);
+  g_launches++;
 }
 
-void launch_panel_step(const int* flist, int nf, const FrontDev* fr, double* F, int k,
-                       int max_rows, DevError* err, cudaStream_t st) {
+void launch_potrf(const int* flist, int nf, const FrontDev* fr, double* F, int k, DevError* err,
+                  cudaStream_t st) {
   if (nf <= 0) return;
   k_potrf<<<nf, 32, 0, st>>>(flist, fr, F, k, err);
+  g_launches++;
+}
+void launch_trsm(const int* flist, int nf, const FrontDev* fr, double* F, int k, int max_rows,
+                 cudaStream_t st) {
   const int rows = max_rows - k - 1;
-  if (rows <= 0) return;
+  if (nf <= 0 || rows <= 0) return;
   k_trsm<<<dim3((rows + 127) / 128, nf), 128, 0, st>>>(flist, fr, F, k);
+  g_launches++;
+}
+void launch_syrk(const int* flist, int nf, const FrontDev* fr, double* F, int k, int max_rows,
+                 cudaStream_t st) {
+  const int rows = max_rows - k - 1;
+  if (nf <= 0 || rows <= 0) return;
   const int T = (rows + UT - 1) / UT;
   k_syrk<<<dim3(T * (T + 1) / 2, nf), 256, 0, st>>>(flist, fr, F, k);
+  g_launches++;
 }
+
+long long launches_total() { return g_launches.load(); }
 
 void launch_solve_fwd(const int* flist, int nf, const FrontDev* fr, const double* F,
                       const int* dofs, double* X, int64_t ldx, int nrhs, double* W,
                       const int64_t* woff, cudaStream_t st) {
-  if (nf > 0) k_solve_fwd<<<nf, ST, 0, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff);
+  if (nf <= 0) return;
+  k_solve_fwd<<<nf, ST, 0, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff);
+  g_launches++;
 }
 void launch_solve_bwd(const int* flist, int nf, const FrontDev* fr, const double* F,
                       const int* dofs, double* X, int64_t ldx, int nrhs, double* W,
                       const int64_t* woff, cudaStream_t st) {
-  if (nf > 0) k_solve_bwd<<<nf, ST, 0, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff);
+  if (nf <= 0) return;
+  k_solve_bwd<<<nf, ST, 0, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff);
+  g_launches++;
 }
 void launch_apply_up(const int* flist, int nf, const FrontDev* fr, const double* F,
                      const int* dofs, double* X, int64_t ldx, int nrhs, double* W,
                      const int64_t* woff, double* T, cudaStream_t st) {
-  if (nf > 0) k_apply_up<<<nf, ST, 0, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff, T);
+  if (nf <= 0) return;
+  k_apply_up<<<nf, ST, 0, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff, T);
+  g_launches++;
 }
 void launch_apply_down(const int* flist, int nf, const FrontDev* fr, const double* F,
                        const int* dofs, int64_t ldx, int nrhs, double* W, const int64_t* woff,
                        const double* T, cudaStream_t st) {
-  if (nf > 0) k_apply_down<<<nf, ST, 0, st>>>(flist, fr, F, dofs, ldx, nrhs, W, woff, T);
+  if (nf <= 0) return;
+  k_apply_down<<<nf, ST, 0, st>>>(flist, fr, F, dofs, ldx, nrhs, W, woff, T);
+  g_launches++;
 }
 void launch_root_solve(int f, const FrontDev* fr, const double* F, const int* dofs, double* X,
                        int64_t ldx, int nrhs, double* W, const int64_t* woff, cudaStream_t st) {
   k_root_solve<<<1, ST, 0, st>>>(f, fr, F, dofs, X, ldx, nrhs, W, woff);
+  g_launches++;
 }
 void launch_root_apply(int f, const FrontDev* fr, const double* F, const int* dofs, double* X,
                        int64_t ldx, int nrhs, double* W, const int64_t* woff, cudaStream_t st) {
   k_root_apply<<<1, ST, 0, st>>>(f, fr, F, dofs, X, ldx, nrhs, W, woff);
+  g_launches++;
 }
 void launch_sep_gather(const int* slist, int ns, const SepDev* sp, const int* dofs, double* X,
                        int64_t ldx, int nrhs, const double* W, const int64_t* woff,
                        const FrontDev* fr, cudaStream_t st) {
-  if (ns > 0) k_sep_gather<<<ns, ST, 0, st>>>(slist, sp, dofs, X, ldx, nrhs, W, woff, fr);
+  if (ns <= 0) return;
+  k_sep_gather<<<ns, ST, 0, st>>>(slist, sp, dofs, X, ldx, nrhs, W, woff, fr);
+  g_launches++;
 }
 
 }  // namespace mfgpu

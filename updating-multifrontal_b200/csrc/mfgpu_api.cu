@@ -140,6 +140,62 @@ struct Plan {
   }
 };
 
+// Optional per-kernel-class device timing: an event pair around each launch
+// group, read back after the call's final synchronisation.
+struct Profiler {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  struct Mark {
+    int cls;
+    cudaEvent_t a, b;
+  };
+  std::vector<Mark> marks;
+  int64_t launches[MFGPU_KC_COUNT] = {};
+  double ms[MFGPU_KC_COUNT] = {};
+  double flops[MFGPU_KC_COUNT] = {};
+  double bytes[MFGPU_KC_COUNT] = {};
+
+  cudaEvent_t ev() {
+    if (used == pool.size()) {
+      cudaEvent_t e;
+      ck(cudaEventCreate(&e), "profiler event");
+      pool.push_back(e);
+    }
+    return pool[used++];
+  }
+  void begin(int cls, cudaStream_t st) {
+    if (!on) return;
+    Mark m{cls, ev(), nullptr};
+    ck(cudaEventRecord(m.a, st), "profiler record");
+    marks.push_back(m);
+  }
+  void end(cudaStream_t st) {
+    if (!on || marks.empty()) return;
+    marks.back().b = ev();
+    ck(cudaEventRecord(marks.back().b, st), "profiler record");
+  }
+  void collect() {
+    for (const Mark& m : marks) {
+      float t = 0;
+      if (m.b && cudaEventElapsedTime(&t, m.a, m.b) == cudaSuccess) {
+        ms[m.cls] += t;
+        launches[m.cls] += 1;
+      }
+    }
+    marks.clear();
+    used = 0;
+  }
+  void reset() {
+    marks.clear();
+    used = 0;
+    for (int i = 0; i < MFGPU_KC_COUNT; i++) launches[i] = 0, ms[i] = flops[i] = bytes[i] = 0;
+  }
+  ~Profiler() {
+    for (cudaEvent_t e : pool) cudaEventDestroy(e);
+  }
+};
+
 }  // namespace
 
 struct mfgpu_handle {
@@ -174,6 +230,7 @@ struct mfgpu_handle {
   Plan full, upd;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int64_t device_bytes = 0;
+  Profiler prof;
 
   ~mfgpu_handle() {
     if (stream) cudaStreamSynchronize(stream);
@@ -239,10 +296,27 @@ struct mfgpu_handle {
     }
   }
 
-  void runGroup(const Plan& P, const Group& g) {
+  void runGroup(const Plan& P, const Group& g, int64_t bytes) {
     if (g.ntasks == 0 || g.ntiles == 0) return;
+    prof.begin(MFGPU_KC_ASSEMBLE, stream);
     mfgpu::launch_tasks(P.d_tasks + g.task0, P.d_pref + g.pref0, (int)g.ntasks, g.ntiles, d_F, d_Sep,
                         d_rp, d_ci, d_val, d_dofs, stream);
+    prof.end(stream);
+    if (prof.on) prof.bytes[MFGPU_KC_ASSEMBLE] += (double)bytes;
+  }
+
+  // Bytes an assembly group must move: every destination element written,
+  // plus the element read for copies and adds (read twice for adds).
+  int64_t groupBytes(const Plan& P, const Group& g) const {
+    if (!prof.on) return 0;
+    int64_t b = 0;
+    for (int64_t t = g.task0; t < g.task0 + g.ntasks; t++) {
+      const Task& T = P.tasks[t];
+      int64_t e = T.lower ? (int64_t)T.rows * (T.rows + 1) / 2 : (int64_t)T.rows * T.cols;
+      int mult = T.kind == mfgpu::TK_ZERO ? 1 : T.kind == mfgpu::TK_ADD ? 3 : 2;
+      b += e * 8 * mult;
+    }
+    return b;
   }
 
   // Run a factorization plan: per level, separator base assembly, front
@@ -252,16 +326,45 @@ struct mfgpu_handle {
     ck(cudaMemsetAsync(d_err, 0, sizeof(DevError), stream), "clear error word");
     for (int ell = s.levels - 1; ell >= 0; ell--) {
       const Plan::Level& L = P.lv[ell];
-      runGroup(P, L.sbase);
-      runGroup(P, L.ftask);
+      runGroup(P, L.sbase, groupBytes(P, L.sbase));
+      runGroup(P, L.ftask, groupBytes(P, L.ftask));
       if (L.nf > 0) {
-        for (int k = 0; k < L.maxn; k += mfgpu::kPanel)
-          mfgpu::launch_panel_step(P.d_ids + L.f0, (int)L.nf, d_fr, d_F, k, L.maxN, d_err, stream);
+        const int* fl = P.d_ids + L.f0;
+        for (int k = 0; k < L.maxn; k += mfgpu::kPanel) {
+          if (prof.on) {
+            for (int64_t i = L.f0; i < L.f0 + L.nf; i++) {
+              const mfgpu::Front& f = s.fronts[P.ids[i]];
+              if (k >= f.n) continue;
+              double kb = std::min(mfgpu::kPanel, f.n - k), M = f.N - k - kb;
+              prof.flops[MFGPU_KC_POTRF] += kb * kb * kb / 3.0;
+              prof.flops[MFGPU_KC_TRSM] += M * kb * kb;
+              prof.flops[MFGPU_KC_SYRK] += M * M * kb;
+            }
+          }
+          prof.begin(MFGPU_KC_POTRF, stream);
+          mfgpu::launch_potrf(fl, (int)L.nf, d_fr, d_F, k, d_err, stream);
+          prof.end(stream);
+          prof.begin(MFGPU_KC_TRSM, stream);
+          mfgpu::launch_trsm(fl, (int)L.nf, d_fr, d_F, k, L.maxN, stream);
+          prof.end(stream);
+          prof.begin(MFGPU_KC_SYRK, stream);
+          mfgpu::launch_syrk(fl, (int)L.nf, d_fr, d_F, k, L.maxN, stream);
+          prof.end(stream);
+        }
       }
-      runGroup(P, L.sadd0);
-      runGroup(P, L.sadd1);
+      runGroup(P, L.sadd0, groupBytes(P, L.sadd0));
+      runGroup(P, L.sadd1, groupBytes(P, L.sadd1));
     }
     ck(cudaGetLastError(), "factor launch");
+  }
+
+  // Replace the matrix values (same pattern) and refactor a plan.
+  void factorWith(const double* val, bool device, const Plan& P) {
+    if (val)
+      ck(cudaMemcpyAsync(d_val, val, nnz * sizeof(double),
+                         device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream),
+         "upload values");
+    runPlan(P);
   }
 
   void checkDevError() {
@@ -485,14 +588,19 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n
   return MFGPU_OK;
 }
 
-int mfgpu_factor(mfgpu_handle* h) {
+static int factorImpl(mfgpu_handle* h, const double* val, int64_t nnz, bool device) {
+  if (!h) return MFGPU_ERR_ARG;
+  if (val && nnz != h->nnz)
+    return fail(h, MFGPU_ERR_ARG, "values must match the pattern given at creation");
   return guarded(h, [&]() {
+    h->factored = false;
     ck(cudaEventRecord(h->ev0, h->stream), "event");
-    h->runPlan(h->full);
+    h->factorWith(val, device, h->full);
     ck(cudaEventRecord(h->ev1, h->stream), "event");
     h->checkDevError();
     float ms = 0;
     ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "elapsed");
+    h->prof.collect();
     h->stats.seconds = ms * 1e-3;
     h->stats.flops = h->full.flops;
     h->stats.fronts = h->full.nfronts;
@@ -500,7 +608,18 @@ int mfgpu_factor(mfgpu_handle* h) {
   });
 }
 
-int mfgpu_update(mfgpu_handle* h, const double* val, int64_t nnz, const int* mod, int nmod) {
+int mfgpu_factor(mfgpu_handle* h) { return factorImpl(h, nullptr, 0, false); }
+int mfgpu_refactor(mfgpu_handle* h, const double* val, int64_t nnz) {
+  if (!val) return fail(h, MFGPU_ERR_ARG, "null values");
+  return factorImpl(h, val, nnz, false);
+}
+int mfgpu_refactor_device(mfgpu_handle* h, const double* d_val, int64_t nnz) {
+  if (!d_val) return fail(h, MFGPU_ERR_ARG, "null values");
+  return factorImpl(h, d_val, nnz, true);
+}
+
+static int updateImpl(mfgpu_handle* h, const double* val, int64_t nnz, const int* mod, int nmod,
+                      bool device) {
   if (!h) return MFGPU_ERR_ARG;
   if (!h->factored) return fail(h, MFGPU_ERR_STATE, "Update() before Factor()");
   if (!val || nnz != h->nnz || (nmod > 0 && !mod) || nmod < 0)
@@ -509,31 +628,57 @@ int mfgpu_update(mfgpu_handle* h, const double* val, int64_t nnz, const int* mod
     if (mod[i] < 0 || mod[i] >= h->n) return fail(h, MFGPU_ERR_ARG, "modified DOF out of range");
   return guarded(h, [&]() {
     const Schedule& s = *h->S;
-    // dirty leaves (mf2d.cpp:163-174), then their root paths
-    std::vector<char> dirty(s.fronts.size(), 0);
-    for (int i = 0; i < nmod; i++) {
-      int f = s.leaf_of_dof(mod[i]);
-      while (f >= 0 && !dirty[f]) {
-        dirty[f] = 1;
-        f = s.fronts[f].parent;
-      }
-    }
-    dirty[0] = 1;   // the root is always refactored (mf2d.cpp:633-657)
-    h->buildPlan(h->upd, dirty);
+    std::vector<char> dirty;
+    const size_t ndirty = s.dirty_fronts(mod, nmod, dirty);
     ck(cudaEventRecord(h->ev0, h->stream), "event");
-    ck(cudaMemcpyAsync(h->d_val, val, nnz * sizeof(double), cudaMemcpyHostToDevice, h->stream),
-       "upload values");
-    h->upd.upload(h->stream);
-    h->runPlan(h->upd);
+    const Plan* P = &h->full;
+    if (ndirty < s.fronts.size()) {
+      h->buildPlan(h->upd, dirty);
+      h->upd.upload(h->stream);
+      P = &h->upd;
+    }
+    h->factored = false;
+    h->factorWith(val, device, *P);
     ck(cudaEventRecord(h->ev1, h->stream), "event");
     h->checkDevError();
+    h->factored = true;
     float ms = 0;
     ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "elapsed");
+    h->prof.collect();
     h->stats.seconds = ms * 1e-3;
-    h->stats.flops = h->upd.flops;
-    h->stats.fronts = h->upd.nfronts;
+    h->stats.flops = P->flops;
+    h->stats.fronts = P->nfronts;
   });
 }
+
+int mfgpu_update(mfgpu_handle* h, const double* val, int64_t nnz, const int* mod, int nmod) {
+  return updateImpl(h, val, nnz, mod, nmod, false);
+}
+int mfgpu_update_device(mfgpu_handle* h, const double* d_val, int64_t nnz, const int* mod,
+                        int nmod) {
+  return updateImpl(h, d_val, nnz, mod, nmod, true);
+}
+
+int mfgpu_profile_enable(mfgpu_handle* h, int on) {
+  if (!h) return MFGPU_ERR_ARG;
+  h->prof.on = on != 0;
+  return MFGPU_OK;
+}
+int mfgpu_profile_reset(mfgpu_handle* h) {
+  if (!h) return MFGPU_ERR_ARG;
+  h->prof.reset();
+  return MFGPU_OK;
+}
+int mfgpu_profile_read(const mfgpu_handle* h, int cls, int64_t* launches, double* ms,
+                       double* flops, double* bytes) {
+  if (!h || cls < 0 || cls >= MFGPU_KC_COUNT) return MFGPU_ERR_ARG;
+  if (launches) *launches = h->prof.launches[cls];
+  if (ms) *ms = h->prof.ms[cls];
+  if (flops) *flops = h->prof.flops[cls];
+  if (bytes) *bytes = h->prof.bytes[cls];
+  return MFGPU_OK;
+}
+long long mfgpu_kernel_launches(void) { return mfgpu::launches_total(); }
 
 static int solveOrApply(mfgpu_handle* h, const double* in, double* out, int nrhs, int64_t ld,
                         bool device, bool apply) {
@@ -552,8 +697,23 @@ static int solveOrApply(mfgpu_handle* h, const double* in, double* out, int nrhs
         ck(cudaMemcpyAsync(X + (int64_t)c * h->n, in + (int64_t)(c0 + c) * ld, h->n * sizeof(double),
                            device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream),
            "copy rhs in");
+      h->prof.begin(apply ? MFGPU_KC_APPLY : MFGPU_KC_SOLVE, h->stream);
       if (apply) h->applyChunk(X, h->n, nc);
       else h->solveChunk(X, h->n, nc);
+      h->prof.end(h->stream);
+      if (h->prof.on) {
+        // L11 (lower) and L21 are read once forward and once backward; the
+        // right-hand sides are gathered and scattered per front.
+        double fl = 0, by = 0;
+        for (const mfgpu::Front& f : h->S->fronts) {
+          fl += 2.0 * ((double)f.n * f.n + 2.0 * f.n * f.m) * nc;
+          by += 2.0 * 8.0 * ((double)f.n * (f.n + 1) / 2 + (double)f.n * f.m) +
+                8.0 * 4.0 * f.N * nc;
+        }
+        const int kc = apply ? MFGPU_KC_APPLY : MFGPU_KC_SOLVE;
+        h->prof.flops[kc] += fl;
+        h->prof.bytes[kc] += by;
+      }
       for (int c = 0; c < nc; c++)
         ck(cudaMemcpyAsync(out + (int64_t)(c0 + c) * ld, X + (int64_t)c * h->n, h->n * sizeof(double),
                            device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream),
@@ -562,6 +722,7 @@ static int solveOrApply(mfgpu_handle* h, const double* in, double* out, int nrhs
     }
     ck(cudaEventRecord(h->ev1, h->stream), "event");
     ck(cudaEventSynchronize(h->ev1), "solve");
+    h->prof.collect();
     float ms = 0;
     ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "elapsed");
     h->stats.seconds = ms * 1e-3;
@@ -705,6 +866,22 @@ int64_t mfgpu_symbolic_tasks(const mfgpu_symbolic* s, int which, const void** ta
                                             : &s->S->sep_add_tasks;
   if (tasks) *tasks = v->data();
   return (int64_t)v->size();
+}
+
+int64_t mfgpu_symbolic_dirty(const mfgpu_symbolic* s, const int* mod, int nmod,
+                             unsigned char* dirty, double* flops) {
+  if (!s || nmod < 0 || (nmod > 0 && !mod)) return -1;
+  for (int i = 0; i < nmod; i++)
+    if (mod[i] < 0 || mod[i] >= s->S->ndof) return -1;
+  std::vector<char> d;
+  size_t nd = s->S->dirty_fronts(mod, nmod, d);
+  double fl = 0;
+  for (size_t f = 0; f < d.size(); f++) {
+    if (dirty) dirty[f] = (unsigned char)d[f];
+    if (d[f]) fl += s->S->front_flops(s->S->fronts[f]);
+  }
+  if (flops) *flops = fl;
+  return (int64_t)nd;
 }
 
 int mfgpu_symbolic_layout(const mfgpu_symbolic* s, int front_or_sep, int id, int64_t* off, int* ld) {

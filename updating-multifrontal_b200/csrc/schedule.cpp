@@ -677,6 +677,29 @@ int Schedule::leaf_of_dof(int dof) const {
   return lv[levels - 1].front0 + box;
 }
 
+// The reference marks the leaf of each modified DOF (mf2d.cpp:163-174) and, at
+// every level, the parents of both boxes next to each marked separator
+// (mf2d.cpp:607-614).  A box's Schur complement depends only on its own subtree
+// and a separator is recomputed whenever a box next to it is, so refactoring
+// the root paths of the marked leaves gives the same factors with fewer fronts.
+size_t Schedule::dirty_fronts(const int* mod, int nmod, std::vector<char>& dirty) const {
+  dirty.assign(fronts.size(), 0);
+  size_t nd = 0;
+  for (int i = 0; i < nmod; i++) {
+    int f = leaf_of_dof(mod[i]);
+    while (f >= 0 && !dirty[f]) {
+      dirty[f] = 1;
+      nd++;
+      f = fronts[f].parent;
+    }
+  }
+  if (!dirty[0]) {
+    dirty[0] = 1;   // the root is always refactored (mf2d.cpp:633-657)
+    nd++;
+  }
+  return nd;
+}
+
 double Schedule::front_flops(const Front& f) const {
   double n = f.n, m = f.m;
   return n * n * n / 3.0 + n * n * m + n * m * m;

@@ -89,6 +89,9 @@ class Schedule {
   std::vector<Task> sep_add_tasks;        // two per separator: += box0 block, += box1 block
   // Per leaf box the global front id, for the modified-DOF -> leaf map.
   int leaf_of_dof(int dof) const;
+  // Fronts a localized update must refactor: the leaves holding modified DOFs
+  // and all their ancestors, plus the root.  Returns how many are marked.
+  size_t dirty_fronts(const int* mod, int nmod, std::vector<char>& dirty) const;
 
   // Work model (Cholesky form): sum over fronts of n^3/3 + n^2 m + n m^2.
   double front_flops(const Front& f) const;

@@ -104,6 +104,49 @@ class _MFBase:
         return self._vec_op(x, self._lib.mfgpu_apply)
 
     # -- extras ----------------------------------------------------------
+    def refactor(self, val):
+        """Replace every matrix value (same pattern) and refactor all fronts."""
+        val = np.ascontiguousarray(val, np.float64)
+        self._check(self._lib.mfgpu_refactor(self._h, _lib._ptr(val), val.size))
+
+    def refactor_device(self, val_ptr, nnz):
+        self._check(self._lib.mfgpu_refactor_device(self._h, C.c_void_p(val_ptr), nnz))
+
+    def update_device(self, val_ptr, nnz, modifiedDOFs):
+        mod = np.ascontiguousarray(sorted(set(int(d) for d in modifiedDOFs)), np.int32)
+        self._check(self._lib.mfgpu_update_device(self._h, C.c_void_p(val_ptr), nnz,
+                                                  _lib._ptr(mod), len(mod)))
+
+    def update_host_ptr(self, val_ptr, nnz, mod):
+        """Update from a raw host pointer (e.g. pinned memory); mod int32 array."""
+        self._check(self._lib.mfgpu_update(self._h, C.c_void_p(val_ptr), nnz, _lib._ptr(mod),
+                                           len(mod)))
+
+    def refactor_host_ptr(self, val_ptr, nnz):
+        self._check(self._lib.mfgpu_refactor(self._h, C.c_void_p(val_ptr), nnz))
+
+    def solve_host_ptr(self, b_ptr, x_ptr, nrhs, ld):
+        self._check(self._lib.mfgpu_solve(self._h, C.c_void_p(b_ptr), C.c_void_p(x_ptr), nrhs, ld))
+
+    def profile(self, on=True):
+        self._check(self._lib.mfgpu_profile_enable(self._h, 1 if on else 0))
+
+    def profile_reset(self):
+        self._check(self._lib.mfgpu_profile_reset(self._h))
+
+    def profile_read(self):
+        out = {}
+        for i, nm in enumerate(_lib.KERNEL_CLASSES):
+            la, ms, fl, by = C.c_int64(), C.c_double(), C.c_double(), C.c_double()
+            self._check(self._lib.mfgpu_profile_read(self._h, i, C.byref(la), C.byref(ms),
+                                                     C.byref(fl), C.byref(by)))
+            out[nm] = dict(launches=la.value, ms=ms.value, flops=fl.value, bytes=by.value)
+        return out
+
+    @staticmethod
+    def kernel_launches():
+        return int(_lib.load().mfgpu_kernel_launches())
+
     def solve_device(self, b_ptr, x_ptr, nrhs, ld):
         self._check(self._lib.mfgpu_solve_device(self._h, C.c_void_p(b_ptr), C.c_void_p(x_ptr),
                                                  nrhs, ld))
@@ -191,6 +234,17 @@ class Symbolic:
         self._lib.mfgpu_symbolic_layout(self._h, 1, k, C.byref(off), C.byref(ld))
         return dict(level=lv.value, idx=ix.value, size=sz.value, dofs=d, boxes=list(boxes),
                     rows=list(rows), off=off.value, ld=ld.value)
+
+    def dirty(self, modifiedDOFs):
+        """(dirty flags per front, their flops) of a localized update."""
+        mod = np.ascontiguousarray(sorted(set(int(d) for d in modifiedDOFs)), np.int32)
+        out = np.zeros(self.n_fronts, np.uint8)
+        fl = C.c_double()
+        n = self._lib.mfgpu_symbolic_dirty(self._h, _lib._ptr(mod), len(mod), _lib._ptr(out),
+                                           C.byref(fl))
+        if n < 0:
+            raise ValueError("modified DOF out of range")
+        return out.astype(bool), fl.value
 
     def tasks(self, which):
         p = C.c_void_p()

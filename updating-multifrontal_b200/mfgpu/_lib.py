@@ -28,8 +28,12 @@ EXPORTED = [
     "mfgpu_set_stream", "mfgpu_get_info", "mfgpu_last_stats", "mfgpu_last_error",
     "mfgpu_destroy", "mfgpu_symbolic_create", "mfgpu_symbolic_destroy", "mfgpu_symbolic_error",
     "mfgpu_symbolic_sizes", "mfgpu_symbolic_front", "mfgpu_symbolic_sep", "mfgpu_symbolic_tasks",
-    "mfgpu_symbolic_layout",
+    "mfgpu_symbolic_layout", "mfgpu_update_device", "mfgpu_refactor", "mfgpu_refactor_device",
+    "mfgpu_profile_enable", "mfgpu_profile_reset", "mfgpu_profile_read", "mfgpu_kernel_launches",
+    "mfgpu_symbolic_dirty",
 ]
+
+KERNEL_CLASSES = ["assemble", "potrf", "trsm", "syrk", "solve", "apply"]
 
 
 class Options(C.Structure):
@@ -86,6 +90,20 @@ def load(path=None):
         f = getattr(lib, nm)
         f.argtypes = [P, C.c_void_p, C.c_void_p, C.c_int, C.c_int64]
         f.restype = C.c_int
+    lib.mfgpu_update_device.argtypes = [P, C.c_void_p, C.c_int64, C.c_void_p, C.c_int]
+    lib.mfgpu_update_device.restype = C.c_int
+    lib.mfgpu_refactor.argtypes = [P, C.c_void_p, C.c_int64]
+    lib.mfgpu_refactor.restype = C.c_int
+    lib.mfgpu_refactor_device.argtypes = [P, C.c_void_p, C.c_int64]
+    lib.mfgpu_refactor_device.restype = C.c_int
+    lib.mfgpu_profile_enable.argtypes = [P, C.c_int]
+    lib.mfgpu_profile_enable.restype = C.c_int
+    lib.mfgpu_profile_reset.argtypes = [P]
+    lib.mfgpu_profile_reset.restype = C.c_int
+    lib.mfgpu_profile_read.argtypes = [P, C.c_int, C.POINTER(C.c_int64), dp, dp, dp]
+    lib.mfgpu_profile_read.restype = C.c_int
+    lib.mfgpu_kernel_launches.argtypes = []
+    lib.mfgpu_kernel_launches.restype = C.c_longlong
     lib.mfgpu_set_stream.argtypes = [P, C.c_void_p]
     lib.mfgpu_set_stream.restype = C.c_int
     lib.mfgpu_get_info.argtypes = [P, C.POINTER(Info)]
@@ -110,6 +128,8 @@ def load(path=None):
     lib.mfgpu_symbolic_sep.restype = C.c_int
     lib.mfgpu_symbolic_tasks.argtypes = [P, C.c_int, C.POINTER(C.c_void_p)]
     lib.mfgpu_symbolic_tasks.restype = C.c_int64
+    lib.mfgpu_symbolic_dirty.argtypes = [P, C.c_void_p, C.c_int, C.c_void_p, dp]
+    lib.mfgpu_symbolic_dirty.restype = C.c_int64
     lib.mfgpu_symbolic_layout.argtypes = [P, C.c_int, C.c_int, C.POINTER(C.c_int64), i32p]
     lib.mfgpu_symbolic_layout.restype = C.c_int
     _lib = lib
