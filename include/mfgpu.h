@@ -114,6 +114,28 @@ int mfgpu_apply(mfgpu_handle* h, const double* x, double* b, int nrhs, int64_t l
 int mfgpu_solve_device(mfgpu_handle* h, const double* d_b, double* d_x, int nrhs, int64_t ld);
 int mfgpu_apply_device(mfgpu_handle* h, const double* d_x, double* d_b, int nrhs, int64_t ld);
 
+/* Solve with device buffers and no device allocation (no counterpart in the
+ * reference, which is host-only).  mfgpu_solve_device grows its workspace with
+ * cudaMalloc when it first sees a problem or a larger right-hand-side count;
+ * callers that may not allocate at solve time — a service that reserves all
+ * device memory at start-up and must stay inside that budget, or a real-time
+ * loop that cannot take cudaMalloc's implicit device-wide synchronisation —
+ * call this instead.  Its workspace is a fixed 32 MiB array compiled into the
+ * library, present on every GPU that loads it until the process exits.
+ *   - Problems whose workspace for one right-hand side exceeds 32 MiB are
+ *     rejected with MFGPU_ERR_ARG and a message giving the sizes; larger nrhs
+ *     is processed in chunks that fit.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture.
+ *   - Every call, from every handle on the device, shares the array and leaves
+ *     its last contents in it; calls that overlap on the GPU (other streams,
+ *     other threads) race on it and must be serialised by the caller.
+ * d_b and d_x are n x nrhs column-major with leading dimension ld in device
+ * memory; d_x may equal d_b (in-place).  Returns after the solve completes. */
+int mfgpu_solve_device_noalloc(mfgpu_handle* h, const double* d_b, double* d_x, int nrhs,
+                               int64_t ld);
+
 /* Use an external CUDA stream (cudaStream_t) for all later work; NULL restores
  * the handle's own stream. */
 int mfgpu_set_stream(mfgpu_handle* h, void* cuda_stream);

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -419,6 +420,25 @@ struct mfgpu_handle {
     ck(cudaGetLastError(), "solve launch");
   }
 
+  // The same sweeps as solveChunk, with the per-front workspace at W (used
+  // by the no-allocation entry point, which passes its static scratch).
+  void solveChunkScratch(double* X, int64_t ldx, int nrhs, double* W) {
+    const Schedule& s = *S;
+    for (int ell = s.levels - 1; ell >= 1; ell--) {
+      const int f0 = s.lv[ell].front0, s0 = s.lv[ell].sep0;
+      mfgpu::launch_solve_fwd(d_all + f0, s.lv[ell].nbox, d_fr, d_F, d_dofs, X, ldx, nrhs, W,
+                              d_woff, stream);
+      mfgpu::launch_sep_gather(d_all + s.fronts.size() + s0, s.lv[ell].nsep, d_sp, d_dofs, X, ldx,
+                               nrhs, W, d_woff, d_fr, stream);
+    }
+    mfgpu::launch_root_solve(0, d_fr, d_F, d_dofs, X, ldx, nrhs, W, d_woff, stream);
+    for (int ell = 1; ell < s.levels; ell++) {
+      mfgpu::launch_solve_bwd(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, d_F, d_dofs, X, ldx,
+                              nrhs, W, d_woff, stream);
+    }
+    ck(cudaGetLastError(), "solve launch");
+  }
+
   void applyChunk(double* X, int64_t ldx, int nrhs) {
     const Schedule& s = *S;
     for (int ell = s.levels - 1; ell >= 1; ell--)
@@ -743,6 +763,70 @@ int mfgpu_solve_device(mfgpu_handle* h, const double* b, double* x, int nrhs, in
 }
 int mfgpu_apply_device(mfgpu_handle* h, const double* x, double* b, int nrhs, int64_t ld) {
   return solveOrApply(h, x, b, nrhs, ld, true, true);
+}
+
+// ---- solve without any device allocation ----
+//
+// mfgpu_solve_device grows a workspace with cudaMalloc the first time it sees
+// a problem or a larger right-hand-side count.  Callers that may not allocate
+// device memory at solve time (a service that reserves all device memory when
+// it starts and must stay inside that budget, or a real-time loop that cannot
+// afford cudaMalloc's implicit device-wide synchronisation) use this variant:
+// its workspace is a fixed array compiled into the library, 32 MiB on every
+// GPU that loads the library, held until the process exits.
+namespace {
+constexpr size_t kNoAllocScratchDoubles = size_t(4) << 20;   // 32 MiB
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on device `dev`, which must be current.
+// Host code cannot use the array's name as a device pointer, so the address is
+// looked up once per device and cached.
+double* noallocScratch(int dev) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    throw CudaError("device ordinal out of range for the no-allocation scratch", MFGPU_ERR_ARG);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    ck(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(no-allocation scratch)");
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  return g_noalloc_ptr[dev];
+}
+}  // namespace
+
+int mfgpu_solve_device_noalloc(mfgpu_handle* h, const double* d_b, double* d_x, int nrhs,
+                               int64_t ld) {
+  if (!h) return MFGPU_ERR_ARG;
+  const int64_t per_rhs = h->woffTotal;   // workspace doubles one right-hand side needs
+  if (per_rhs > (int64_t)kNoAllocScratchDoubles) {
+    char buf[256];
+    snprintf(buf, sizeof buf,
+             "problem too large for mfgpu_solve_device_noalloc: one right-hand side needs %.1f MiB "
+             "of workspace, the fixed scratch holds %.1f MiB; use mfgpu_solve_device",
+             per_rhs * 8.0 / 1048576.0, kNoAllocScratchDoubles * 8.0 / 1048576.0);
+    return fail(h, MFGPU_ERR_ARG, buf);
+  }
+  if (!h->factored) return fail(h, MFGPU_ERR_STATE, "Solve() before Factor()");
+  if (!d_b || !d_x || nrhs < 0 || ld < h->n) return fail(h, MFGPU_ERR_ARG, "bad vector arguments");
+  if (nrhs == 0) return MFGPU_OK;
+  return guarded(h, [&]() {
+    double* W = noallocScratch(h->device);
+    const int chunk = (int)std::min<int64_t>(16, (int64_t)kNoAllocScratchDoubles / per_rhs);
+    for (int c0 = 0; c0 < nrhs; c0 += chunk) {
+      const int nc = std::min(chunk, nrhs - c0);
+      double* X = d_x + (int64_t)c0 * ld;
+      if (d_x != d_b)
+        for (int c = 0; c < nc; c++)
+          ck(cudaMemcpyAsync(X + (int64_t)c * ld, d_b + (int64_t)(c0 + c) * ld, h->n * sizeof(double),
+                             cudaMemcpyDeviceToDevice, h->stream),
+             "copy rhs");
+      h->solveChunkScratch(X, ld, nc, W);
+    }
+    ck(cudaStreamSynchronize(h->stream), "solve");
+  });
 }
 
 int mfgpu_set_stream(mfgpu_handle* h, void* st) {
