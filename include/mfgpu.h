@@ -152,7 +152,8 @@ enum mfgpu_kernel_class {
   MFGPU_KC_SYRK = 3,      /* trailing symmetric updates (Schur complements)  */
   MFGPU_KC_SOLVE = 4,     /* forward / backward sweeps                       */
   MFGPU_KC_APPLY = 5,     /* factored-operator application                   */
-  MFGPU_KC_COUNT = 6
+  MFGPU_KC_FRONT = 6,     /* fused partial factorization, one CTA per front  */
+  MFGPU_KC_COUNT = 7
 };
 int mfgpu_profile_enable(mfgpu_handle* h, int on);
 int mfgpu_profile_reset(mfgpu_handle* h);

@@ -51,15 +51,29 @@ void launch_trsm(const int* flist, int nf, const FrontDev* fr, double* F, int k,
 void launch_syrk(const int* flist, int nf, const FrontDev* fr, double* F, int k, int max_rows,
                  cudaStream_t st);
 
+// Fused partial factorization of every front in flist, one CTA per front
+// (fronts with n + m <= 640; small_front_fits tells).
+bool small_front_fits(int maxN);
+void launch_front_small(const int* flist, int nf, int maxN, const FrontDev* fr, double* F,
+                        DevError* err, cudaStream_t st);
+
+// Partial factorization of every front in flist (at most 256 fronts) by one
+// cooperative persistent launch over all SMs.
+// `slots` holds coop_slot_doubles() doubles of device scratch.
+bool coop_fits(int nf);
+size_t coop_slot_doubles();
+cudaError_t launch_level_coop(const int* flist, int nf, int maxn, const FrontDev* fr, double* F,
+                              DevError* err, double* slots, cudaStream_t st);
+
 // Number of kernels this library has launched since it was loaded.
 long long launches_total();
 
 // Solve / apply sweeps (nrhs <= 16 per call).  W holds 2*N*nrhs doubles per
 // front at offset woff[f]*nrhs (woff = exclusive prefix of 2*N).
-void launch_solve_fwd(const int* flist, int nf, const FrontDev* fr, const double* F,
+void launch_solve_fwd(const int* flist, int nf, int maxN, const FrontDev* fr, const double* F,
                       const int* dofs, double* X, int64_t ldx, int nrhs, double* W,
                       const int64_t* woff, cudaStream_t st);
-void launch_solve_bwd(const int* flist, int nf, const FrontDev* fr, const double* F,
+void launch_solve_bwd(const int* flist, int nf, int maxN, const FrontDev* fr, const double* F,
                       const int* dofs, double* X, int64_t ldx, int nrhs, double* W,
                       const int64_t* woff, cudaStream_t st);
 void launch_sep_gather(const int* slist, int ns, const SepDev* sp, const int* dofs, double* X,
@@ -71,8 +85,9 @@ void launch_apply_up(const int* flist, int nf, const FrontDev* fr, const double*
 void launch_apply_down(const int* flist, int nf, const FrontDev* fr, const double* F,
                        const int* dofs, int64_t ldx, int nrhs, double* W, const int64_t* woff,
                        const double* T, cudaStream_t st);
-void launch_root_solve(int f, const FrontDev* fr, const double* F, const int* dofs, double* X,
-                       int64_t ldx, int nrhs, double* W, const int64_t* woff, cudaStream_t st);
+void launch_root_solve(int f, int N, const FrontDev* fr, const double* F, const int* dofs,
+                       double* X, int64_t ldx, int nrhs, double* W, const int64_t* woff,
+                       cudaStream_t st);
 void launch_root_apply(int f, const FrontDev* fr, const double* F, const int* dofs, double* X,
                        int64_t ldx, int nrhs, double* W, const int64_t* woff, cudaStream_t st);
 

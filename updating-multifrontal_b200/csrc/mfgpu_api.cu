@@ -150,7 +150,10 @@ struct Profiler {
   struct Mark {
     int cls;
     cudaEvent_t a, b;
+    int level;
   };
+  bool verbose = false;   // MFGPU_VERBOSE=1: one stderr line per launch group
+  int level = -1;         // level tag of the next marks
   std::vector<Mark> marks;
   int64_t launches[MFGPU_KC_COUNT] = {};
   double ms[MFGPU_KC_COUNT] = {};
@@ -167,7 +170,7 @@ struct Profiler {
   }
   void begin(int cls, cudaStream_t st) {
     if (!on) return;
-    Mark m{cls, ev(), nullptr};
+    Mark m{cls, ev(), nullptr, level};
     ck(cudaEventRecord(m.a, st), "profiler record");
     marks.push_back(m);
   }
@@ -182,6 +185,7 @@ struct Profiler {
       if (m.b && cudaEventElapsedTime(&t, m.a, m.b) == cudaSuccess) {
         ms[m.cls] += t;
         launches[m.cls] += 1;
+        if (verbose) fprintf(stderr, "[mfgpu] class %d level %d %.3f ms\n", m.cls, m.level, t);
       }
     }
     marks.clear();
@@ -221,6 +225,7 @@ struct mfgpu_handle {
   SepDev* d_sp = nullptr;
   int64_t* d_woff = nullptr;
   DevError* d_err = nullptr;
+  double* d_slots = nullptr;   // diagonal-block hand-off slots of the cooperative kernel
   double* d_W = nullptr;
   size_t capW = 0;
   double* d_X = nullptr;
@@ -232,6 +237,8 @@ struct mfgpu_handle {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int64_t device_bytes = 0;
   Profiler prof;
+  std::vector<int> lvMaxN;   // largest front (n + m) per level
+  bool stepped = false;      // MFGPU_STEPPED=1: per-step launches instead of the cooperative kernel
 
   ~mfgpu_handle() {
     if (stream) cudaStreamSynchronize(stream);
@@ -247,6 +254,7 @@ struct mfgpu_handle {
     cudaFree(d_sp);
     cudaFree(d_woff);
     cudaFree(d_err);
+    cudaFree(d_slots);
     cudaFree(d_W);
     cudaFree(d_X);
     cudaFree(d_T);
@@ -302,6 +310,7 @@ struct mfgpu_handle {
     prof.begin(MFGPU_KC_ASSEMBLE, stream);
     mfgpu::launch_tasks(P.d_tasks + g.task0, P.d_pref + g.pref0, (int)g.ntasks, g.ntiles, d_F, d_Sep,
                         d_rp, d_ci, d_val, d_dofs, stream);
+    ck(cudaGetLastError(), "launch assembly (k_tasks)");
     prof.end(stream);
     if (prof.on) prof.bytes[MFGPU_KC_ASSEMBLE] += (double)bytes;
   }
@@ -327,9 +336,27 @@ struct mfgpu_handle {
     ck(cudaMemsetAsync(d_err, 0, sizeof(DevError), stream), "clear error word");
     for (int ell = s.levels - 1; ell >= 0; ell--) {
       const Plan::Level& L = P.lv[ell];
+      prof.level = ell;
       runGroup(P, L.sbase, groupBytes(P, L.sbase));
       runGroup(P, L.ftask, groupBytes(P, L.ftask));
-      if (L.nf > 0) {
+      if (L.nf > 0 && mfgpu::small_front_fits(L.maxN)) {
+        if (prof.on)
+          for (int64_t i = L.f0; i < L.f0 + L.nf; i++)
+            prof.flops[MFGPU_KC_FRONT] += s.front_flops(s.fronts[P.ids[i]]);
+        prof.begin(MFGPU_KC_FRONT, stream);
+        mfgpu::launch_front_small(P.d_ids + L.f0, (int)L.nf, L.maxN, d_fr, d_F, d_err, stream);
+        ck(cudaGetLastError(), "launch fused front factorization (k_front_small)");
+        prof.end(stream);
+      } else if (L.nf > 0 && mfgpu::coop_fits((int)L.nf) && !stepped) {
+        if (prof.on)
+          for (int64_t i = L.f0; i < L.f0 + L.nf; i++)
+            prof.flops[MFGPU_KC_FRONT] += s.front_flops(s.fronts[P.ids[i]]);
+        prof.begin(MFGPU_KC_FRONT, stream);
+        ck(mfgpu::launch_level_coop(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, d_F, d_err, d_slots,
+                                    stream),
+           "launch cooperative level factorization (k_level_coop)");
+        prof.end(stream);
+      } else if (L.nf > 0) {
         const int* fl = P.d_ids + L.f0;
         for (int k = 0; k < L.maxn; k += mfgpu::kPanel) {
           if (prof.on) {
@@ -344,12 +371,15 @@ struct mfgpu_handle {
           }
           prof.begin(MFGPU_KC_POTRF, stream);
           mfgpu::launch_potrf(fl, (int)L.nf, d_fr, d_F, k, d_err, stream);
+          ck(cudaGetLastError(), "launch panel Cholesky (k_potrf)");
           prof.end(stream);
           prof.begin(MFGPU_KC_TRSM, stream);
           mfgpu::launch_trsm(fl, (int)L.nf, d_fr, d_F, k, L.maxN, stream);
+          ck(cudaGetLastError(), "launch panel solve (k_trsm)");
           prof.end(stream);
           prof.begin(MFGPU_KC_SYRK, stream);
           mfgpu::launch_syrk(fl, (int)L.nf, d_fr, d_F, k, L.maxN, stream);
+          ck(cudaGetLastError(), "launch trailing update (k_syrk)");
           prof.end(stream);
         }
       }
@@ -403,19 +433,40 @@ struct mfgpu_handle {
   }
 
   // Solve in place on device data X (n x nrhs, ld = ldx), nrhs <= 16.
+  // MFGPU_VERBOSE: per-level marks inside the solve (class SOLVE, level tag).
+  void vmark(bool begin, int level) {
+    if (!prof.verbose) return;
+    if (begin) {
+      prof.level = level;
+      prof.begin(MFGPU_KC_SOLVE, stream);
+    } else {
+      prof.end(stream);
+    }
+  }
+
   void solveChunk(double* X, int64_t ldx, int nrhs) {
     const Schedule& s = *S;
     for (int ell = s.levels - 1; ell >= 1; ell--) {
       const int f0 = s.lv[ell].front0, s0 = s.lv[ell].sep0;
-      mfgpu::launch_solve_fwd(d_all + f0, s.lv[ell].nbox, d_fr, d_F, d_dofs, X, ldx, nrhs, d_W,
+      vmark(true, ell);
+      mfgpu::launch_solve_fwd(d_all + f0, s.lv[ell].nbox, lvMaxN[ell], d_fr, d_F, d_dofs, X, ldx, nrhs, d_W,
                               d_woff, stream);
+      vmark(false, ell);
+      ck(cudaGetLastError(), "launch forward sweep (k_solve_fwd)");
       mfgpu::launch_sep_gather(d_all + s.fronts.size() + s0, s.lv[ell].nsep, d_sp, d_dofs, X, ldx,
                                nrhs, d_W, d_woff, d_fr, stream);
+      ck(cudaGetLastError(), "launch separator gather (k_sep_gather)");
     }
-    mfgpu::launch_root_solve(0, d_fr, d_F, d_dofs, X, ldx, nrhs, d_W, d_woff, stream);
+    vmark(true, 0);
+    mfgpu::launch_root_solve(0, s.fronts[0].N, d_fr, d_F, d_dofs, X, ldx, nrhs, d_W, d_woff, stream);
+    vmark(false, 0);
+    ck(cudaGetLastError(), "launch root solve (k_root_solve)");
     for (int ell = 1; ell < s.levels; ell++) {
-      mfgpu::launch_solve_bwd(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, d_F, d_dofs, X, ldx,
+      vmark(true, 100 + ell);
+      mfgpu::launch_solve_bwd(d_all + s.lv[ell].front0, s.lv[ell].nbox, lvMaxN[ell], d_fr, d_F, d_dofs, X, ldx,
                               nrhs, d_W, d_woff, stream);
+      vmark(false, 100 + ell);
+      ck(cudaGetLastError(), "launch backward sweep (k_solve_bwd)");
     }
     ck(cudaGetLastError(), "solve launch");
   }
@@ -426,15 +477,19 @@ struct mfgpu_handle {
     const Schedule& s = *S;
     for (int ell = s.levels - 1; ell >= 1; ell--) {
       const int f0 = s.lv[ell].front0, s0 = s.lv[ell].sep0;
-      mfgpu::launch_solve_fwd(d_all + f0, s.lv[ell].nbox, d_fr, d_F, d_dofs, X, ldx, nrhs, W,
+      mfgpu::launch_solve_fwd(d_all + f0, s.lv[ell].nbox, lvMaxN[ell], d_fr, d_F, d_dofs, X, ldx, nrhs, W,
                               d_woff, stream);
+      ck(cudaGetLastError(), "launch forward sweep (k_solve_fwd)");
       mfgpu::launch_sep_gather(d_all + s.fronts.size() + s0, s.lv[ell].nsep, d_sp, d_dofs, X, ldx,
                                nrhs, W, d_woff, d_fr, stream);
+      ck(cudaGetLastError(), "launch separator gather (k_sep_gather)");
     }
-    mfgpu::launch_root_solve(0, d_fr, d_F, d_dofs, X, ldx, nrhs, W, d_woff, stream);
+    mfgpu::launch_root_solve(0, s.fronts[0].N, d_fr, d_F, d_dofs, X, ldx, nrhs, W, d_woff, stream);
+    ck(cudaGetLastError(), "launch root solve (k_root_solve)");
     for (int ell = 1; ell < s.levels; ell++) {
-      mfgpu::launch_solve_bwd(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, d_F, d_dofs, X, ldx,
+      mfgpu::launch_solve_bwd(d_all + s.lv[ell].front0, s.lv[ell].nbox, lvMaxN[ell], d_fr, d_F, d_dofs, X, ldx,
                               nrhs, W, d_woff, stream);
+      ck(cudaGetLastError(), "launch backward sweep (k_solve_bwd)");
     }
     ck(cudaGetLastError(), "solve launch");
   }
@@ -444,12 +499,16 @@ struct mfgpu_handle {
     for (int ell = s.levels - 1; ell >= 1; ell--)
       mfgpu::launch_apply_up(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, d_F, d_dofs, X, ldx,
                              nrhs, d_W, d_woff, d_T, stream);
+      ck(cudaGetLastError(), "launch apply up (k_apply_up)");
     mfgpu::launch_root_apply(0, d_fr, d_F, d_dofs, X, ldx, nrhs, d_W, d_woff, stream);
+    ck(cudaGetLastError(), "launch root apply (k_root_apply)");
     for (int ell = 1; ell < s.levels; ell++) {
       mfgpu::launch_apply_down(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, d_F, d_dofs, ldx,
                                nrhs, d_W, d_woff, d_T, stream);
+      ck(cudaGetLastError(), "launch apply down (k_apply_down)");
       mfgpu::launch_sep_gather(d_all + s.fronts.size() + s.lv[ell].sep0, s.lv[ell].nsep, d_sp, d_dofs,
                                X, ldx, nrhs, d_W, d_woff, d_fr, stream);
+      ck(cudaGetLastError(), "launch separator gather (k_sep_gather)");
     }
     ck(cudaGetLastError(), "apply launch");
   }
@@ -549,6 +608,8 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n
   }
   h->n = n;
   h->nnz = row_ptr[n];
+  if (const char* e = getenv("MFGPU_STEPPED")) h->stepped = e[0] == '1';
+  if (const char* e = getenv("MFGPU_VERBOSE")) h->prof.verbose = e[0] == '1';
   h->h_rowptr.assign(row_ptr, row_ptr + n + 1);
   h->h_colind.assign(col_ind, col_ind + h->nnz);
   int st = guarded(h.get(), [&]() {
@@ -571,6 +632,8 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n
       woff[i + 1] = woff[i] + 2 * (int64_t)f.N;
     }
     H.woffTotal = woff.back();
+    H.lvMaxN.assign(s.levels, 0);
+    for (const mfgpu::Front& f : s.fronts) H.lvMaxN[f.level] = std::max(H.lvMaxN[f.level], f.N);
     std::vector<SepDev> sp(s.seps.size());
     for (size_t i = 0; i < s.seps.size(); i++) {
       const mfgpu::Sep& e = s.seps[i];
@@ -583,6 +646,7 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n
     H.d_sp = dalloc<SepDev>(std::max<size_t>(1, sp.size()), "alloc seps");
     H.d_woff = dalloc<int64_t>(woff.size(), "alloc woff");
     H.d_err = dalloc<DevError>(1, "alloc error word");
+    H.d_slots = dalloc<double>(mfgpu::coop_slot_doubles(), "alloc diagonal slots");
     H.d_all = dalloc<int>(all.size(), "alloc id list");
     ck(cudaMemcpy(H.d_val, val, H.nnz * sizeof(double), cudaMemcpyHostToDevice), "upload val");
     ck(cudaMemcpy(H.d_rp, row_ptr, (n + 1) * sizeof(int), cudaMemcpyHostToDevice), "upload rows");
@@ -717,10 +781,10 @@ static int solveOrApply(mfgpu_handle* h, const double* in, double* out, int nrhs
         ck(cudaMemcpyAsync(X + (int64_t)c * h->n, in + (int64_t)(c0 + c) * ld, h->n * sizeof(double),
                            device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream),
            "copy rhs in");
-      h->prof.begin(apply ? MFGPU_KC_APPLY : MFGPU_KC_SOLVE, h->stream);
+      if (!h->prof.verbose) h->prof.begin(apply ? MFGPU_KC_APPLY : MFGPU_KC_SOLVE, h->stream);
       if (apply) h->applyChunk(X, h->n, nc);
       else h->solveChunk(X, h->n, nc);
-      h->prof.end(h->stream);
+      if (!h->prof.verbose) h->prof.end(h->stream);
       if (h->prof.on) {
         // L11 (lower) and L21 are read once forward and once backward; the
         // right-hand sides are gathered and scattered per front.
