@@ -271,12 +271,18 @@ int runTiming(const Input& in, SMat& M1, SMat& M2, MF* F) {
 
 int main(int argc, char** argv) {
   if (argc < 4) {
-    fprintf(stderr, "usage: %s dump|time input.bin output.bin\n", argv[0]);
+    fprintf(stderr, "usage: %s dump|time|csr input.bin output.bin\n", argv[0]);
     return 2;
   }
   std::string mode = argv[1];
   Input in = readInput(argv[2]);
   try {
+    if (mode == "csr") {   // only the fixture's CSR (buildLaplacian.hpp), no factorization
+      SMat M1 = in.dim == 2 ? build2(in, in.coef1) : build3(in, in.coef1);
+      Writer w(argv[3]);
+      dumpCSR(w, "A1.", M1);
+      return 0;
+    }
     if (in.dim == 2) {
       SMat M1 = build2(in, in.coef1);
       SMat M2 = in.doUpdate ? build2(in, in.coef2) : M1;

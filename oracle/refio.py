@@ -93,6 +93,16 @@ def run_reference(workdir, dim, N, width, max_side, coef1, coef2=None, rhs=None,
     return read_records(outp)
 
 
+def reference_csr(workdir, dim, N, width, coef, h=(1.0, 1.0, 1.0)):
+    """CSR built by the reference fixture only (test_include/DE/buildLaplacian.hpp)."""
+    os.makedirs(workdir, exist_ok=True)
+    inp = os.path.join(workdir, "csr_in.bin")
+    outp = os.path.join(workdir, "csr_out.bin")
+    write_input(inp, dim, N, width, 1, coef, None, None, h, 0, 0)
+    subprocess.run([REF_BIN, "csr", inp, outp], check=True, timeout=600)
+    return read_records(outp)
+
+
 def time_reference(workdir, dim, N, width, max_side, coef1, coef2=None, rhs=None,
                    h=(1.0, 1.0, 1.0), reps=1, solve_reps=1, threads=None, timeout=3600):
     """Time the reference's Factor / Update / Solve; returns the parsed JSON."""

@@ -17,5 +17,9 @@ def pytest_configure(config):
 
 @pytest.fixture(scope="session")
 def lib():
+    """libmfgpu.so, built in-tree (nvcc cross-compiles without a GPU) if missing."""
+    import subprocess
     from mfgpu import _lib
+    if not os.path.isfile(_lib.LIB_PATH):
+        subprocess.run(["make", "-j", "8"], cwd=PKG, check=True, capture_output=True)
     return _lib.load()

@@ -32,7 +32,7 @@ def make(dim, N, A, ms, **kw):
 
 
 @pytest.mark.parametrize("dim,N,ms", CASES)
-def test_factor_solve_apply_vs_oracle(dim, N, ms):
+def test_factor_solve_apply_vs_oracle(dim, N, ms, lib):
     a, A, b = problem(dim, N, seed=11, nrhs=3)
     O = mf_oracle.MFOracle(A.to_scipy(), N, 1, ms)
     O.factor()
