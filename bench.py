@@ -121,11 +121,12 @@ class ClockSampler:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
 
 
-def measured_fp64_peak(torch):
-    """cuBLAS DGEMM throughput (torch float64 matmul, 8192^3), best of 5, TFLOP/s."""
+def measured_gemm_peak(torch, dtype):
+    """cuBLAS GEMM throughput (torch matmul, 8192^3, TF32 off), best of 5, TFLOP/s."""
     n = 8192
-    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
-    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(n, n, dtype=dtype, device="cuda")
+    b = torch.randn(n, n, dtype=dtype, device="cuda")
     torch.matmul(a, b)
     torch.cuda.synchronize()
     best = 0.0
@@ -206,7 +207,8 @@ def run_reference_arm(args, w):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s",
         "n_gpus": args.gpus, "steps": len(steps), "warmup": 1, "ms_per_step": t * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32 factor + f64 refinement",
         "data": "synthetic (seeded coefficients and right-hand sides)",
         "config": config_of(w, args),
         "phases_s": {"factor_p50": statistics.median(tf), "update_p50": statistics.median(tu),
@@ -247,7 +249,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="2d-1023", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--json-out", default=None)
     args = ap.parse_args()
@@ -258,8 +260,9 @@ def main():
     import torch
     import torch.distributed as dist
 
-    from mfgpu import MF2D, MF3D
+    from mfgpu import MF2D, MF3D, MFGPU_FP64, MFGPU_MIXED
 
+    prec = MFGPU_MIXED if args.precision == "mixed" else MFGPU_FP64
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -270,9 +273,10 @@ def main():
     a1, a2, A1, A2, mod, b = make_problem(w, rank)
     n, nnz, nrhs = A1.n, A1.nnz, w["nrhs"]
     if w["dim"] == 2:
-        F = MF2D(A1, w["N"][0], w["N"][1], 1, w["max_side"], device=local)
+        F = MF2D(A1, w["N"][0], w["N"][1], 1, w["max_side"], device=local, precision=prec)
     else:
-        F = MF3D(A1, w["N"][0], w["N"][1], w["N"][2], 1, w["max_side"], device=local)
+        F = MF3D(A1, w["N"][0], w["N"][1], w["N"][2], 1, w["max_side"], device=local,
+                 precision=prec)
     stream = torch.cuda.Stream()
     F.set_stream(stream.cuda_stream)
     dv1 = torch.from_numpy(A1.val).to("cuda")
@@ -371,13 +375,16 @@ def main():
     P = prof[dom]
     roof = None
     if rank == 0:
-        if dom in ("potrf", "trsm", "syrk"):
-            fp64 = measured_fp64_peak(torch)
+        if dom in ("potrf", "trsm", "syrk", "front"):
+            dt, nm = (torch.float32, "SGEMM (float32") if args.precision == "mixed" else \
+                (torch.float64, "DGEMM (float64")
+            pk = measured_gemm_peak(torch, dt)
             ach = P["flops"] / (P["ms"] * 1e-3) / 1e12
-            roof = {"bound": "tensor", "kernel": dom, "achieved": ach, "peak": fp64,
-                    "unit": "TFLOP/s", "frac": ach / fp64, "traffic": traffic_for(dom),
-                    "peak_source": "measured cuBLAS DGEMM (torch float64 matmul 8192^3) on this "
-                                   "GPU; FP64 has no entry in MEASURED_PEAKS.json",
+            roof = {"bound": "tensor", "kernel": dom, "achieved": ach, "peak": pk,
+                    "unit": "TFLOP/s", "frac": ach / pk, "traffic": traffic_for(dom),
+                    "peak_source": f"measured cuBLAS {nm} matmul 8192^3, TF32 off) on this "
+                                   "GPU; the factor's precision has no entry in "
+                                   "MEASURED_PEAKS.json",
                     "launches": P["launches"], "avg_launch_ms": P["ms"] / max(1, P["launches"])}
         else:
             ach = P["bytes"] / (P["ms"] * 1e-3) / 1e9
@@ -403,12 +410,14 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32 factor + f64 refinement",
             "data": "synthetic (seeded coefficients and right-hand sides)",
             "config": config_of(w, args),
             "step_ms_p50": statistics.median(step_ms),
             "step_ms_p99": float(np.percentile(step_ms, 99)),
             "resid": resid,
+            "refine_iterations": F.stats()["iterations"] if args.precision == "mixed" else 0,
             "flops_per_step": {"factor": info["factor_flops"], "update": upd_fl,
                                "solve": solve_flops(fl, nrhs)},
             "kernel_classes": {k: {"launches": v["launches"], "ms": v["ms"]} for k, v in prof.items()},

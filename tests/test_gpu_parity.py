@@ -122,3 +122,33 @@ def test_errors():
     # the handle stays usable: a good factorization on the same process works
     F.Factor()
     assert rel(A.matvec(F.Solve(b[0])), b[0]) < 1e-13
+
+
+@pytest.fixture
+def env_var(monkeypatch):
+    """Set an MFGPU_* switch for the handles created inside the test."""
+    def set_(name, value):
+        monkeypatch.setenv(name, str(value))
+    return set_
+
+
+@pytest.mark.parametrize("dim,N,ms", [(2, (127, 127), 4), (2, (130, 70), 4), (3, (15, 15, 15), 4),
+                                      (3, (13, 17, 11), 3), (3, (31, 31, 31), 4)])
+@pytest.mark.parametrize("nrhs", [1, 3, 9])
+def test_cooperative_sweeps_vs_oracle(dim, N, ms, nrhs, env_var):
+    # every level of at most 256 fronts through the multi-CTA blocked sweeps
+    env_var("MFGPU_SOLVE_COOP_MIN_N", 1)
+    a, A, b = problem(dim, N, seed=13, nrhs=nrhs)
+    F = make(dim, N, A, ms)
+    F.Factor()
+    X = F.Solve(b.T)
+    O = mf_oracle.MFOracle(A.to_scipy(), N, 1, ms)
+    O.factor()
+    for r in range(nrhs):
+        assert rel(X[:, r], O.solve(b[r])) < 1e-12
+    env_var("MFGPU_SOLVE_COOP_MIN_N", 0)
+    G = make(dim, N, A, ms)
+    G.Factor()
+    Xg = G.Solve(b.T)
+    assert rel(X, Xg) < 1e-13
+    assert np.array_equal(F.Solve(b.T), X)      # deterministic

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <vector>
 
 #include "schedule.hpp"
 
@@ -36,14 +37,17 @@ struct DevError {
 constexpr int kTaskTile = 32;   // assembly tile edge
 constexpr int kPanel = 32;      // panel width of the partial Cholesky
 
-// Assembly tasks: tstart has ntasks+1 exclusive prefix sums of tile counts.
-void launch_tasks(const Task* tasks, const int64_t* tstart, int ntasks, int64_t ntiles,
-                  double* fronts, double* seps, const int* rp, const int* ci, const double* va,
-                  const int* dofs, cudaStream_t st);
+// Kernel launch wrappers.  T = double (FP64 path) or float (mixed path).
 
-// One panel step k of the partial Cholesky for every front in flist: the
-// diagonal block factorization, the triangular solve of the rows below it
-// (max_rows bounds N - k over the list) and the trailing symmetric update.
+// Assembly tasks: tstart has ntasks+1 exclusive prefix sums of tile counts.
+// `scale` (may be null) multiplies sparse entries a_rc by scale[r] * scale[c].
+template <class T>
+void launch_tasks(const Task* tasks, const int64_t* tstart, int ntasks, int64_t ntiles, T* fronts,
+                  T* seps, const int* rp, const int* ci, const double* va, const int* dofs,
+                  const double* scale, cudaStream_t st);
+
+// Stepped FP64 path (one launch per panel step and kernel), kept for levels a
+// cooperative launch cannot take.
 void launch_potrf(const int* flist, int nf, const FrontDev* fr, double* F, int k, DevError* err,
                   cudaStream_t st);
 void launch_trsm(const int* flist, int nf, const FrontDev* fr, double* F, int k, int max_rows,
@@ -51,44 +55,97 @@ void launch_trsm(const int* flist, int nf, const FrontDev* fr, double* F, int k,
 void launch_syrk(const int* flist, int nf, const FrontDev* fr, double* F, int k, int max_rows,
                  cudaStream_t st);
 
-// Fused partial factorization of every front in flist, one CTA per front
-// (fronts with n + m <= 640; small_front_fits tells).
-bool small_front_fits(int maxN);
-void launch_front_small(const int* flist, int nf, int maxN, const FrontDev* fr, double* F,
-                        DevError* err, cudaStream_t st);
+// Fused partial factorization, one CTA per front, for levels whose widest
+// front's staged panel fits in shared memory.
+bool small_front_fits(int maxN, int elem_bytes);
+template <class T>
+void launch_front_small(const int* flist, int nf, int maxN, const FrontDev* fr, T* F, DevError* err,
+                        cudaStream_t st);
 
-// Partial factorization of every front in flist (at most 256 fronts) by one
-// cooperative persistent launch over all SMs.
-// `slots` holds coop_slot_doubles() doubles of device scratch.
+// Partial factorization of every front in flist by one cooperative persistent
+// launch over all SMs.  `slots` holds coop_slot_elems() elements of scratch;
+// `phase_pref` the per-phase work-item prefixes from coop_phase_prefix.
 bool coop_fits(int nf);
-size_t coop_slot_doubles();
-cudaError_t launch_level_coop(const int* flist, int nf, int maxn, const FrontDev* fr, double* F,
-                              DevError* err, double* slots, cudaStream_t st);
+size_t coop_slot_elems();
+std::vector<int> coop_phase_prefix(const std::vector<int>& n, const std::vector<int>& N, int maxn);
+// K0/K1/phase0/trailing restrict the launch to the outer panels [K0, K1)
+// (K1 < 0: to the end) and optionally leave the last trailing update out.
+template <class T>
+cudaError_t launch_level_coop(const int* flist, int nf, int maxn, const FrontDev* fr, T* F,
+                              DevError* err, T* slots, const int* phase_pref, cudaStream_t st,
+                              int K0 = 0, int K1 = -1, int phase0 = 0, int trailing = 1);
+int coop_outer();                   // outer panel width of the cooperative kernel
+int coop_phases(int K, int maxn);   // phases of outer panel K in the prefix table
+
+// Tensor-core (tcgen05, TF32) trailing update of the mixed path after outer
+// panel K of every front in flist: C(k1:N, k1:N) -= P P^T with P the panel's
+// columns, split = 1 (TF32) or 3 (hi/lo three-term TF32, about FP32 accuracy).
+int tc_outer();
+int tc_max_fronts();
+int64_t tc_tiles(const std::vector<int>& n, const std::vector<int>& N, int K);
+cudaError_t launch_trail_tc(const int* flist, int nf, int64_t ntiles, const FrontDev* fr, float* F,
+                            int K, int split, DevError* err, cudaStream_t st);
+
+// Cooperative sweeps over all fronts of one level (at most
+// solve_coop_max_fronts() fronts, nrhs <= 16): forward = gather, L11 solve
+// and boundary update; backward = gather, L21^T update and L11^T solve.
+int solve_coop_max_fronts();
+template <class T>
+cudaError_t launch_solve_coop(bool forward, const int* flist, int nf, int maxn, const FrontDev* fr,
+                              const T* F, const int* dofs, T* X, int64_t ldx, int nrhs, T* W,
+                              const int64_t* woff, cudaStream_t st);
 
 // Number of kernels this library has launched since it was loaded.
 long long launches_total();
 
-// Solve / apply sweeps (nrhs <= 16 per call).  W holds 2*N*nrhs doubles per
+// Solve / apply sweeps (nrhs <= 16 per call).  W holds 2*N*nrhs elements per
 // front at offset woff[f]*nrhs (woff = exclusive prefix of 2*N).
-void launch_solve_fwd(const int* flist, int nf, int maxN, const FrontDev* fr, const double* F,
-                      const int* dofs, double* X, int64_t ldx, int nrhs, double* W,
-                      const int64_t* woff, cudaStream_t st);
-void launch_solve_bwd(const int* flist, int nf, int maxN, const FrontDev* fr, const double* F,
-                      const int* dofs, double* X, int64_t ldx, int nrhs, double* W,
-                      const int64_t* woff, cudaStream_t st);
-void launch_sep_gather(const int* slist, int ns, const SepDev* sp, const int* dofs, double* X,
-                       int64_t ldx, int nrhs, const double* W, const int64_t* woff,
-                       const FrontDev* fr, cudaStream_t st);
-void launch_apply_up(const int* flist, int nf, const FrontDev* fr, const double* F,
-                     const int* dofs, double* X, int64_t ldx, int nrhs, double* W,
-                     const int64_t* woff, double* T, cudaStream_t st);
-void launch_apply_down(const int* flist, int nf, const FrontDev* fr, const double* F,
-                       const int* dofs, int64_t ldx, int nrhs, double* W, const int64_t* woff,
-                       const double* T, cudaStream_t st);
-void launch_root_solve(int f, int N, const FrontDev* fr, const double* F, const int* dofs,
-                       double* X, int64_t ldx, int nrhs, double* W, const int64_t* woff,
+template <class T>
+void launch_solve_fwd(const int* flist, int nf, int maxN, const FrontDev* fr, const T* F,
+                      const int* dofs, T* X, int64_t ldx, int nrhs, T* W, const int64_t* woff,
+                      cudaStream_t st);
+template <class T>
+void launch_solve_bwd(const int* flist, int nf, int maxN, const FrontDev* fr, const T* F,
+                      const int* dofs, T* X, int64_t ldx, int nrhs, T* W, const int64_t* woff,
+                      cudaStream_t st);
+template <class T>
+void launch_root_solve(int f, int N, const FrontDev* fr, const T* F, const int* dofs, T* X,
+                       int64_t ldx, int nrhs, T* W, const int64_t* woff, cudaStream_t st);
+template <class T>
+void launch_sep_gather(const int* slist, int ns, const SepDev* sp, const int* dofs, T* X,
+                       int64_t ldx, int nrhs, const T* W, const int64_t* woff, const FrontDev* fr,
                        cudaStream_t st);
-void launch_root_apply(int f, const FrontDev* fr, const double* F, const int* dofs, double* X,
-                       int64_t ldx, int nrhs, double* W, const int64_t* woff, cudaStream_t st);
+template <class T>
+void launch_apply_up(const int* flist, int nf, const FrontDev* fr, const T* F, const int* dofs, T* X,
+                     int64_t ldx, int nrhs, T* W, const int64_t* woff, T* Tb, cudaStream_t st);
+template <class T>
+void launch_apply_down(const int* flist, int nf, const FrontDev* fr, const T* F, const int* dofs,
+                       int64_t ldx, int nrhs, T* W, const int64_t* woff, const T* Tb,
+                       cudaStream_t st);
+template <class T>
+void launch_root_apply(int f, const FrontDev* fr, const T* F, const int* dofs, T* X, int64_t ldx,
+                       int nrhs, T* W, const int64_t* woff, cudaStream_t st);
+
+// Vector kernels of the mixed-precision solve (kernels_vec.cu).
+void launch_diag_scale(const int* rp, const int* ci, const double* va, int n, double* s,
+                       double* is, cudaStream_t st);
+void launch_spmv(const int* rp, const int* ci, const double* va, int n, const double* x, int64_t ldx,
+                 double* y, int64_t ldy, int nrhs, cudaStream_t st);
+void launch_residual(const int* rp, const int* ci, const double* va, int n, const double* b,
+                     int64_t ldb, const double* x, int64_t ldx, double* r, int64_t ldr, int nrhs,
+                     cudaStream_t st);
+size_t dot_scratch_elems(int nrhs);
+void launch_dot(const double* x, int64_t ldx, const double* y, int64_t ldy, int n, int nrhs,
+                double* part, double* out, cudaStream_t st);
+template <class T>
+void launch_scale_to(const double* src, int64_t lds, T* dst, int64_t ldd, const double* s, int n,
+                     int nrhs, cudaStream_t st);
+template <class T>
+void launch_scale_from(const T* src, int64_t lds, double* dst, int64_t ldd, const double* s, int n,
+                       int nrhs, cudaStream_t st);
+void launch_pcg_xr(double* x, double* r, const double* p, const double* q, int64_t ld, int n,
+                   int nrhs, const double* rz, const double* pq, const int* active, cudaStream_t st);
+void launch_pcg_p(double* p, const double* z, int64_t ld, int n, int nrhs, const double* rz_new,
+                  const double* rz_old, const int* active, int first, cudaStream_t st);
 
 }  // namespace mfgpu

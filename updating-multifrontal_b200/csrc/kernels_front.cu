@@ -1,5 +1,9 @@
-// FP64 kernels: front / separator assembly from task tables, panel-stepped
-// partial Cholesky of every front of a level, and the solve / apply sweeps.
+// Front kernels for both precisions (T = double for the FP64 path, T = float
+// for the mixed-precision factorization): front / separator assembly from
+// task tables, partial Cholesky of every front of a level (fused per front, or
+// one cooperative launch per level), and the solve / apply sweeps.  FP64 tiles
+// use the FP64 tensor cores (mma.sync m8n8k4); FP32 tiles use CUDA-core FMAs
+// with the same fragment layout.
 //
 // Fronts are column-major with leading dimension ld; only the lower triangle
 // is read or written.  After the partial factorization of a front with n
@@ -11,8 +15,10 @@
 //                            A11 + S elsewhere (the reference's A11post).
 #include <cooperative_groups.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
+#include <vector>
 
 #include "device.cuh"
 
@@ -34,14 +40,16 @@ __device__ __forceinline__ double sparse_at(const int* __restrict__ rp, const in
   return v;
 }
 
+template <class T>
 __global__ void __launch_bounds__(256) k_tasks(const Task* __restrict__ tasks,
                                                const int64_t* __restrict__ tstart, int ntasks,
-                                               double* __restrict__ F, double* __restrict__ SA,
+                                               T* __restrict__ F, T* __restrict__ SA,
                                                const int* __restrict__ rp,
                                                const int* __restrict__ ci,
                                                const double* __restrict__ va,
-                                               const int* __restrict__ dofs) {
-  __shared__ double sm[kTaskTile][kTaskTile + 1];
+                                               const int* __restrict__ dofs,
+                                               const double* __restrict__ scale) {
+  __shared__ T sm[kTaskTile][kTaskTile + 1];
   __shared__ int s_task;
   const int64_t tile = (int64_t)blockIdx.x + (int64_t)blockIdx.y * gridDim.x;
   if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -55,41 +63,47 @@ __global__ void __launch_bounds__(256) k_tasks(const Task* __restrict__ tasks,
   }
   __syncthreads();
   if (tile >= tstart[ntasks]) return;
-  const Task T = tasks[s_task];
+  const Task Tk = tasks[s_task];
   const int64_t local = tile - tstart[s_task];
-  const int tr = (T.rows + kTaskTile - 1) / kTaskTile;
+  const int tr = (Tk.rows + kTaskTile - 1) / kTaskTile;
   const int i0 = (int)(local % tr) * kTaskTile;
   const int j0 = (int)(local / tr) * kTaskTile;
-  if (T.lower && i0 + kTaskTile - 1 < j0) return;
-  double* dst = (T.dst_arena == AR_FRONT ? F : SA) + T.dst_off;
-  const double* src = (T.src_arena == AR_FRONT ? F : SA) + T.src_off;
+  if (Tk.lower && i0 + kTaskTile - 1 < j0) return;
+  T* dst = (Tk.dst_arena == AR_FRONT ? F : SA) + Tk.dst_off;
+  const T* src = (Tk.src_arena == AR_FRONT ? F : SA) + Tk.src_off;
   const int tx = threadIdx.x, ty = threadIdx.y;
-  if (T.kind == TK_COPY && T.trans) {
+  if (Tk.kind == TK_COPY && Tk.trans) {
     // dst(i, j) = src[j + i*ld]: stage through shared memory so both sides coalesce
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       int ii = i0 + ty + 8 * q, jj = j0 + tx;
-      if (ii < T.rows && jj < T.cols) sm[ty + 8 * q][tx] = src[jj + (int64_t)ii * T.src_ld];
+      if (ii < Tk.rows && jj < Tk.cols) sm[ty + 8 * q][tx] = src[jj + (int64_t)ii * Tk.src_ld];
     }
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       int i = i0 + tx, j = j0 + ty + 8 * q;
-      if (i < T.rows && j < T.cols && (!T.lower || i >= j))
-        dst[i + (int64_t)j * T.dst_ld] = sm[tx][ty + 8 * q];
+      if (i < Tk.rows && j < Tk.cols && (!Tk.lower || i >= j))
+        dst[i + (int64_t)j * Tk.dst_ld] = sm[tx][ty + 8 * q];
     }
     return;
   }
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const int i = i0 + tx, j = j0 + ty + 8 * q;
-    if (i >= T.rows || j >= T.cols || (T.lower && i < j)) continue;
-    double* d = dst + i + (int64_t)j * T.dst_ld;
-    switch (T.kind) {
-      case TK_ZERO: *d = 0.0; break;
-      case TK_COPY: *d = src[i + (int64_t)j * T.src_ld]; break;
-      case TK_ADD: *d = *d + src[i + (int64_t)j * T.src_ld]; break;
-      case TK_SPARSE: *d = sparse_at(rp, ci, va, dofs[T.row_dof + i], dofs[T.col_dof + j]); break;
+    if (i >= Tk.rows || j >= Tk.cols || (Tk.lower && i < j)) continue;
+    T* d = dst + i + (int64_t)j * Tk.dst_ld;
+    switch (Tk.kind) {
+      case TK_ZERO: *d = T(0); break;
+      case TK_COPY: *d = src[i + (int64_t)j * Tk.src_ld]; break;
+      case TK_ADD: *d = *d + src[i + (int64_t)j * Tk.src_ld]; break;
+      case TK_SPARSE: {
+        const int r = dofs[Tk.row_dof + i], c = dofs[Tk.col_dof + j];
+        double v = sparse_at(rp, ci, va, r, c);
+        if (scale) v = v * scale[r] * scale[c];   // symmetric diagonal scaling
+        *d = (T)v;
+        break;
+      }
     }
   }
 }
@@ -166,34 +180,38 @@ __device__ __forceinline__ void warp_factor_diag(double* A, int64_t ld, int k, i
 // short.  On exit A and Ls hold L, Li holds L^{-1} (lower, stride kLi) and
 // Dinv the reciprocals of the diagonal.  Called by one full warp.
 constexpr int kLi = 36;
-__device__ void warp_factor_inv(double* A, int64_t ld, int k, int kb, double (*Ls)[kPanel + 1],
-                                double* Li, double* Dinv, DevError* err, int f) {
+__device__ __forceinline__ double rsq(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
+
+template <class T>
+__device__ void warp_factor_inv(T* A, int64_t ld, int k, int kb, T (*Ls)[kPanel + 1],
+                                T* Li, T* Dinv, DevError* err, int f) {
   const int lane = threadIdx.x & 31;
-  double row[kPanel];
+  T row[kPanel];
 #pragma unroll
   for (int t = 0; t < kPanel; t++)
-    row[t] = (lane < kb && t < kb && t <= lane) ? A[(k + lane) + (int64_t)(k + t) * ld] : 0.0;
+    row[t] = (lane < kb && t < kb && t <= lane) ? A[(k + lane) + (int64_t)(k + t) * ld] : T(0);
   int bad = -1;
 #pragma unroll
   for (int j = 0; j < kPanel; j++) {
     if (j < kb) {
-      double s0 = row[j], s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      T s0 = row[j], s1 = T(0), s2 = T(0), s3 = T(0);
 #pragma unroll
       for (int t = 0; t < j; t++) {
-        const double l = Ls[j][t];
+        const T l = Ls[j][t];
         if ((t & 3) == 0) s0 -= row[t] * l;
         else if ((t & 3) == 1) s1 -= row[t] * l;
         else if ((t & 3) == 2) s2 -= row[t] * l;
         else s3 -= row[t] * l;
       }
-      const double sv = (s0 + s1) + (s2 + s3);
-      double piv = __shfl_sync(kFull, sv, j);
-      if (!(piv > 0.0)) {                // non-positive or NaN pivot: not SPD
+      const T sv = (s0 + s1) + (s2 + s3);
+      T piv = __shfl_sync(kFull, sv, j);
+      if (!(piv > T(0))) {                // non-positive or NaN pivot: not SPD
         if (bad < 0) bad = j;
-        piv = 1.0;
+        piv = T(1);
       }
-      const double r = rsqrt(piv);
-      row[j] = lane == j ? piv * r : (lane > j ? sv * r : 0.0);
+      const T r = rsq(piv);
+      row[j] = lane == j ? piv * r : (lane > j ? sv * r : T(0));
       if (lane >= j && lane < kb) Ls[lane][j] = row[j];
       if (lane == j) Dinv[j] = r;
       __syncwarp();
@@ -204,23 +222,23 @@ __device__ void warp_factor_inv(double* A, int64_t ld, int k, int kb, double (*L
   for (int t = 0; t < kPanel; t++)
     if (lane < kb && t < kb && t <= lane) A[(k + lane) + (int64_t)(k + t) * ld] = row[t];
   // inverse: lane c computes column c, x_i = -(sum_{c<=t<i} L(i,t) x_t) / L(i,i)
-  double x[kPanel];
+  T x[kPanel];
 #pragma unroll
   for (int i = 0; i < kPanel; i++) {
-    double v = 0.0;
+    T v = T(0);
     if (i < kb) {
-      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      T s0 = T(0), s1 = T(0), s2 = T(0), s3 = T(0);
 #pragma unroll
       for (int t = 0; t < i; t++) {
-        const double l = Ls[i][t];
-        const double xt = t >= lane ? x[t] : 0.0;
+        const T l = Ls[i][t];
+        const T xt = t >= lane ? x[t] : T(0);
         if ((t & 3) == 0) s0 += l * xt;
         else if ((t & 3) == 1) s1 += l * xt;
         else if ((t & 3) == 2) s2 += l * xt;
         else s3 += l * xt;
       }
-      const double di = Dinv[i];
-      v = i == lane ? di : (i > lane ? -((s0 + s1) + (s2 + s3)) * di : 0.0);
+      const T di = Dinv[i];
+      v = i == lane ? di : (i > lane ? -((s0 + s1) + (s2 + s3)) * di : T(0));
     }
     x[i] = v;
     Li[i * kLi + lane] = v;
@@ -237,16 +255,15 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
 }
 
 constexpr int kPS = 36;   // shared-memory row stride (doubles) of a staged panel
-constexpr int kSmallMaxN = 640;  // widest front the fused kernel handles (panel in smem)
 
-// acc(32x32) = X[I0:I0+32, 0:kk] * Y[J0:J0+32, 0:kk]^T for row-major operands
+// acc(32x32) += X[I0:I0+32, 0:kk] * Y[J0:J0+32, 0:kk]^T for row-major operands
 // in shared memory (strides sx, sy; rows padded with zeros to the tile edge).
-__device__ __forceinline__ void warp_gemm_nt(const double* X, int sx, int I0, const double* Y, int sy,
-                                             int J0, int kk, int lane, double (&acc)[4][4][2]) {
-#pragma unroll
-  for (int a = 0; a < 4; a++)
-#pragma unroll
-    for (int b = 0; b < 4; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
+// Lane (rr = lane/4, cc = lane%4) owns rows I0 + 8a + rr and columns
+// J0 + 8b + 2cc + q of the tile: the FP64 tensor-core (m8n8k4) accumulator
+// layout, which the FP32 version reproduces with CUDA-core FMAs.
+__device__ __forceinline__ void warp_gemm_nt_acc(const double* X, int sx, int I0, const double* Y,
+                                                 int sy, int J0, int kk, int lane,
+                                                 double (&acc)[4][4][2]) {
   const int rr = lane >> 2, cc = lane & 3;
   for (int k = 0; k < kk; k += 4) {
     double fa[4], fb[4];
@@ -261,18 +278,57 @@ __device__ __forceinline__ void warp_gemm_nt(const double* X, int sx, int I0, co
   }
 }
 
-__device__ __forceinline__ void warp_syrk_tile(const double* P, int I0, int J0, int kk, int lane,
-                                               double (&acc)[4][4][2]) {
+__device__ __forceinline__ void warp_gemm_nt_acc(const float* X, int sx, int I0, const float* Y,
+                                                 int sy, int J0, int kk, int lane,
+                                                 float (&acc)[4][4][2]) {
+  const int rr = lane >> 2, cc = lane & 3;
+  for (int k = 0; k < kk; k++) {
+    float fa[4], fb[4][2];
+#pragma unroll
+    for (int a = 0; a < 4; a++) fa[a] = X[(I0 + 8 * a + rr) * sx + k];
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      fb[b][0] = Y[(J0 + 8 * b + 2 * cc) * sy + k];
+      fb[b][1] = Y[(J0 + 8 * b + 2 * cc + 1) * sy + k];
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        acc[a][b][0] = fmaf(fa[a], fb[b][0], acc[a][b][0]);
+        acc[a][b][1] = fmaf(fa[a], fb[b][1], acc[a][b][1]);
+      }
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void acc_zero(T (&acc)[4][4][2]) {
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[a][b][0] = acc[a][b][1] = T(0);
+}
+
+template <class T>
+__device__ __forceinline__ void warp_gemm_nt(const T* X, int sx, int I0, const T* Y, int sy, int J0,
+                                             int kk, int lane, T (&acc)[4][4][2]) {
+  acc_zero(acc);
+  warp_gemm_nt_acc(X, sx, I0, Y, sy, J0, kk, lane, acc);
+}
+
+template <class T>
+__device__ __forceinline__ void warp_syrk_tile(const T* P, int I0, int J0, int kk, int lane,
+                                               T (&acc)[4][4][2]) {
   warp_gemm_nt(P, kPS, I0, P, kPS, J0, kk, lane, acc);
 }
 
 // Panel triangular solve of the 32-row block R0 of P in place with the explicit
 // inverse: P(R0 block) <- P(R0 block) Li^T; rows < M are also written to A at
 // (r0 + row, k + col), cols < kb.
-__device__ __forceinline__ void warp_trsm_block(double* P, int R0, const double* Li, int kb,
-                                                double* A, int64_t ld, int r0, int k, int M,
-                                                int lane) {
-  double acc[4][4][2];
+template <class T>
+__device__ __forceinline__ void warp_trsm_block(T* P, int R0, const T* Li, int kb, T* A, int64_t ld,
+                                                int r0, int k, int M, int lane) {
+  T acc[4][4][2];
   warp_gemm_nt(P, kPS, R0, Li, kLi, 0, (kb + 3) & ~3, lane, acc);
   __syncwarp();
   const int rr = lane >> 2, cc = lane & 3;
@@ -289,9 +345,12 @@ __device__ __forceinline__ void warp_trsm_block(double* P, int R0, const double*
 }
 
 // C(r0 + i, r0 + j) -= acc for the tile at (I0, J0); lower triangle and i, j < M.
-__device__ __forceinline__ void warp_tile_sub(double* A, int64_t ld, int r0, int M, int I0, int J0,
-                                              int lane, const double (&acc)[4][4][2]) {
+template <class T>
+__device__ __forceinline__ void warp_tile_sub(T* A, int64_t ld, int r0, int M, int I0, int J0,
+                                              int lane, const T (&acc)[4][4][2]) {
   const int rr = lane >> 2, cc = lane & 3;
+  // all loads first, then all stores, so the accesses overlap
+  T cur[4][4][2];
 #pragma unroll
   for (int b = 0; b < 4; b++)
 #pragma unroll
@@ -300,7 +359,18 @@ __device__ __forceinline__ void warp_tile_sub(double* A, int64_t ld, int r0, int
 #pragma unroll
       for (int a = 0; a < 4; a++) {
         const int i = I0 + 8 * a + rr;
-        if (i < M && j < M && i >= j) A[(r0 + i) + (int64_t)(r0 + j) * ld] -= acc[a][b][q];
+        cur[a][b][q] = (i < M && j < M && i >= j) ? A[(r0 + i) + (int64_t)(r0 + j) * ld] : T(0);
+      }
+    }
+#pragma unroll
+  for (int b = 0; b < 4; b++)
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int j = J0 + 8 * b + 2 * cc + q;
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const int i = I0 + 8 * a + rr;
+        if (i < M && j < M && i >= j) A[(r0 + i) + (int64_t)(r0 + j) * ld] = cur[a][b][q] - acc[a][b][q];
       }
     }
 }
@@ -331,16 +401,18 @@ __device__ __forceinline__ void row_trsm(double (&x)[kPanel], const double (*L)[
 // Fused partial factorization, one CTA per front (fronts up to kSmallMaxN).
 // The panel of each step is staged in shared memory for the tensor-core update.
 // ---------------------------------------------------------------------------
+template <class T>
 __global__ void __launch_bounds__(256) k_front_small(const int* __restrict__ flist,
                                                      const FrontDev* __restrict__ fr,
-                                                     double* __restrict__ F, DevError* err) {
-  extern __shared__ double Psm[];
-  __shared__ double Ls[kPanel][kPanel + 1];
-  __shared__ double Li[kPanel * kLi];
-  __shared__ double Dinv[kPanel];
+                                                     T* __restrict__ F, DevError* err) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* Psm = reinterpret_cast<T*>(smraw);
+  __shared__ T Ls[kPanel][kPanel + 1];
+  __shared__ T Li[kPanel * kLi];
+  __shared__ T Dinv[kPanel];
   const int f = flist[blockIdx.x];
   const FrontDev d = fr[f];
-  double* A = F + d.off;
+  T* A = F + d.off;
   const int64_t ld = d.ld;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (warp == 0) warp_factor_inv(A, ld, 0, min(kPanel, d.n), Ls, Li, Dinv, err, f);
@@ -352,19 +424,19 @@ __global__ void __launch_bounds__(256) k_front_small(const int* __restrict__ fli
     // stage the panel rows below the diagonal block (zero padded)
     for (int idx = tid; idx < Mp * kPanel; idx += blockDim.x) {
       const int rr = idx % Mp, t = idx / Mp;
-      Psm[rr * kPS + t] = (rr < M && t < kb) ? A[(r0 + rr) + (int64_t)(k + t) * ld] : 0.0;
+      Psm[rr * kPS + t] = (rr < M && t < kb) ? A[(r0 + rr) + (int64_t)(k + t) * ld] : T(0);
     }
     __syncthreads();
     for (int R0 = warp * 32; R0 < Mp; R0 += 256) warp_trsm_block(Psm, R0, Li, kb, A, ld, r0, k, M, lane);
     __syncthreads();
-    const int T = Mp >> 5;
-    const int ntile = T * (T + 1) / 2;
+    const int TT = Mp >> 5;
+    const int ntile = TT * (TT + 1) / 2;
     const int kk = (kb + 3) & ~3;
     if (warp == 0) {
       // lookahead: tile (0, 0) holds the next diagonal block; update it, then
       // factor it while the other warps finish the trailing update
       if (ntile > 0) {
-        double acc[4][4][2];
+        T acc[4][4][2];
         warp_syrk_tile(Psm, 0, 0, kk, lane, acc);
         warp_tile_sub(A, ld, r0, M, 0, 0, lane, acc);
       }
@@ -374,7 +446,7 @@ __global__ void __launch_bounds__(256) k_front_small(const int* __restrict__ fli
       for (int t = warp; t < ntile; t += 7) {   // warps 1..7 take tiles 1, 2, ...
         int I, J;
         tri_index(t, I, J);
-        double acc[4][4][2];
+        T acc[4][4][2];
         warp_syrk_tile(Psm, I * 32, J * 32, kk, lane, acc);
         warp_tile_sub(A, ld, r0, M, I * 32, J * 32, lane, acc);
       }
@@ -496,19 +568,17 @@ __global__ void __launch_bounds__(128) k_syrk(const int* __restrict__ flist,
 // ---------------------------------------------------------------------------
 constexpr int kOuter = 256;
 constexpr int kCT = 128;           // threads per CTA of the cooperative kernel
-constexpr int kMaxCoopFronts = 256;
+constexpr int kMaxCoopFronts = 8192;
 
 // C(tile) -= X(rows) X(cols)^T over columns [k0, k1) of the front, 64 x 64 tile
 // at rows [ri, ri+64), cols [ci, ci+64); rows < N, cols < cmax, row >= col.
-__device__ void coop_tile_update(double* A, int64_t ld, int N, int cmax, int ri, int ci, int k0,
-                                 int k1, double* Xa, double* Xb) {
+template <class T>
+__device__ void coop_tile_update(T* A, int64_t ld, int N, int cmax, int ri, int ci, int k0, int k1,
+                                 T* Xa, T* Xb) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wi = warp >> 1, wj = warp & 1;
-  double acc[4][4][2];
-#pragma unroll
-  for (int a = 0; a < 4; a++)
-#pragma unroll
-    for (int b = 0; b < 4; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
+  T acc[4][4][2];
+  acc_zero(acc);
   const bool diag = (ri == ci);
   const bool live = !(diag && wi < wj);
   for (int kc = k0; kc < k1; kc += kPanel) {
@@ -518,28 +588,16 @@ __device__ void coop_tile_update(double* A, int64_t ld, int N, int cmax, int ri,
       const int i = idx % 64, t = idx / 64;
       const bool ok = t < kb;
       const int ra = ri + i, rb = ci + i;
-      Xa[i * kPS + t] = (ok && ra < N) ? A[ra + (int64_t)(kc + t) * ld] : 0.0;
-      Xb[i * kPS + t] = (ok && rb < N) ? A[rb + (int64_t)(kc + t) * ld] : 0.0;
+      Xa[i * kPS + t] = (ok && ra < N) ? A[ra + (int64_t)(kc + t) * ld] : T(0);
+      Xb[i * kPS + t] = (ok && rb < N) ? A[rb + (int64_t)(kc + t) * ld] : T(0);
     }
     __syncthreads();
-    if (live) {
-      const int rr = lane >> 2, cc = lane & 3;
-      const int kk = (kb + 3) & ~3;
-      for (int t = 0; t < kk; t += 4) {
-        double fa[4], fb[4];
-#pragma unroll
-        for (int a = 0; a < 4; a++) fa[a] = Xa[(wi * 32 + 8 * a + rr) * kPS + t + cc];
-#pragma unroll
-        for (int b = 0; b < 4; b++) fb[b] = Xb[(wj * 32 + 8 * b + rr) * kPS + t + cc];
-#pragma unroll
-        for (int a = 0; a < 4; a++)
-#pragma unroll
-          for (int b = 0; b < 4; b++) dmma(acc[a][b][0], acc[a][b][1], fa[a], fb[b]);
-      }
-    }
+    if (live) warp_gemm_nt_acc(Xa, kPS, wi * 32, Xb, kPS, wj * 32, (kb + 3) & ~3, lane, acc);
   }
   if (!live) return;
   const int rr = lane >> 2, cc = lane & 3;
+  // all loads first, then all stores, so the accesses overlap
+  T cur[4][4][2];
 #pragma unroll
   for (int b = 0; b < 4; b++)
 #pragma unroll
@@ -548,7 +606,18 @@ __device__ void coop_tile_update(double* A, int64_t ld, int N, int cmax, int ri,
 #pragma unroll
       for (int a = 0; a < 4; a++) {
         const int r = ri + wi * 32 + 8 * a + rr;
-        if (r < N && c < cmax && r >= c) A[r + (int64_t)c * ld] -= acc[a][b][q];
+        cur[a][b][q] = (r < N && c < cmax && r >= c) ? A[r + (int64_t)c * ld] : T(0);
+      }
+    }
+#pragma unroll
+  for (int b = 0; b < 4; b++)
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int c = ci + wj * 32 + 8 * b + 2 * cc + q;
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const int r = ri + wi * 32 + 8 * a + rr;
+        if (r < N && c < cmax && r >= c) A[r + (int64_t)c * ld] = cur[a][b][q] - acc[a][b][q];
       }
     }
 }
@@ -560,8 +629,9 @@ constexpr int kDiagSlot = kPanel * kLi;
 
 // Warp 0 of the calling CTA factors the diagonal block at (k, k), writes it
 // back into the front and publishes it in `slot`.  Every thread must call.
-__device__ void coop_factor_publish(double* A, int64_t ld, int k, int kb, double* slot,
-                                    double (*Ls)[kPanel + 1], double* Li, double* Dinv,
+template <class T>
+__device__ void coop_factor_publish(T* A, int64_t ld, int k, int kb, T* slot,
+                                    T (*Ls)[kPanel + 1], T* Li, T* Dinv,
                                     DevError* err, int f) {
   __syncthreads();
   if (threadIdx.x < 32) {
@@ -573,88 +643,87 @@ __device__ void coop_factor_publish(double* A, int64_t ld, int k, int kb, double
 
 __device__ __forceinline__ int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
+// Per-phase work-item prefixes come from the host (coop_phase_prefix): for
+// phase p, pref[p * (nf + 1) + i] is the first item of front i.  Each CTA
+// copies the phase's prefix into shared memory and binary-searches it.
+//
+// One launch covers the outer panels [K0, K1) (K0 a multiple of kOuter);
+// phase0 is the index of the first phase of outer panel K0 in phase_pref.  With
+// trailing == 0 the last outer panel's phase C is left to the caller (the
+// tensor-core trailing update of the mixed path), and the next launch factors
+// and publishes its first diagonal block itself.
+template <class T>
 __global__ void __launch_bounds__(kCT) k_level_coop(const int* __restrict__ flist, int nf,
                                                     const FrontDev* __restrict__ fr,
-                                                    double* __restrict__ F, DevError* err, int maxn,
-                                                    double* __restrict__ slots) {
+                                                    T* __restrict__ F, DevError* err, int maxn,
+                                                    T* __restrict__ slots,
+                                                    const int* __restrict__ phase_pref, int K0,
+                                                    int K1, int phase0, int trailing) {
   cg::grid_group grid = cg::this_grid();
-  __shared__ double Ls[kPanel][kPanel + 1];
-  __shared__ double Li[kPanel * kLi];
-  __shared__ double Dinv[kPanel];
-  extern __shared__ double Xab[];   // 2 * 64 * kPS doubles (dynamic)
-  __shared__ int pre[kMaxCoopFronts + 1];
-  double* Xa = Xab;             // phase B / C tile operands
-  double* Xb = Xab + 64 * kPS;
-  double* Rows = Xab;           // phase A: kCT = 128 staged rows
+  __shared__ T Ls[kPanel][kPanel + 1];
+  __shared__ T Li[kPanel * kLi];
+  __shared__ T Dinv[kPanel];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* Xa = reinterpret_cast<T*>(smraw);      // phase B / C tile operands
+  T* Xb = Xa + 64 * kPS;
+  T* Rows = Xa;                             // phase A: kCT = 128 staged rows
+  int* pre = reinterpret_cast<int*>(Xa + 2 * 64 * kPS);
   const int tid = threadIdx.x;
+  int phase = phase0;
+  auto load_phase = [&]() {
+    __syncthreads();
+    const int* p = phase_pref + (int64_t)(phase++) * (nf + 1);
+    for (int i = tid; i <= nf; i += kCT) pre[i] = p[i];
+    __syncthreads();
+  };
+  auto find = [&](int item) {   // largest i with pre[i] <= item
+    int lo = 0, hi = nf - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (pre[mid] <= item) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
+  };
   // the first diagonal block of every front
   for (int i = blockIdx.x; i < nf; i += gridDim.x) {
     const int f = flist[i];
     const FrontDev d = fr[f];
-    if (d.n > 0)
-      coop_factor_publish(F + d.off, d.ld, 0, min(kPanel, d.n), slots + (int64_t)i * kDiagSlot, Ls,
-                          Li, Dinv, err, f);
+    if (d.n > K0)
+      coop_factor_publish(F + d.off, d.ld, K0, min(kPanel, d.n - K0), slots + (int64_t)i * kDiagSlot,
+                          Ls, Li, Dinv, err, f);
   }
   grid.sync();
-  for (int K = 0; K < maxn; K += kOuter) {
+  for (int K = K0; K < K1 && K < maxn; K += kOuter) {
     for (int k = K; k < K + kOuter && k < maxn; k += kPanel) {
       // ---- phase A: rows below the (already factored) diagonal block ----
-      __syncthreads();
-      if (tid == 0) {
-        pre[0] = 0;
-        for (int i = 0; i < nf; i++) {
-          const FrontDev d = fr[flist[i]];
-          int c = 0;
-          if (k < d.n) c = ceil_div(d.N - k - min(kPanel, d.n - k), kCT);
-          pre[i + 1] = pre[i] + c;
-        }
-      }
-      __syncthreads();
+      load_phase();
       for (int item = blockIdx.x; item < pre[nf]; item += gridDim.x) {
-        int i = 0;
-        while (pre[i + 1] <= item) i++;
+        const int i = find(item);
         const FrontDev d = fr[flist[i]];
-        double* A = F + d.off;
+        T* A = F + d.off;
         const int kb = min(kPanel, d.n - k);
-        const double* slot = slots + (int64_t)i * kDiagSlot;
+        const T* slot = slots + (int64_t)i * kDiagSlot;
         const int rbase = k + kb + (item - pre[i]) * kCT;
         const int Mi = min(kCT, d.N - rbase);
         __syncthreads();
         for (int idx = tid; idx < kPanel * kLi; idx += kCT) Li[idx] = slot[idx];
         for (int idx = tid; idx < kCT * kPanel; idx += kCT) {
           const int rr = idx % kCT, t = idx / kCT;
-          Rows[rr * kPS + t] = (rr < Mi && t < kb) ? A[(rbase + rr) + (int64_t)(k + t) * d.ld] : 0.0;
+          Rows[rr * kPS + t] = (rr < Mi && t < kb) ? A[(rbase + rr) + (int64_t)(k + t) * d.ld] : T(0);
         }
         __syncthreads();
-        warp_trsm_block(Rows, (tid >> 5) * 32, Li, kb, A, d.ld, rbase, k, Mi, tid & 31);
+        warp_trsm_block(Rows, (tid >> 5) * 32, (const T*)Li, kb, A, d.ld, rbase, k, Mi, tid & 31);
       }
       grid.sync();
       // ---- phase B: update the outer panel's remaining columns; the CTA that
       // updates the next diagonal block factors and publishes it ----
-      __syncthreads();
-      if (tid == 0) {
-        pre[0] = 0;
-        for (int i = 0; i < nf; i++) {
-          const FrontDev d = fr[flist[i]];
-          int c = 0;
-          if (k < d.n) {
-            const int kb = min(kPanel, d.n - k);
-            const int c0 = k + kb, cmax = min(K + kOuter, d.n);
-            if (cmax > c0) {
-              const int TI = ceil_div(d.N - c0, 64), TJ = ceil_div(cmax - c0, 64);
-              for (int J = 0; J < TJ; J++) c += TI - J;
-            }
-          }
-          pre[i + 1] = pre[i] + c;
-        }
-      }
-      __syncthreads();
+      load_phase();
       for (int item = blockIdx.x; item < pre[nf]; item += gridDim.x) {
-        int i = 0;
-        while (pre[i + 1] <= item) i++;
+        const int i = find(item);
         const int f = flist[i];
         const FrontDev d = fr[f];
-        double* A = F + d.off;
+        T* A = F + d.off;
         const int kb = min(kPanel, d.n - k);
         int local = item - pre[i];
         const int c0 = k + kb, cmax = min(K + kOuter, d.n);
@@ -673,24 +742,10 @@ __global__ void __launch_bounds__(kCT) k_level_coop(const int* __restrict__ flis
       grid.sync();
     }
     // ---- phase C: trailing update with the outer panel ----
-    __syncthreads();
-    if (tid == 0) {
-      pre[0] = 0;
-      for (int i = 0; i < nf; i++) {
-        const FrontDev d = fr[flist[i]];
-        int c = 0;
-        const int k1 = min(K + kOuter, d.n);
-        if (K < d.n && d.N > k1) {
-          const int T = ceil_div(d.N - k1, 64);
-          c = T * (T + 1) / 2;
-        }
-        pre[i + 1] = pre[i] + c;
-      }
-    }
-    __syncthreads();
+    if (!trailing && K + kOuter >= K1) break;
+    load_phase();
     for (int item = blockIdx.x; item < pre[nf]; item += gridDim.x) {
-      int i = 0;
-      while (pre[i + 1] <= item) i++;
+      const int i = find(item);
       const int f = flist[i];
       const FrontDev d = fr[f];
       const int k1 = min(K + kOuter, d.n);
@@ -714,11 +769,11 @@ constexpr int ST = 256;
 // Forward solve with the front's first n columns, right-looking over 32-column
 // blocks.  On exit W[0,n) = L11^{-1} b_piv and W[n,N) = -L21 W[0,n).  W is the
 // front's right-hand-side block (N x nrhs, ld N) in shared or global memory.
-template <int NR>
-__device__ void front_forward(const FrontDev& d, const double* __restrict__ A, double* W,
+template <class T, int NR>
+__device__ void front_forward(const FrontDev& d, const T* __restrict__ A, T* W,
                               int nrhs) {
-  __shared__ double Ls[kPanel][kPanel + 1];
-  __shared__ double xs[kPanel][NR + 1];
+  __shared__ T Ls[kPanel][kPanel + 1];
+  __shared__ T xs[kPanel][NR + 1];
   const int N = d.N, n = d.n, ld = d.ld, tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   for (int k = 0; k < n; k += kPanel) {
@@ -736,14 +791,14 @@ __device__ void front_forward(const FrontDev& d, const double* __restrict__ A, d
       // column-oriented substitution: lane i owns row i of the block
       for (int j = 0; j < kb; j++) {
         if (lane == j) {
-          const double djj = Ls[j][j];
+          const T djj = Ls[j][j];
 #pragma unroll
           for (int c = 0; c < NR; c++)
             if (c < nrhs) xs[j][c] = xs[j][c] / djj;
         }
         __syncwarp();
         if (lane > j && lane < kb) {
-          const double l = Ls[lane][j];
+          const T l = Ls[lane][j];
 #pragma unroll
           for (int c = 0; c < NR; c++)
             if (c < nrhs) xs[lane][c] -= l * xs[j][c];
@@ -758,13 +813,13 @@ __device__ void front_forward(const FrontDev& d, const double* __restrict__ A, d
     }
     // rows below the block: W(r, :) -= L(r, k:k+kb) x   (thread per row, coalesced L)
     for (int r = k + kb + tid; r < N; r += blockDim.x) {
-      double acc[NR];
+      T acc[NR];
 #pragma unroll
-      for (int c = 0; c < NR; c++) acc[c] = 0.0;
-      const double* Lr = A + r + (int64_t)k * ld;
+      for (int c = 0; c < NR; c++) acc[c] = T(0);
+      const T* Lr = A + r + (int64_t)k * ld;
       if (kb == kPanel) {
         // all 32 loads issued before the FMAs: memory-level parallelism
-        double l[kPanel];
+        T l[kPanel];
 #pragma unroll
         for (int t = 0; t < kPanel; t++) l[t] = Lr[(int64_t)t * ld];
 #pragma unroll
@@ -773,7 +828,7 @@ __device__ void front_forward(const FrontDev& d, const double* __restrict__ A, d
           for (int c = 0; c < NR; c++) acc[c] = fma(l[t], xs[t][c], acc[c]);
       } else {
         for (int t = 0; t < kb; t++) {
-          const double l = Lr[(int64_t)t * ld];
+          const T l = Lr[(int64_t)t * ld];
 #pragma unroll
           for (int c = 0; c < NR; c++) acc[c] = fma(l, xs[t][c], acc[c]);
         }
@@ -787,11 +842,11 @@ __device__ void front_forward(const FrontDev& d, const double* __restrict__ A, d
 }
 
 // Backward solve: W[0,n) <- L11^{-T} (W[0,n) - L21^T W[n,N)).
-template <int NR>
-__device__ void front_backward(const FrontDev& d, const double* __restrict__ A, double* W,
+template <class T, int NR>
+__device__ void front_backward(const FrontDev& d, const T* __restrict__ A, T* W,
                                int nrhs) {
-  __shared__ double Ls[kPanel][kPanel + 1];
-  __shared__ double xs[kPanel][NR + 1];
+  __shared__ T Ls[kPanel][kPanel + 1];
+  __shared__ T xs[kPanel][NR + 1];
   const int N = d.N, n = d.n, ld = d.ld, tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   const int nblk = (n + kPanel - 1) / kPanel;
@@ -804,17 +859,17 @@ __device__ void front_backward(const FrontDev& d, const double* __restrict__ A, 
     }
     // xs(j, c) = W(k+j, c) - sum_{r >= k+kb} L(r, k+j) W(r, c): warp per column
     for (int j = warp; j < kb; j += nw) {
-      double acc[NR];
+      T acc[NR];
 #pragma unroll
-      for (int c = 0; c < NR; c++) acc[c] = 0.0;
-      const double* Lc = A + (int64_t)(k + j) * ld;
+      for (int c = 0; c < NR; c++) acc[c] = T(0);
+      const T* Lc = A + (int64_t)(k + j) * ld;
       int r = k + kb + lane;
       for (; r + 96 < N; r += 128) {      // four independent loads in flight
-        const double l0 = Lc[r], l1 = Lc[r + 32], l2 = Lc[r + 64], l3 = Lc[r + 96];
+        const T l0 = Lc[r], l1 = Lc[r + 32], l2 = Lc[r + 64], l3 = Lc[r + 96];
 #pragma unroll
         for (int c = 0; c < NR; c++)
           if (c < nrhs) {
-            const double* w = W + (int64_t)c * N + r;
+            const T* w = W + (int64_t)c * N + r;
             acc[c] = fma(l0, w[0], acc[c]);
             acc[c] = fma(l1, w[32], acc[c]);
             acc[c] = fma(l2, w[64], acc[c]);
@@ -822,14 +877,14 @@ __device__ void front_backward(const FrontDev& d, const double* __restrict__ A, 
           }
       }
       for (; r < N; r += 32) {
-        const double l = Lc[r];
+        const T l = Lc[r];
 #pragma unroll
         for (int c = 0; c < NR; c++)
           if (c < nrhs) acc[c] = fma(l, W[r + (int64_t)c * N], acc[c]);
       }
 #pragma unroll
       for (int c = 0; c < NR; c++) {
-        double v = acc[c];
+        T v = acc[c];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0 && c < nrhs) xs[j][c] = W[k + j + (int64_t)c * N] - v;
       }
@@ -838,14 +893,14 @@ __device__ void front_backward(const FrontDev& d, const double* __restrict__ A, 
     if (warp == 0) {
       for (int j = kb - 1; j >= 0; j--) {
         if (lane == j) {
-          const double djj = Ls[j][j];
+          const T djj = Ls[j][j];
 #pragma unroll
           for (int c = 0; c < NR; c++)
             if (c < nrhs) xs[j][c] = xs[j][c] / djj;
         }
         __syncwarp();
         if (lane < j) {
-          const double l = Ls[j][lane];
+          const T l = Ls[j][lane];
 #pragma unroll
           for (int c = 0; c < NR; c++)
             if (c < nrhs) xs[lane][c] -= l * xs[j][c];
@@ -865,25 +920,27 @@ __device__ void front_backward(const FrontDev& d, const double* __restrict__ A, 
 // Shared-memory staging of a front's right-hand-side block when it fits.
 constexpr int kSolveSmemBytes = 200 * 1024;
 
-template <int NR>
+
+template <class T, int NR>
 __global__ void __launch_bounds__(ST) k_solve_fwd(const int* __restrict__ flist,
                                                   const FrontDev* __restrict__ fr,
-                                                  const double* __restrict__ F,
-                                                  const int* __restrict__ dofs, double* X,
-                                                  int64_t ldx, int nrhs, double* Wb,
+                                                  const T* __restrict__ F,
+                                                  const int* __restrict__ dofs, T* X,
+                                                  int64_t ldx, int nrhs, T* Wb,
                                                   const int64_t* __restrict__ woff, int use_smem) {
-  extern __shared__ double smW[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* smW = reinterpret_cast<T*>(smraw);
   const int f = flist[blockIdx.x];
   const FrontDev d = fr[f];
-  double* Wg = Wb + woff[f] * nrhs;
-  double* W = use_smem ? smW : Wg;
+  T* Wg = Wb + woff[f] * nrhs;
+  T* W = use_smem ? smW : Wg;
   const int* dl = dofs + d.dof_off;
   for (int idx = threadIdx.x; idx < d.N * nrhs; idx += blockDim.x) {
     const int i = idx % d.N, c = idx / d.N;
-    W[idx] = i < d.n ? X[dl[i] + (int64_t)c * ldx] : 0.0;
+    W[idx] = i < d.n ? X[dl[i] + (int64_t)c * ldx] : T(0);
   }
   __syncthreads();
-  front_forward<NR>(d, F + d.off, W, nrhs);
+  front_forward<T, NR>(d, F + d.off, W, nrhs);
   for (int idx = threadIdx.x; idx < d.N * nrhs; idx += blockDim.x) {
     const int i = idx % d.N, c = idx / d.N;
     if (i < d.n) X[dl[i] + (int64_t)c * ldx] = W[idx];
@@ -891,47 +948,49 @@ __global__ void __launch_bounds__(ST) k_solve_fwd(const int* __restrict__ flist,
   }
 }
 
-template <int NR>
+template <class T, int NR>
 __global__ void __launch_bounds__(ST) k_solve_bwd(const int* __restrict__ flist,
                                                   const FrontDev* __restrict__ fr,
-                                                  const double* __restrict__ F,
-                                                  const int* __restrict__ dofs, double* X,
-                                                  int64_t ldx, int nrhs, double* Wb,
+                                                  const T* __restrict__ F,
+                                                  const int* __restrict__ dofs, T* X,
+                                                  int64_t ldx, int nrhs, T* Wb,
                                                   const int64_t* __restrict__ woff, int use_smem) {
-  extern __shared__ double smW[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* smW = reinterpret_cast<T*>(smraw);
   const int f = flist[blockIdx.x];
   const FrontDev d = fr[f];
-  double* W = use_smem ? smW : Wb + woff[f] * nrhs;
+  T* W = use_smem ? smW : Wb + woff[f] * nrhs;
   const int* dl = dofs + d.dof_off;
   for (int idx = threadIdx.x; idx < d.N * nrhs; idx += blockDim.x) {
     const int i = idx % d.N, c = idx / d.N;
     W[idx] = X[dl[i] + (int64_t)c * ldx];
   }
   __syncthreads();
-  front_backward<NR>(d, F + d.off, W, nrhs);
+  front_backward<T, NR>(d, F + d.off, W, nrhs);
   for (int idx = threadIdx.x; idx < d.n * nrhs; idx += blockDim.x) {
     const int i = idx % d.n, c = idx / d.n;
     X[dl[i] + (int64_t)c * ldx] = W[i + (int64_t)c * d.N];
   }
 }
 
-template <int NR>
+template <class T, int NR>
 __global__ void __launch_bounds__(ST) k_root_solve(int f, const FrontDev* __restrict__ fr,
-                                                   const double* __restrict__ F,
-                                                   const int* __restrict__ dofs, double* X,
-                                                   int64_t ldx, int nrhs, double* Wb,
+                                                   const T* __restrict__ F,
+                                                   const int* __restrict__ dofs, T* X,
+                                                   int64_t ldx, int nrhs, T* Wb,
                                                    const int64_t* __restrict__ woff, int use_smem) {
-  extern __shared__ double smW[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* smW = reinterpret_cast<T*>(smraw);
   const FrontDev d = fr[f];
-  double* W = use_smem ? smW : Wb + woff[f] * nrhs;
+  T* W = use_smem ? smW : Wb + woff[f] * nrhs;
   const int* dl = dofs + d.dof_off;
   for (int idx = threadIdx.x; idx < d.N * nrhs; idx += blockDim.x) {
     const int i = idx % d.N, c = idx / d.N;
     W[idx] = X[dl[i] + (int64_t)c * ldx];
   }
   __syncthreads();
-  front_forward<NR>(d, F + d.off, W, nrhs);
-  front_backward<NR>(d, F + d.off, W, nrhs);
+  front_forward<T, NR>(d, F + d.off, W, nrhs);
+  front_backward<T, NR>(d, F + d.off, W, nrhs);
   for (int idx = threadIdx.x; idx < d.n * nrhs; idx += blockDim.x) {
     const int i = idx % d.n, c = idx / d.n;
     X[dl[i] + (int64_t)c * ldx] = W[i + (int64_t)c * d.N];
@@ -940,35 +999,37 @@ __global__ void __launch_bounds__(ST) k_root_solve(int f, const FrontDev* __rest
 
 // X(sep) = (X(sep) + W_box0(sep rows)) + W_box1(sep rows), the reference's
 // per-box accumulation order (mf2d.cpp:992-1011, 1036-1047).
+template <class T>
 __global__ void __launch_bounds__(ST) k_sep_gather(const int* __restrict__ slist,
                                                    const SepDev* __restrict__ sp,
-                                                   const int* __restrict__ dofs, double* X,
+                                                   const int* __restrict__ dofs, T* X,
                                                    int64_t ldx, int nrhs,
-                                                   const double* __restrict__ Wb,
+                                                   const T* __restrict__ Wb,
                                                    const int64_t* __restrict__ woff,
                                                    const FrontDev* __restrict__ fr) {
   const SepDev s = sp[slist[blockIdx.x]];
   const int* dl = dofs + s.dof_off;
   const int N0 = fr[s.box0].N, N1 = fr[s.box1].N;
-  const double* W0 = Wb + woff[s.box0] * nrhs;
-  const double* W1 = Wb + woff[s.box1] * nrhs;
+  const T* W0 = Wb + woff[s.box0] * nrhs;
+  const T* W1 = Wb + woff[s.box1] * nrhs;
   for (int idx = threadIdx.x; idx < s.s * nrhs; idx += blockDim.x) {
     const int i = idx % s.s, c = idx / s.s;
-    double* x = X + dl[i] + (int64_t)c * ldx;
+    T* x = X + dl[i] + (int64_t)c * ldx;
     *x = (*x + W0[s.pos0 + i + (int64_t)c * N0]) + W1[s.pos1 + i + (int64_t)c * N1];
   }
 }
 
 // Apply, upward part: t = L11^T b_piv + L21^T b_bd ; b_piv = L11 t ; T(piv) = t.
-__device__ void front_apply_up(const FrontDev& d, const double* __restrict__ A, double* W,
-                               double* Tt, int nrhs) {
+template <class T>
+__device__ void front_apply_up(const FrontDev& d, const T* __restrict__ A, T* W,
+                               T* Tt, int nrhs) {
   // W holds [b_piv; b_bd] (N x nrhs); Tt receives t (n x nrhs, ld n).
   const int N = d.N, n = d.n, ld = d.ld, tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   for (int jc = warp; jc < n * nrhs; jc += nw) {
     const int j = jc % n, c = jc / n;
-    const double* w = W + (int64_t)c * N;
-    double s = 0.0;
+    const T* w = W + (int64_t)c * N;
+    T s = T(0);
     for (int r = j + lane; r < N; r += 32) s += A[r + (int64_t)j * ld] * w[r];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if (lane == 0) Tt[j + (int64_t)c * n] = s;
@@ -976,80 +1037,83 @@ __device__ void front_apply_up(const FrontDev& d, const double* __restrict__ A, 
   __syncthreads();
   for (int idx = tid; idx < n * nrhs; idx += blockDim.x) {
     const int r = idx % n, c = idx / n;
-    const double* t = Tt + (int64_t)c * n;
-    double s = 0.0;
+    const T* t = Tt + (int64_t)c * n;
+    T s = T(0);
     for (int j = 0; j <= r; j++) s += A[r + (int64_t)j * ld] * t[j];
     W[r + (int64_t)c * N] = s;
   }
   __syncthreads();
 }
 
+template <class T>
 __global__ void __launch_bounds__(ST) k_apply_up(const int* __restrict__ flist,
                                                  const FrontDev* __restrict__ fr,
-                                                 const double* __restrict__ F,
-                                                 const int* __restrict__ dofs, double* X,
-                                                 int64_t ldx, int nrhs, double* Wb,
-                                                 const int64_t* __restrict__ woff, double* T) {
+                                                 const T* __restrict__ F,
+                                                 const int* __restrict__ dofs, T* X,
+                                                 int64_t ldx, int nrhs, T* Wb,
+                                                 const int64_t* __restrict__ woff, T* Tb) {
   const int f = flist[blockIdx.x];
   const FrontDev d = fr[f];
-  double* W = Wb + woff[f] * nrhs;
+  T* W = Wb + woff[f] * nrhs;
   const int* dl = dofs + d.dof_off;
   for (int idx = threadIdx.x; idx < d.N * nrhs; idx += blockDim.x) {
     const int i = idx % d.N, c = idx / d.N;
     W[idx] = X[dl[i] + (int64_t)c * ldx];
   }
   __syncthreads();
-  double* Tt = W + (int64_t)d.N * nrhs;  // second half of the front's workspace
+  T* Tt = W + (int64_t)d.N * nrhs;  // second half of the front's workspace
   front_apply_up(d, F + d.off, W, Tt, nrhs);
   for (int idx = threadIdx.x; idx < d.n * nrhs; idx += blockDim.x) {
     const int i = idx % d.n, c = idx / d.n;
     X[dl[i] + (int64_t)c * ldx] = W[i + (int64_t)c * d.N];
-    T[dl[i] + (int64_t)c * ldx] = Tt[i + (int64_t)c * d.n];
+    Tb[dl[i] + (int64_t)c * ldx] = Tt[i + (int64_t)c * d.n];
   }
 }
 
 // Apply, downward part: W[n,N) = L21 t (t read from T by DOF).
+template <class T>
 __global__ void __launch_bounds__(ST) k_apply_down(const int* __restrict__ flist,
                                                    const FrontDev* __restrict__ fr,
-                                                   const double* __restrict__ F,
+                                                   const T* __restrict__ F,
                                                    const int* __restrict__ dofs, int64_t ldx,
-                                                   int nrhs, double* Wb,
+                                                   int nrhs, T* Wb,
                                                    const int64_t* __restrict__ woff,
-                                                   const double* __restrict__ T) {
+                                                   const T* __restrict__ Tb) {
   const int f = flist[blockIdx.x];
   const FrontDev d = fr[f];
-  double* W = Wb + woff[f] * nrhs;
+  T* W = Wb + woff[f] * nrhs;
   const int* dl = dofs + d.dof_off;
-  const double* A = F + d.off;
-  double* Tt = W + (int64_t)d.N * nrhs;
+  const T* A = F + d.off;
+  T* Tt = W + (int64_t)d.N * nrhs;
   for (int idx = threadIdx.x; idx < d.n * nrhs; idx += blockDim.x) {
     const int i = idx % d.n, c = idx / d.n;
-    Tt[i + (int64_t)c * d.n] = T[dl[i] + (int64_t)c * ldx];
+    Tt[i + (int64_t)c * d.n] = Tb[dl[i] + (int64_t)c * ldx];
   }
   __syncthreads();
   for (int idx = threadIdx.x; idx < d.m * nrhs; idx += blockDim.x) {
     const int r = d.n + idx % d.m, c = idx / d.m;
-    const double* t = Tt + (int64_t)c * d.n;
-    double s = 0.0;
+    const T* t = Tt + (int64_t)c * d.n;
+    T s = T(0);
     for (int j = 0; j < d.n; j++) s += A[r + (int64_t)j * d.ld] * t[j];
     W[r + (int64_t)c * d.N] = s;
   }
 }
 
+template <class T>
 __global__ void __launch_bounds__(ST) k_root_apply(int f, const FrontDev* __restrict__ fr,
-                                                   const double* __restrict__ F,
-                                                   const int* __restrict__ dofs, double* X,
-                                                   int64_t ldx, int nrhs, double* Wb,
+                                                   const T* __restrict__ F,
+                                                   const int* __restrict__ dofs, T* X,
+                                                   int64_t ldx, int nrhs, T* Wb,
                                                    const int64_t* __restrict__ woff) {
   const FrontDev d = fr[f];
-  double* W = Wb + woff[f] * nrhs;
+  T* W = Wb + woff[f] * nrhs;
   const int* dl = dofs + d.dof_off;
   for (int idx = threadIdx.x; idx < d.N * nrhs; idx += blockDim.x) {
     const int i = idx % d.N, c = idx / d.N;
     W[idx] = X[dl[i] + (int64_t)c * ldx];
   }
   __syncthreads();
-  double* Tt = W + (int64_t)d.N * nrhs;
+  T* Tt = W + (int64_t)d.N * nrhs;
   front_apply_up(d, F + d.off, W, Tt, nrhs);
   for (int idx = threadIdx.x; idx < d.n * nrhs; idx += blockDim.x) {
     const int i = idx % d.n, c = idx / d.n;
@@ -1059,14 +1123,15 @@ __global__ void __launch_bounds__(ST) k_root_apply(int f, const FrontDev* __rest
 
 }  // namespace
 
-void launch_tasks(const Task* tasks, const int64_t* tstart, int ntasks, int64_t ntiles,
-                  double* fronts, double* seps, const int* rp, const int* ci, const double* va,
-                  const int* dofs, cudaStream_t st) {
+template <class T>
+void launch_tasks(const Task* tasks, const int64_t* tstart, int ntasks, int64_t ntiles, T* fronts,
+                  T* seps, const int* rp, const int* ci, const double* va, const int* dofs,
+                  const double* scale, cudaStream_t st) {
   if (ntasks <= 0 || ntiles <= 0) return;
   const int64_t gx = ntiles < 65535 * 32 ? ntiles : 65535 * 32;
   const int64_t gy = (ntiles + gx - 1) / gx;
-  k_tasks<<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(tasks, tstart, ntasks, fronts,
-                                                                      seps, rp, ci, va, dofs);
+  k_tasks<T><<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(tasks, tstart, ntasks, fronts,
+                                                                         seps, rp, ci, va, dofs, scale);
   g_launches++;
 }
 
@@ -1094,38 +1159,90 @@ void launch_syrk(const int* flist, int nf, const FrontDev* fr, double* F, int k,
 
 long long launches_total() { return g_launches.load(); }
 
-bool small_front_fits(int maxN) { return maxN <= kSmallMaxN; }
+bool small_front_fits(int maxN, int elem_bytes) {
+  // the staged panel (maxN x kPS) plus static shared memory must fit in 227 KB
+  return (size_t)((maxN + 31) & ~31) * kPS * elem_bytes <= 200 * 1024;
+}
 
 bool coop_fits(int nf) { return nf <= kMaxCoopFronts; }
-size_t coop_slot_doubles() { return (size_t)kMaxCoopFronts * kDiagSlot; }
+size_t coop_slot_elems() { return (size_t)kMaxCoopFronts * kDiagSlot; }
 
-cudaError_t launch_level_coop(const int* flist, int nf, int maxn, const FrontDev* fr, double* F,
-                              DevError* err, double* slots, cudaStream_t st) {
+// Work items per phase of k_level_coop for fronts (n_i, N_i), in the kernel's
+// phase order: for each outer panel K, for each 32-column step k, phases A and
+// B; then phase C.  Returns the per-phase prefixes (nf + 1 ints each).
+std::vector<int> coop_phase_prefix(const std::vector<int>& n, const std::vector<int>& N, int maxn) {
+  const int nf = (int)n.size();
+  std::vector<int> out;
+  auto cdiv = [](int a, int b) { return (a + b - 1) / b; };
+  auto push = [&](auto count) {
+    int acc = 0;
+    out.push_back(0);
+    for (int i = 0; i < nf; i++) {
+      acc += count(i);
+      out.push_back(acc);
+    }
+  };
+  for (int K = 0; K < maxn; K += kOuter) {
+    for (int k = K; k < K + kOuter && k < maxn; k += kPanel) {
+      push([&](int i) { return k < n[i] ? cdiv(N[i] - k - std::min(kPanel, n[i] - k), kCT) : 0; });
+      push([&](int i) {
+        if (k >= n[i]) return 0;
+        const int kb = std::min(kPanel, n[i] - k), c0 = k + kb, cmax = std::min(K + kOuter, n[i]);
+        if (cmax <= c0) return 0;
+        const int TI = cdiv(N[i] - c0, 64), TJ = cdiv(cmax - c0, 64);
+        int c = 0;
+        for (int J = 0; J < TJ; J++) c += TI - J;
+        return c;
+      });
+    }
+    push([&](int i) {
+      const int k1 = std::min(K + kOuter, n[i]);
+      if (K >= n[i] || N[i] <= k1) return 0;
+      const int T = cdiv(N[i] - k1, 64);
+      return T * (T + 1) / 2;
+    });
+  }
+  return out;
+}
+
+int coop_outer() { return kOuter; }
+
+int coop_phases(int K, int maxn) {
+  return 2 * ((std::min(kOuter, maxn - K) + kPanel - 1) / kPanel) + 1;
+}
+
+template <class T>
+cudaError_t launch_level_coop(const int* flist, int nf, int maxn, const FrontDev* fr, T* F,
+                              DevError* err, T* slots, const int* phase_pref, cudaStream_t st,
+                              int K0, int K1, int phase0, int trailing) {
   if (nf <= 0) return cudaSuccess;
-  const size_t sm = 2 * 64 * kPS * sizeof(double);
-  static int grid = 0;   // co-resident CTAs on this device (same for every call)
+  if (K1 < 0) K1 = maxn;
+  const size_t sm = 2 * 64 * kPS * sizeof(T) + (size_t)(kMaxCoopFronts + 1) * sizeof(int);
+  static int grid = 0;   // co-resident CTAs of this instantiation on this device
   if (grid == 0) {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaFuncSetAttribute(k_level_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_level_coop, kCT, sm);
+    cudaFuncSetAttribute(k_level_coop<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_level_coop<T>, kCT, sm);
     grid = sms * (per > 0 ? per : 1);
   }
-  void* args[] = {(void*)&flist, (void*)&nf, (void*)&fr, (void*)&F, (void*)&err, (void*)&maxn,
-                  (void*)&slots};
-  cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_level_coop, dim3(grid), dim3(kCT), args,
-                                              sm, st);
+  void* args[] = {(void*)&flist, (void*)&nf,    (void*)&fr,         (void*)&F,
+                  (void*)&err,   (void*)&maxn,  (void*)&slots,      (void*)&phase_pref,
+                  (void*)&K0,    (void*)&K1,    (void*)&phase0,     (void*)&trailing};
+  cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_level_coop<T>, dim3(grid), dim3(kCT),
+                                              args, sm, st);
   g_launches++;
   return e;
 }
 
-void launch_front_small(const int* flist, int nf, int maxN, const FrontDev* fr, double* F,
-                        DevError* err, cudaStream_t st) {
+template <class T>
+void launch_front_small(const int* flist, int nf, int maxN, const FrontDev* fr, T* F, DevError* err,
+                        cudaStream_t st) {
   if (nf <= 0) return;
-  const size_t sm = (size_t)((maxN + 31) & ~31) * kPS * sizeof(double);
-  cudaFuncSetAttribute(k_front_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_front_small<<<nf, 256, sm, st>>>(flist, fr, F, err);
+  const size_t sm = (size_t)((maxN + 31) & ~31) * kPS * sizeof(T);
+  cudaFuncSetAttribute(k_front_small<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_front_small<T><<<nf, 256, sm, st>>>(flist, fr, F, err);
   g_launches++;
 }
 
@@ -1133,93 +1250,128 @@ void launch_front_small(const int* flist, int nf, int maxN, const FrontDev* fr, 
 // the front's right-hand-side block in dynamic shared memory when the largest
 // front's fits.
 namespace {
-template <int NR>
-void fwd_launch(int grid, size_t sm, int use, cudaStream_t st, const int* fl, const FrontDev* fr,
-                const double* F, const int* dofs, double* X, int64_t ldx, int nrhs, double* W,
-                const int64_t* woff) {
-  if (sm) cudaFuncSetAttribute(k_solve_fwd<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_solve_fwd<NR><<<grid, ST, sm, st>>>(fl, fr, F, dofs, X, ldx, nrhs, W, woff, use);
-}
-template <int NR>
-void bwd_launch(int grid, size_t sm, int use, cudaStream_t st, const int* fl, const FrontDev* fr,
-                const double* F, const int* dofs, double* X, int64_t ldx, int nrhs, double* W,
-                const int64_t* woff) {
-  if (sm) cudaFuncSetAttribute(k_solve_bwd<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_solve_bwd<NR><<<grid, ST, sm, st>>>(fl, fr, F, dofs, X, ldx, nrhs, W, woff, use);
-}
-template <int NR>
-void root_launch(size_t sm, int use, cudaStream_t st, int f, const FrontDev* fr, const double* F,
-                 const int* dofs, double* X, int64_t ldx, int nrhs, double* W, const int64_t* woff) {
-  if (sm) cudaFuncSetAttribute(k_root_solve<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_root_solve<NR><<<1, ST, sm, st>>>(f, fr, F, dofs, X, ldx, nrhs, W, woff, use);
-}
-void smemFor(int maxN, int nrhs, size_t& sm, int& use) {
-  const size_t need = (size_t)maxN * nrhs * sizeof(double);
+void smemFor(int maxN, int nrhs, size_t elem, size_t& sm, int& use) {
+  const size_t need = (size_t)maxN * nrhs * elem;
   use = need <= (size_t)kSolveSmemBytes;
   sm = use ? need : 0;
 }
 }  // namespace
 
-void launch_solve_fwd(const int* flist, int nf, int maxN, const FrontDev* fr, const double* F,
-                      const int* dofs, double* X, int64_t ldx, int nrhs, double* W,
-                      const int64_t* woff, cudaStream_t st) {
+template <class T>
+void launch_solve_fwd(const int* flist, int nf, int maxN, const FrontDev* fr, const T* F,
+                      const int* dofs, T* X, int64_t ldx, int nrhs, T* W, const int64_t* woff,
+                      cudaStream_t st) {
   if (nf <= 0) return;
   size_t sm;
   int use;
-  smemFor(maxN, nrhs, sm, use);
-  if (nrhs == 1) fwd_launch<1>(nf, sm, use, st, flist, fr, F, dofs, X, ldx, nrhs, W, woff);
-  else if (nrhs <= 4) fwd_launch<4>(nf, sm, use, st, flist, fr, F, dofs, X, ldx, nrhs, W, woff);
-  else fwd_launch<16>(nf, sm, use, st, flist, fr, F, dofs, X, ldx, nrhs, W, woff);
+  smemFor(maxN, nrhs, sizeof(T), sm, use);
+#define MFGPU_FWD(NR)                                                                          \
+  do {                                                                                         \
+    if (sm) cudaFuncSetAttribute(k_solve_fwd<T, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 (int)sm);                                                     \
+    k_solve_fwd<T, NR><<<nf, ST, sm, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff, use);    \
+  } while (0)
+  if (nrhs == 1) MFGPU_FWD(1);
+  else if (nrhs <= 4) MFGPU_FWD(4);
+  else MFGPU_FWD(16);
+#undef MFGPU_FWD
   g_launches++;
 }
-void launch_solve_bwd(const int* flist, int nf, int maxN, const FrontDev* fr, const double* F,
-                      const int* dofs, double* X, int64_t ldx, int nrhs, double* W,
-                      const int64_t* woff, cudaStream_t st) {
+
+template <class T>
+void launch_solve_bwd(const int* flist, int nf, int maxN, const FrontDev* fr, const T* F,
+                      const int* dofs, T* X, int64_t ldx, int nrhs, T* W, const int64_t* woff,
+                      cudaStream_t st) {
   if (nf <= 0) return;
   size_t sm;
   int use;
-  smemFor(maxN, nrhs, sm, use);
-  if (nrhs == 1) bwd_launch<1>(nf, sm, use, st, flist, fr, F, dofs, X, ldx, nrhs, W, woff);
-  else if (nrhs <= 4) bwd_launch<4>(nf, sm, use, st, flist, fr, F, dofs, X, ldx, nrhs, W, woff);
-  else bwd_launch<16>(nf, sm, use, st, flist, fr, F, dofs, X, ldx, nrhs, W, woff);
+  smemFor(maxN, nrhs, sizeof(T), sm, use);
+#define MFGPU_BWD(NR)                                                                          \
+  do {                                                                                         \
+    if (sm) cudaFuncSetAttribute(k_solve_bwd<T, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 (int)sm);                                                     \
+    k_solve_bwd<T, NR><<<nf, ST, sm, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff, use);    \
+  } while (0)
+  if (nrhs == 1) MFGPU_BWD(1);
+  else if (nrhs <= 4) MFGPU_BWD(4);
+  else MFGPU_BWD(16);
+#undef MFGPU_BWD
   g_launches++;
 }
-void launch_apply_up(const int* flist, int nf, const FrontDev* fr, const double* F,
-                     const int* dofs, double* X, int64_t ldx, int nrhs, double* W,
-                     const int64_t* woff, double* T, cudaStream_t st) {
+
+template <class T>
+void launch_root_solve(int f, int N, const FrontDev* fr, const T* F, const int* dofs, T* X,
+                       int64_t ldx, int nrhs, T* W, const int64_t* woff, cudaStream_t st) {
+  size_t sm;
+  int use;
+  smemFor(N, nrhs, sizeof(T), sm, use);
+#define MFGPU_ROOT(NR)                                                                          \
+  do {                                                                                          \
+    if (sm) cudaFuncSetAttribute(k_root_solve<T, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 (int)sm);                                                      \
+    k_root_solve<T, NR><<<1, ST, sm, st>>>(f, fr, F, dofs, X, ldx, nrhs, W, woff, use);         \
+  } while (0)
+  if (nrhs == 1) MFGPU_ROOT(1);
+  else if (nrhs <= 4) MFGPU_ROOT(4);
+  else MFGPU_ROOT(16);
+#undef MFGPU_ROOT
+  g_launches++;
+}
+
+template <class T>
+void launch_apply_up(const int* flist, int nf, const FrontDev* fr, const T* F, const int* dofs, T* X,
+                     int64_t ldx, int nrhs, T* W, const int64_t* woff, T* Tb, cudaStream_t st) {
   if (nf <= 0) return;
-  k_apply_up<<<nf, ST, 0, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff, T);
+  k_apply_up<T><<<nf, ST, 0, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff, Tb);
   g_launches++;
 }
-void launch_apply_down(const int* flist, int nf, const FrontDev* fr, const double* F,
-                       const int* dofs, int64_t ldx, int nrhs, double* W, const int64_t* woff,
-                       const double* T, cudaStream_t st) {
-  if (nf <= 0) return;
-  k_apply_down<<<nf, ST, 0, st>>>(flist, fr, F, dofs, ldx, nrhs, W, woff, T);
-  g_launches++;
-}
-void launch_root_solve(int f, int N, const FrontDev* fr, const double* F, const int* dofs,
-                       double* X, int64_t ldx, int nrhs, double* W, const int64_t* woff,
+template <class T>
+void launch_apply_down(const int* flist, int nf, const FrontDev* fr, const T* F, const int* dofs,
+                       int64_t ldx, int nrhs, T* W, const int64_t* woff, const T* Tb,
                        cudaStream_t st) {
-  size_t sm;
-  int use;
-  smemFor(N, nrhs, sm, use);
-  if (nrhs == 1) root_launch<1>(sm, use, st, f, fr, F, dofs, X, ldx, nrhs, W, woff);
-  else if (nrhs <= 4) root_launch<4>(sm, use, st, f, fr, F, dofs, X, ldx, nrhs, W, woff);
-  else root_launch<16>(sm, use, st, f, fr, F, dofs, X, ldx, nrhs, W, woff);
+  if (nf <= 0) return;
+  k_apply_down<T><<<nf, ST, 0, st>>>(flist, fr, F, dofs, ldx, nrhs, W, woff, Tb);
   g_launches++;
 }
-void launch_root_apply(int f, const FrontDev* fr, const double* F, const int* dofs, double* X,
-                       int64_t ldx, int nrhs, double* W, const int64_t* woff, cudaStream_t st) {
-  k_root_apply<<<1, ST, 0, st>>>(f, fr, F, dofs, X, ldx, nrhs, W, woff);
+template <class T>
+void launch_root_apply(int f, const FrontDev* fr, const T* F, const int* dofs, T* X, int64_t ldx,
+                       int nrhs, T* W, const int64_t* woff, cudaStream_t st) {
+  k_root_apply<T><<<1, ST, 0, st>>>(f, fr, F, dofs, X, ldx, nrhs, W, woff);
   g_launches++;
 }
-void launch_sep_gather(const int* slist, int ns, const SepDev* sp, const int* dofs, double* X,
-                       int64_t ldx, int nrhs, const double* W, const int64_t* woff,
-                       const FrontDev* fr, cudaStream_t st) {
+template <class T>
+void launch_sep_gather(const int* slist, int ns, const SepDev* sp, const int* dofs, T* X,
+                       int64_t ldx, int nrhs, const T* W, const int64_t* woff, const FrontDev* fr,
+                       cudaStream_t st) {
   if (ns <= 0) return;
-  k_sep_gather<<<ns, ST, 0, st>>>(slist, sp, dofs, X, ldx, nrhs, W, woff, fr);
+  k_sep_gather<T><<<ns, ST, 0, st>>>(slist, sp, dofs, X, ldx, nrhs, W, woff, fr);
   g_launches++;
 }
+
+#define MFGPU_INSTANTIATE(T)                                                                      \
+  template void launch_tasks<T>(const Task*, const int64_t*, int, int64_t, T*, T*, const int*,     \
+                                const int*, const double*, const int*, const double*, cudaStream_t); \
+  template cudaError_t launch_level_coop<T>(const int*, int, int, const FrontDev*, T*, DevError*,  \
+                                            T*, const int*, cudaStream_t, int, int, int, int);      \
+  template void launch_front_small<T>(const int*, int, int, const FrontDev*, T*, DevError*,        \
+                                      cudaStream_t);                                                \
+  template void launch_solve_fwd<T>(const int*, int, int, const FrontDev*, const T*, const int*,   \
+                                    T*, int64_t, int, T*, const int64_t*, cudaStream_t);            \
+  template void launch_solve_bwd<T>(const int*, int, int, const FrontDev*, const T*, const int*,   \
+                                    T*, int64_t, int, T*, const int64_t*, cudaStream_t);            \
+  template void launch_root_solve<T>(int, int, const FrontDev*, const T*, const int*, T*, int64_t, \
+                                     int, T*, const int64_t*, cudaStream_t);                        \
+  template void launch_apply_up<T>(const int*, int, const FrontDev*, const T*, const int*, T*,     \
+                                   int64_t, int, T*, const int64_t*, T*, cudaStream_t);             \
+  template void launch_apply_down<T>(const int*, int, const FrontDev*, const T*, const int*,       \
+                                     int64_t, int, T*, const int64_t*, const T*, cudaStream_t);     \
+  template void launch_root_apply<T>(int, const FrontDev*, const T*, const int*, T*, int64_t, int, \
+                                     T*, const int64_t*, cudaStream_t);                             \
+  template void launch_sep_gather<T>(const int*, int, const SepDev*, const int*, T*, int64_t, int, \
+                                     const T*, const int64_t*, const FrontDev*, cudaStream_t);
+
+MFGPU_INSTANTIATE(double)
+MFGPU_INSTANTIATE(float)
+#undef MFGPU_INSTANTIATE
 
 }  // namespace mfgpu

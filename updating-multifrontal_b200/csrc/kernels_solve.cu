@@ -1,0 +1,501 @@
+// Cooperative forward / backward sweeps for the levels of large fronts.
+//
+// The one-CTA-per-front sweeps (kernels_front.cu) serialise a front's whole
+// triangular solve on one SM, which leaves a level of a few large fronts (the
+// top of a 3D tree, the root of every problem) far below HBM bandwidth.  These
+// kernels spread every front of a level over all SMs with one cooperative
+// launch and a blocked, right-looking substitution over 64-column blocks:
+//
+//   forward  (src/DE/mf2d.cpp:976-1014, the per-box L11 solve and the
+//   boundary update b_bd -= L21 y):
+//     step j: every CTA takes 256 rows below block j and applies
+//             W(rows) -= L(rows, block j) y_j; the CTA holding the rows of
+//             block j+1 then solves that block (lookahead); grid barrier.
+//   backward (src/DE/mf2d.cpp:1016-1054, x_piv = L11^{-T}(y - L21^T x_bd)):
+//     first r = y - L21^T x_bd by column blocks, then for j = last .. 1
+//     every CTA takes one column block c < j and applies
+//     r_c -= L(block j, block c)^T x_j; the CTA holding block j-1 then solves
+//     it; grid barrier.
+//
+// Each front's L is read once per sweep.  W is the front's right-hand-side
+// block (N x nrhs, ld N) in the same workspace the per-front kernels use, so
+// the separator gathers between levels are unchanged.
+#include <cooperative_groups.h>
+
+#include <atomic>
+#include <cstdint>
+
+#include "device.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace mfgpu {
+
+extern std::atomic<long long> g_launches;
+
+namespace {
+
+constexpr int SB = 64;          // diagonal block of the substitution
+constexpr int SCT = 256;        // threads per CTA
+constexpr int kMaxSolveCoopFronts = SCT;
+constexpr int SP = 32;          // sub-block solved by one warp
+
+__host__ __device__ __forceinline__ int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+// pre[0..nf] = exclusive prefix of the per-front counts (thread t holds front
+// t's count); every thread must call.
+__device__ void scan_counts(int v, int nf, int* pre, int* wt) {
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  __syncthreads();   // pre / wt may still be read by the previous step
+  if (lane == 31) wt[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int t = lane < SCT / 32 ? wt[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    if (lane < SCT / 32) wt[lane] = t;
+  }
+  __syncthreads();
+  if (tid < nf) pre[tid + 1] = (w > 0 ? wt[w - 1] : 0) + x;
+  if (tid == 0) pre[0] = 0;
+  __syncthreads();
+}
+
+__device__ __forceinline__ int find_front(const int* pre, int nf, int item) {
+  int lo = 0, hi = nf - 1;   // largest i with pre[i] <= item
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// In place: W(k:k+kb, :) <- L(k:k+kb, k:k+kb)^{-1} W(k:k+kb, :), kb <= SB.
+// Warp 0 substitutes 32-row sub-blocks; the whole CTA updates the rows of the
+// second sub-block in between.  Every thread must call.
+template <class T, int NR>
+__device__ void diag_lower_solve(const T* __restrict__ A, int64_t ld, T* W, int N, int k, int kb,
+                                 int nrhs, T (*Ls)[SP + 1], T (*xs)[NR + 1]) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int s = 0; s < kb; s += SP) {
+    const int sb = min(SP, kb - s), k0 = k + s;
+    __syncthreads();
+    for (int idx = tid; idx < sb * sb; idx += SCT) {
+      const int i = idx % sb, j = idx / sb;
+      if (i >= j) Ls[i][j] = A[(k0 + i) + (int64_t)(k0 + j) * ld];
+    }
+    for (int idx = tid; idx < sb * nrhs; idx += SCT) {
+      const int i = idx % sb, c = idx / sb;
+      xs[i][c] = W[k0 + i + (int64_t)c * N];
+    }
+    __syncthreads();
+    if (warp == 0) {
+      for (int j = 0; j < sb; j++) {
+        if (lane == j) {
+          const T djj = Ls[j][j];
+#pragma unroll
+          for (int c = 0; c < NR; c++)
+            if (c < nrhs) xs[j][c] = xs[j][c] / djj;
+        }
+        __syncwarp();
+        if (lane > j && lane < sb) {
+          const T l = Ls[lane][j];
+#pragma unroll
+          for (int c = 0; c < NR; c++)
+            if (c < nrhs) xs[lane][c] -= l * xs[j][c];
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < sb * nrhs; idx += SCT) {
+      const int i = idx % sb, c = idx / sb;
+      W[k0 + i + (int64_t)c * N] = xs[i][c];
+    }
+    // rows of the remaining sub-block: W(r) -= L(r, k0:k0+sb) x
+    const int rend = k + kb;
+    for (int idx = tid; idx < (rend - k0 - sb) * nrhs; idx += SCT) {
+      const int r = k0 + sb + idx % (rend - k0 - sb), c = idx / (rend - k0 - sb);
+      T acc = T(0);
+      for (int t = 0; t < sb; t++) acc = fma(A[r + (int64_t)(k0 + t) * ld], xs[t][c], acc);
+      W[r + (int64_t)c * N] -= acc;
+    }
+  }
+  __syncthreads();
+}
+
+// In place: W(k:k+kb, :) <- L(k:k+kb, k:k+kb)^{-T} W(k:k+kb, :), kb <= SB.
+template <class T, int NR>
+__device__ void diag_upper_solve(const T* __restrict__ A, int64_t ld, T* W, int N, int k, int kb,
+                                 int nrhs, T (*Ls)[SP + 1], T (*xs)[NR + 1]) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nsub = cdiv(kb, SP);
+  for (int q = nsub - 1; q >= 0; q--) {
+    const int s = q * SP, sb = min(SP, kb - s), k0 = k + s;
+    __syncthreads();
+    for (int idx = tid; idx < sb * sb; idx += SCT) {
+      const int i = idx % sb, j = idx / sb;
+      if (i >= j) Ls[i][j] = A[(k0 + i) + (int64_t)(k0 + j) * ld];
+    }
+    for (int idx = tid; idx < sb * nrhs; idx += SCT) {
+      const int i = idx % sb, c = idx / sb;
+      xs[i][c] = W[k0 + i + (int64_t)c * N];
+    }
+    __syncthreads();
+    if (warp == 0) {
+      for (int j = sb - 1; j >= 0; j--) {
+        if (lane == j) {
+          const T djj = Ls[j][j];
+#pragma unroll
+          for (int c = 0; c < NR; c++)
+            if (c < nrhs) xs[j][c] = xs[j][c] / djj;
+        }
+        __syncwarp();
+        if (lane < j) {
+          const T l = Ls[j][lane];
+#pragma unroll
+          for (int c = 0; c < NR; c++)
+            if (c < nrhs) xs[lane][c] -= l * xs[j][c];
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < sb * nrhs; idx += SCT) {
+      const int i = idx % sb, c = idx / sb;
+      W[k0 + i + (int64_t)c * N] = xs[i][c];
+    }
+    // columns of the earlier sub-block: W(col) -= L(k0:k0+sb, col)^T x
+    for (int idx = tid; idx < s * nrhs; idx += SCT) {
+      const int col = k + idx % s, c = idx / s;
+      T acc = T(0);
+      for (int t = 0; t < sb; t++) acc = fma(A[(k0 + t) + (int64_t)col * ld], xs[t][c], acc);
+      W[col + (int64_t)c * N] -= acc;
+    }
+  }
+  __syncthreads();
+}
+
+template <class T, int NR>
+__global__ void __launch_bounds__(SCT) k_solve_coop_fwd(const int* __restrict__ flist, int nf,
+                                                        const FrontDev* __restrict__ fr,
+                                                        const T* __restrict__ F,
+                                                        const int* __restrict__ dofs, T* X,
+                                                        int64_t ldx, int nrhs, T* Wb,
+                                                        const int64_t* __restrict__ woff,
+                                                        int maxnb) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ int pre[kMaxSolveCoopFronts + 1];
+  __shared__ int wt[SCT / 32];
+  __shared__ T ys[SB][NR + 1];
+  __shared__ T Ls[SP][SP + 1];
+  __shared__ T xs[SP][NR + 1];
+  const int tid = threadIdx.x;
+  const int64_t gstride = (int64_t)gridDim.x * SCT;
+  // gather: pivot rows from X, boundary rows zero
+  for (int i = 0; i < nf; i++) {
+    const int f = flist[i];
+    const FrontDev d = fr[f];
+    T* W = Wb + woff[f] * nrhs;
+    const int* dl = dofs + d.dof_off;
+    for (int64_t idx = (int64_t)blockIdx.x * SCT + tid; idx < (int64_t)d.N * nrhs; idx += gstride) {
+      const int r = (int)(idx % d.N), c = (int)(idx / d.N);
+      W[idx] = r < d.n ? X[dl[r] + (int64_t)c * ldx] : T(0);
+    }
+  }
+  grid.sync();
+  for (int i = blockIdx.x; i < nf; i += gridDim.x) {
+    const int f = flist[i];
+    const FrontDev d = fr[f];
+    if (d.n > 0)
+      diag_lower_solve<T, NR>(F + d.off, d.ld, Wb + woff[f] * nrhs, d.N, 0, min(SB, d.n), nrhs, Ls,
+                              xs);
+  }
+  grid.sync();
+  for (int j = 0; j < maxnb; j++) {
+    int cnt = 0;
+    if (tid < nf) {
+      const FrontDev d = fr[flist[tid]];
+      const int k = j * SB;
+      if (k < d.n) {
+        const int r0 = k + min(SB, d.n - k);
+        if (d.N > r0) cnt = cdiv(d.N - r0, SCT);
+      }
+    }
+    scan_counts(cnt, nf, pre, wt);
+    for (int item = blockIdx.x; item < pre[nf]; item += gridDim.x) {
+      const int i = find_front(pre, nf, item);
+      const int f = flist[i];
+      const FrontDev d = fr[f];
+      const T* A = F + d.off;
+      T* W = Wb + woff[f] * nrhs;
+      const int k = j * SB, kb = min(SB, d.n - k);
+      const int local = item - pre[i];
+      const int r0 = k + kb + local * SCT;
+      __syncthreads();
+      for (int idx = tid; idx < SB * nrhs; idx += SCT) {
+        const int t = idx % SB, c = idx / SB;
+        ys[t][c] = t < kb ? W[k + t + (int64_t)c * d.N] : T(0);
+      }
+      __syncthreads();
+      const int r = r0 + tid;
+      if (r < d.N) {
+        T acc[NR];
+#pragma unroll
+        for (int c = 0; c < NR; c++) acc[c] = T(0);
+        const T* Lr = A + r + (int64_t)k * d.ld;
+        if (kb == SB) {
+#pragma unroll
+          for (int t0 = 0; t0 < SB; t0 += 16) {
+            T l[16];
+#pragma unroll
+            for (int t = 0; t < 16; t++) l[t] = Lr[(int64_t)(t0 + t) * d.ld];
+#pragma unroll
+            for (int t = 0; t < 16; t++)
+#pragma unroll
+              for (int c = 0; c < NR; c++) acc[c] = fma(l[t], ys[t0 + t][c], acc[c]);
+          }
+        } else {
+          for (int t = 0; t < kb; t++) {
+            const T l = Lr[(int64_t)t * d.ld];
+#pragma unroll
+            for (int c = 0; c < NR; c++) acc[c] = fma(l, ys[t][c], acc[c]);
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < NR; c++)
+          if (c < nrhs) W[r + (int64_t)c * d.N] -= acc[c];
+      }
+      // lookahead: the CTA holding block j+1's rows solves it now
+      if (local == 0 && k + kb < d.n) {
+        __syncthreads();
+        diag_lower_solve<T, NR>(A, d.ld, W, d.N, k + kb, min(SB, d.n - k - kb), nrhs, Ls, xs);
+      }
+    }
+    grid.sync();
+  }
+  // pivots back to X; the boundary part stays in W for the separator gather
+  for (int i = 0; i < nf; i++) {
+    const int f = flist[i];
+    const FrontDev d = fr[f];
+    const T* W = Wb + woff[f] * nrhs;
+    const int* dl = dofs + d.dof_off;
+    for (int64_t idx = (int64_t)blockIdx.x * SCT + tid; idx < (int64_t)d.n * nrhs; idx += gstride) {
+      const int r = (int)(idx % d.n), c = (int)(idx / d.n);
+      X[dl[r] + (int64_t)c * ldx] = W[r + (int64_t)c * d.N];
+    }
+  }
+}
+
+template <class T, int NR>
+__global__ void __launch_bounds__(SCT) k_solve_coop_bwd(const int* __restrict__ flist, int nf,
+                                                        const FrontDev* __restrict__ fr,
+                                                        const T* __restrict__ F,
+                                                        const int* __restrict__ dofs, T* X,
+                                                        int64_t ldx, int nrhs, T* Wb,
+                                                        const int64_t* __restrict__ woff,
+                                                        int maxnb) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ int pre[kMaxSolveCoopFronts + 1];
+  __shared__ int wt[SCT / 32];
+  __shared__ T xj[SB][NR + 1];
+  __shared__ T Ls[SP][SP + 1];
+  __shared__ T xs[SP][NR + 1];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t gstride = (int64_t)gridDim.x * SCT;
+  for (int i = 0; i < nf; i++) {
+    const int f = flist[i];
+    const FrontDev d = fr[f];
+    T* W = Wb + woff[f] * nrhs;
+    const int* dl = dofs + d.dof_off;
+    for (int64_t idx = (int64_t)blockIdx.x * SCT + tid; idx < (int64_t)d.N * nrhs; idx += gstride) {
+      const int r = (int)(idx % d.N), c = (int)(idx / d.N);
+      W[idx] = X[dl[r] + (int64_t)c * ldx];
+    }
+  }
+  grid.sync();
+  // r = y - L21^T x_bd, one column block per item; the CTA with the last
+  // block then solves it
+  {
+    int cnt = 0;
+    if (tid < nf) cnt = cdiv(fr[flist[tid]].n, SB);
+    scan_counts(cnt, nf, pre, wt);
+    for (int item = blockIdx.x; item < pre[nf]; item += gridDim.x) {
+      const int i = find_front(pre, nf, item);
+      const int f = flist[i];
+      const FrontDev d = fr[f];
+      const T* A = F + d.off;
+      T* W = Wb + woff[f] * nrhs;
+      const int cb = item - pre[i], k = cb * SB, kb = min(SB, d.n - k);
+      if (d.m > 0) {
+        for (int jj = warp; jj < kb; jj += SCT / 32) {
+          const T* Lc = A + (int64_t)(k + jj) * d.ld;
+          T acc[NR];
+#pragma unroll
+          for (int c = 0; c < NR; c++) acc[c] = T(0);
+          int r = d.n + lane;
+          for (; r + 96 < d.N; r += 128) {
+            const T l0 = Lc[r], l1 = Lc[r + 32], l2 = Lc[r + 64], l3 = Lc[r + 96];
+#pragma unroll
+            for (int c = 0; c < NR; c++)
+              if (c < nrhs) {
+                const T* w = W + (int64_t)c * d.N + r;
+                acc[c] = fma(l0, w[0], acc[c]);
+                acc[c] = fma(l1, w[32], acc[c]);
+                acc[c] = fma(l2, w[64], acc[c]);
+                acc[c] = fma(l3, w[96], acc[c]);
+              }
+          }
+          for (; r < d.N; r += 32) {
+            const T l = Lc[r];
+#pragma unroll
+            for (int c = 0; c < NR; c++)
+              if (c < nrhs) acc[c] = fma(l, W[r + (int64_t)c * d.N], acc[c]);
+          }
+#pragma unroll
+          for (int c = 0; c < NR; c++) {
+            T v = acc[c];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0 && c < nrhs) W[k + jj + (int64_t)c * d.N] -= v;
+          }
+        }
+      }
+      if (k + kb == d.n) {
+        __syncthreads();
+        diag_upper_solve<T, NR>(A, d.ld, W, d.N, k, kb, nrhs, Ls, xs);
+      }
+    }
+    grid.sync();
+  }
+  // step t: front i works on its block j = nb_i - 1 - t
+  for (int t = 0; t < maxnb - 1; t++) {
+    int cnt = 0;
+    if (tid < nf) {
+      const int j = cdiv(fr[flist[tid]].n, SB) - 1 - t;
+      cnt = j >= 1 ? j : 0;
+    }
+    scan_counts(cnt, nf, pre, wt);
+    for (int item = blockIdx.x; item < pre[nf]; item += gridDim.x) {
+      const int i = find_front(pre, nf, item);
+      const int f = flist[i];
+      const FrontDev d = fr[f];
+      const T* A = F + d.off;
+      T* W = Wb + woff[f] * nrhs;
+      const int j = cdiv(d.n, SB) - 1 - t;
+      const int kj = j * SB, kbj = min(SB, d.n - kj);
+      const int cb = item - pre[i], k = cb * SB;   // column block cb < j (full width)
+      __syncthreads();
+      for (int idx = tid; idx < SB * nrhs; idx += SCT) {
+        const int r = idx % SB, c = idx / SB;
+        xj[r][c] = r < kbj ? W[kj + r + (int64_t)c * d.N] : T(0);
+      }
+      __syncthreads();
+      // thread (cl, q): column k + cl of the block, rows kj + 16 q .. +16; the
+      // four row quarters of a column sit in adjacent lanes
+      const int cl = tid >> 2, q = tid & 3, col = k + cl;
+      T acc[NR];
+#pragma unroll
+      for (int c = 0; c < NR; c++) acc[c] = T(0);
+      const T* Lc = A + (int64_t)col * d.ld + kj + q * 16;
+#pragma unroll
+      for (int rr = 0; rr < 16; rr++) {
+        const int r = q * 16 + rr;
+        if (r < kbj) {
+          const T l = Lc[rr];
+#pragma unroll
+          for (int c = 0; c < NR; c++) acc[c] = fma(l, xj[r][c], acc[c]);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < NR; c++) {
+        acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 1);
+        acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 2);
+      }
+      if (q == 0)
+#pragma unroll
+        for (int c = 0; c < NR; c++)
+          if (c < nrhs) W[col + (int64_t)c * d.N] -= acc[c];
+      if (cb == j - 1) {
+        __syncthreads();
+        diag_upper_solve<T, NR>(A, d.ld, W, d.N, k, SB, nrhs, Ls, xs);
+      }
+    }
+    grid.sync();
+  }
+  for (int i = 0; i < nf; i++) {
+    const int f = flist[i];
+    const FrontDev d = fr[f];
+    const T* W = Wb + woff[f] * nrhs;
+    const int* dl = dofs + d.dof_off;
+    for (int64_t idx = (int64_t)blockIdx.x * SCT + tid; idx < (int64_t)d.n * nrhs; idx += gstride) {
+      const int r = (int)(idx % d.n), c = (int)(idx / d.n);
+      X[dl[r] + (int64_t)c * ldx] = W[r + (int64_t)c * d.N];
+    }
+  }
+}
+
+template <class K>
+int coopGrid(K kern) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, SCT, 0);
+  return sms * (per > 0 ? per : 1);
+}
+
+template <class T, int NR>
+cudaError_t launchCoopSolve(bool fwd, const int* flist, int nf, int maxn, const FrontDev* fr,
+                            const T* F, const int* dofs, T* X, int64_t ldx, int nrhs, T* W,
+                            const int64_t* woff, cudaStream_t st) {
+  static int gf = 0, gb = 0;
+  if (gf == 0) {
+    gf = coopGrid(k_solve_coop_fwd<T, NR>);
+    gb = coopGrid(k_solve_coop_bwd<T, NR>);
+  }
+  int maxnb = cdiv(maxn, SB);
+  void* args[] = {(void*)&flist, (void*)&nf,   (void*)&fr,   (void*)&F,
+                  (void*)&dofs,  (void*)&X,    (void*)&ldx,  (void*)&nrhs,
+                  (void*)&W,     (void*)&woff, (void*)&maxnb};
+  g_launches++;
+  if (fwd)
+    return cudaLaunchCooperativeKernel((const void*)k_solve_coop_fwd<T, NR>, dim3(gf), dim3(SCT),
+                                       args, 0, st);
+  return cudaLaunchCooperativeKernel((const void*)k_solve_coop_bwd<T, NR>, dim3(gb), dim3(SCT), args,
+                                     0, st);
+}
+
+}  // namespace
+
+int solve_coop_max_fronts() { return kMaxSolveCoopFronts; }
+
+template <class T>
+cudaError_t launch_solve_coop(bool forward, const int* flist, int nf, int maxn, const FrontDev* fr,
+                              const T* F, const int* dofs, T* X, int64_t ldx, int nrhs, T* W,
+                              const int64_t* woff, cudaStream_t st) {
+  if (nf <= 0) return cudaSuccess;
+  if (nf > kMaxSolveCoopFronts || nrhs > 16) return cudaErrorInvalidValue;
+  if (nrhs == 1)
+    return launchCoopSolve<T, 1>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, st);
+  if (nrhs <= 4)
+    return launchCoopSolve<T, 4>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, st);
+  return launchCoopSolve<T, 16>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, st);
+}
+
+template cudaError_t launch_solve_coop<double>(bool, const int*, int, int, const FrontDev*,
+                                               const double*, const int*, double*, int64_t, int,
+                                               double*, const int64_t*, cudaStream_t);
+template cudaError_t launch_solve_coop<float>(bool, const int*, int, int, const FrontDev*,
+                                              const float*, const int*, float*, int64_t, int, float*,
+                                              const int64_t*, cudaStream_t);
+
+}  // namespace mfgpu

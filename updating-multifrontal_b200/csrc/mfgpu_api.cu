@@ -63,27 +63,32 @@ struct Plan {
     int64_t f0 = 0, nf = 0, s0 = 0, ns = 0;  // offsets into the id list
     int maxN = 0, maxn = 0;
     Group ftask, sbase, sadd0, sadd1;
+    int64_t cpref0 = 0;   // offset of the cooperative kernel's phase prefixes in cpref
   };
   std::vector<Level> lv;
   std::vector<Task> tasks;
   std::vector<int64_t> pref;
   std::vector<int> ids;
+  std::vector<int> cpref;
   int nfronts = 0;
   double flops = 0;
   // device copies
   Task* d_tasks = nullptr;
   int64_t* d_pref = nullptr;
   int* d_ids = nullptr;
-  size_t cap_tasks = 0, cap_pref = 0, cap_ids = 0;
+  int* d_cpref = nullptr;
+  size_t cap_tasks = 0, cap_pref = 0, cap_ids = 0, cap_cpref = 0;
 
   void release() {
     cudaFree(d_tasks);
     cudaFree(d_pref);
     cudaFree(d_ids);
+    cudaFree(d_cpref);
     d_tasks = nullptr;
     d_pref = nullptr;
     d_ids = nullptr;
-    cap_tasks = cap_pref = cap_ids = 0;
+    d_cpref = nullptr;
+    cap_tasks = cap_pref = cap_ids = cap_cpref = 0;
   }
 
   Group addGroup(const std::vector<Task>& src, const std::vector<int64_t>& ptr,
@@ -127,6 +132,7 @@ struct Plan {
     grow(d_tasks, cap_tasks, tasks.size(), "alloc plan tasks");
     grow(d_pref, cap_pref, pref.size(), "alloc plan prefixes");
     grow(d_ids, cap_ids, ids.size(), "alloc plan ids");
+    grow(d_cpref, cap_cpref, cpref.size(), "alloc plan phase prefixes");
     if (!tasks.empty())
       ck(cudaMemcpyAsync(d_tasks, tasks.data(), tasks.size() * sizeof(Task), cudaMemcpyHostToDevice, st),
          "upload tasks");
@@ -136,6 +142,10 @@ struct Plan {
     if (!ids.empty())
       ck(cudaMemcpyAsync(d_ids, ids.data(), ids.size() * sizeof(int), cudaMemcpyHostToDevice, st),
          "upload ids");
+    if (!cpref.empty())
+      ck(cudaMemcpyAsync(d_cpref, cpref.data(), cpref.size() * sizeof(int), cudaMemcpyHostToDevice,
+                         st),
+         "upload phase prefixes");
     // host vectors must outlive the async copies
     ck(cudaStreamSynchronize(st), "plan upload");
   }
@@ -215,8 +225,8 @@ struct mfgpu_handle {
   int64_t nnz = 0;
   std::vector<int> h_rowptr, h_colind;
 
-  double* d_F = nullptr;
-  double* d_Sep = nullptr;
+  void* d_F = nullptr;             // front arena (double or float)
+  void* d_Sep = nullptr;           // separator arena (double or float)
   double* d_val = nullptr;
   int* d_rp = nullptr;
   int* d_ci = nullptr;
@@ -225,12 +235,29 @@ struct mfgpu_handle {
   SepDev* d_sp = nullptr;
   int64_t* d_woff = nullptr;
   DevError* d_err = nullptr;
-  double* d_slots = nullptr;   // diagonal-block hand-off slots of the cooperative kernel
-  double* d_W = nullptr;
+  void* d_slots = nullptr;     // diagonal-block hand-off slots of the cooperative kernel
+  // solve workspaces (d_Wd / d_Td hold elements of the factor's precision)
+  double* d_Wd = nullptr;
   size_t capW = 0;
   double* d_X = nullptr;
-  double* d_T = nullptr;
   size_t capX = 0;
+  double* d_Td = nullptr;
+  size_t capT = 0;
+  // mixed precision: scaling and refinement buffers
+  bool mixed = false;
+  int tcMinN = 4096;               // mixed: smallest level maxN run on the tensor cores (0 = never)
+  int tcSplit = 3;                 // mixed: 3 = three-term TF32 products, 1 = plain TF32
+  size_t esz = sizeof(double);     // bytes per factor element
+  double* d_scale = nullptr;       // s = 1/sqrt(diag(A)) of the last full factorization
+  double* d_iscale = nullptr;      // 1/s
+  double *d_B = nullptr, *d_R = nullptr, *d_P = nullptr, *d_Q = nullptr, *d_Z = nullptr;
+  size_t capB = 0, capR = 0, capP = 0, capQ = 0, capZ = 0;
+  float* d_x32 = nullptr;
+  size_t cap32 = 0;
+  double* d_dotp = nullptr;
+  size_t capDot = 0;
+  double* d_sc = nullptr;          // refinement scalars
+  int* d_active = nullptr;         // refinement: columns still iterating
   int* d_all = nullptr;      // every front id then every separator id, level order
   int64_t woffTotal = 0;     // sum over fronts of 2N
   Plan full, upd;
@@ -238,6 +265,8 @@ struct mfgpu_handle {
   int64_t device_bytes = 0;
   Profiler prof;
   std::vector<int> lvMaxN;   // largest front (n + m) per level
+  std::vector<int> lvMaxn;   // largest pivot count per level
+  int solveCoopMinN = 1024;  // levels with a front this large use the cooperative sweeps
   bool stepped = false;      // MFGPU_STEPPED=1: per-step launches instead of the cooperative kernel
 
   ~mfgpu_handle() {
@@ -255,9 +284,20 @@ struct mfgpu_handle {
     cudaFree(d_woff);
     cudaFree(d_err);
     cudaFree(d_slots);
-    cudaFree(d_W);
+    cudaFree(d_Wd);
     cudaFree(d_X);
-    cudaFree(d_T);
+    cudaFree(d_Td);
+    cudaFree(d_scale);
+    cudaFree(d_iscale);
+    cudaFree(d_B);
+    cudaFree(d_R);
+    cudaFree(d_P);
+    cudaFree(d_Q);
+    cudaFree(d_Z);
+    cudaFree(d_x32);
+    cudaFree(d_dotp);
+    cudaFree(d_sc);
+    cudaFree(d_active);
     cudaFree(d_all);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -272,6 +312,7 @@ struct mfgpu_handle {
     P.tasks.clear();
     P.pref.clear();
     P.ids.clear();
+    P.cpref.clear();
     P.nfronts = 0;
     P.flops = 0;
     for (int ell = s.levels - 1; ell >= 0; ell--) {
@@ -302,14 +343,26 @@ struct mfgpu_handle {
       L.sbase = P.addGroup(s.sep_tasks, s.sep_task_ptr, sl, -1);
       L.sadd0 = P.addGroup(s.sep_add_tasks, s.sep_task_ptr, sl, 0);
       L.sadd1 = P.addGroup(s.sep_add_tasks, s.sep_task_ptr, sl, 1);
+      L.cpref0 = (int64_t)P.cpref.size();
+      if (!fl.empty() && !mfgpu::small_front_fits(L.maxN, (int)esz) && mfgpu::coop_fits((int)fl.size())) {
+        std::vector<int> nn, NN;
+        for (int f : fl) {
+          nn.push_back(s.fronts[f].n);
+          NN.push_back(s.fronts[f].N);
+        }
+        std::vector<int> pp = mfgpu::coop_phase_prefix(nn, NN, L.maxn);
+        P.cpref.insert(P.cpref.end(), pp.begin(), pp.end());
+      }
     }
   }
 
+  template <class T>
   void runGroup(const Plan& P, const Group& g, int64_t bytes) {
     if (g.ntasks == 0 || g.ntiles == 0) return;
     prof.begin(MFGPU_KC_ASSEMBLE, stream);
-    mfgpu::launch_tasks(P.d_tasks + g.task0, P.d_pref + g.pref0, (int)g.ntasks, g.ntiles, d_F, d_Sep,
-                        d_rp, d_ci, d_val, d_dofs, stream);
+    mfgpu::launch_tasks<T>(P.d_tasks + g.task0, P.d_pref + g.pref0, (int)g.ntasks, g.ntiles,
+                           (T*)d_F, (T*)d_Sep, d_rp, d_ci, d_val, d_dofs, mixed ? d_scale : nullptr,
+                           stream);
     ck(cudaGetLastError(), "launch assembly (k_tasks)");
     prof.end(stream);
     if (prof.on) prof.bytes[MFGPU_KC_ASSEMBLE] += (double)bytes;
@@ -324,77 +377,131 @@ struct mfgpu_handle {
       const Task& T = P.tasks[t];
       int64_t e = T.lower ? (int64_t)T.rows * (T.rows + 1) / 2 : (int64_t)T.rows * T.cols;
       int mult = T.kind == mfgpu::TK_ZERO ? 1 : T.kind == mfgpu::TK_ADD ? 3 : 2;
-      b += e * 8 * mult;
+      b += e * (int64_t)esz * mult;
     }
     return b;
   }
 
   // Run a factorization plan: per level, separator base assembly, front
   // assembly, partial Cholesky, separator accumulation (src/DE/mf2d.cpp:449-753).
-  void runPlan(const Plan& P) {
+  template <class T>
+  void runPlanT(const Plan& P) {
     const Schedule& s = *S;
+    T* F = (T*)d_F;
     ck(cudaMemsetAsync(d_err, 0, sizeof(DevError), stream), "clear error word");
     for (int ell = s.levels - 1; ell >= 0; ell--) {
       const Plan::Level& L = P.lv[ell];
       prof.level = ell;
-      runGroup(P, L.sbase, groupBytes(P, L.sbase));
-      runGroup(P, L.ftask, groupBytes(P, L.ftask));
-      if (L.nf > 0 && mfgpu::small_front_fits(L.maxN)) {
+      runGroup<T>(P, L.sbase, groupBytes(P, L.sbase));
+      runGroup<T>(P, L.ftask, groupBytes(P, L.ftask));
+      const bool fused = L.nf > 0 && mfgpu::small_front_fits(L.maxN, (int)sizeof(T));
+      const bool coop = L.nf > 0 && !fused && mfgpu::coop_fits((int)L.nf) &&
+                        (!stepped || sizeof(T) != sizeof(double));
+      if (fused || coop) {
         if (prof.on)
           for (int64_t i = L.f0; i < L.f0 + L.nf; i++)
             prof.flops[MFGPU_KC_FRONT] += s.front_flops(s.fronts[P.ids[i]]);
         prof.begin(MFGPU_KC_FRONT, stream);
-        mfgpu::launch_front_small(P.d_ids + L.f0, (int)L.nf, L.maxN, d_fr, d_F, d_err, stream);
-        ck(cudaGetLastError(), "launch fused front factorization (k_front_small)");
-        prof.end(stream);
-      } else if (L.nf > 0 && mfgpu::coop_fits((int)L.nf) && !stepped) {
-        if (prof.on)
-          for (int64_t i = L.f0; i < L.f0 + L.nf; i++)
-            prof.flops[MFGPU_KC_FRONT] += s.front_flops(s.fronts[P.ids[i]]);
-        prof.begin(MFGPU_KC_FRONT, stream);
-        ck(mfgpu::launch_level_coop(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, d_F, d_err, d_slots,
-                                    stream),
-           "launch cooperative level factorization (k_level_coop)");
+        if (fused) {
+          mfgpu::launch_front_small<T>(P.d_ids + L.f0, (int)L.nf, L.maxN, d_fr, F, d_err, stream);
+          ck(cudaGetLastError(), "launch fused front factorization (k_front_small)");
+        } else if (sizeof(T) == sizeof(float) && tcLevel(L)) {
+          runTensorLevel(P, L);
+        } else {
+          ck(mfgpu::launch_level_coop<T>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, F, d_err,
+                                         (T*)d_slots, P.d_cpref + L.cpref0, stream),
+             "launch cooperative level factorization (k_level_coop)");
+        }
         prof.end(stream);
       } else if (L.nf > 0) {
-        const int* fl = P.d_ids + L.f0;
-        for (int k = 0; k < L.maxn; k += mfgpu::kPanel) {
-          if (prof.on) {
-            for (int64_t i = L.f0; i < L.f0 + L.nf; i++) {
-              const mfgpu::Front& f = s.fronts[P.ids[i]];
-              if (k >= f.n) continue;
-              double kb = std::min(mfgpu::kPanel, f.n - k), M = f.N - k - kb;
-              prof.flops[MFGPU_KC_POTRF] += kb * kb * kb / 3.0;
-              prof.flops[MFGPU_KC_TRSM] += M * kb * kb;
-              prof.flops[MFGPU_KC_SYRK] += M * M * kb;
-            }
-          }
-          prof.begin(MFGPU_KC_POTRF, stream);
-          mfgpu::launch_potrf(fl, (int)L.nf, d_fr, d_F, k, d_err, stream);
-          ck(cudaGetLastError(), "launch panel Cholesky (k_potrf)");
-          prof.end(stream);
-          prof.begin(MFGPU_KC_TRSM, stream);
-          mfgpu::launch_trsm(fl, (int)L.nf, d_fr, d_F, k, L.maxN, stream);
-          ck(cudaGetLastError(), "launch panel solve (k_trsm)");
-          prof.end(stream);
-          prof.begin(MFGPU_KC_SYRK, stream);
-          mfgpu::launch_syrk(fl, (int)L.nf, d_fr, d_F, k, L.maxN, stream);
-          ck(cudaGetLastError(), "launch trailing update (k_syrk)");
-          prof.end(stream);
-        }
+        if (sizeof(T) != sizeof(double))
+          throw CudaError("no single-precision path for this level", MFGPU_ERR_ARG);
+        runStepped(P, L);
       }
-      runGroup(P, L.sadd0, groupBytes(P, L.sadd0));
-      runGroup(P, L.sadd1, groupBytes(P, L.sadd1));
+      runGroup<T>(P, L.sadd0, groupBytes(P, L.sadd0));
+      runGroup<T>(P, L.sadd1, groupBytes(P, L.sadd1));
     }
     ck(cudaGetLastError(), "factor launch");
   }
 
-  // Replace the matrix values (same pattern) and refactor a plan.
-  void factorWith(const double* val, bool device, const Plan& P) {
+  // Mixed path: levels of large fronts run the cooperative kernel one outer
+  // panel at a time (diagonal blocks, panel solves and in-panel updates) and
+  // the trailing update of each panel on the tensor cores.
+  bool tcLevel(const Plan::Level& L) const {
+    return tcMinN > 0 && L.maxN >= tcMinN && L.nf <= mfgpu::tc_max_fronts();
+  }
+
+  void runTensorLevel(const Plan& P, const Plan::Level& L) {
+    const Schedule& s = *S;
+    std::vector<int> nn(L.nf), NN(L.nf);
+    for (int64_t i = 0; i < L.nf; i++) {
+      nn[i] = s.fronts[P.ids[L.f0 + i]].n;
+      NN[i] = s.fronts[P.ids[L.f0 + i]].N;
+    }
+    const int outer = mfgpu::coop_outer();
+    int phase0 = 0;
+    for (int K = 0; K < L.maxn; K += outer) {
+      ck(mfgpu::launch_level_coop<float>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, (float*)d_F,
+                                         d_err, (float*)d_slots, P.d_cpref + L.cpref0, stream, K,
+                                         K + outer, phase0, 0),
+         "launch cooperative panel factorization (k_level_coop)");
+      phase0 += mfgpu::coop_phases(K, L.maxn);
+      const int64_t nt = mfgpu::tc_tiles(nn, NN, K);
+      ck(mfgpu::launch_trail_tc(P.d_ids + L.f0, (int)L.nf, nt, d_fr, (float*)d_F, K, tcSplit, d_err,
+                                stream),
+         "launch tensor-core trailing update (k_trail_tc)");
+    }
+  }
+
+  // FP64 per-step launches (MFGPU_STEPPED=1, or levels no cooperative launch takes).
+  void runStepped(const Plan& P, const Plan::Level& L) {
+    const Schedule& s = *S;
+    double* F = (double*)d_F;
+    const int* fl = P.d_ids + L.f0;
+    for (int k = 0; k < L.maxn; k += mfgpu::kPanel) {
+      if (prof.on) {
+        for (int64_t i = L.f0; i < L.f0 + L.nf; i++) {
+          const mfgpu::Front& f = s.fronts[P.ids[i]];
+          if (k >= f.n) continue;
+          double kb = std::min(mfgpu::kPanel, f.n - k), M = f.N - k - kb;
+          prof.flops[MFGPU_KC_POTRF] += kb * kb * kb / 3.0;
+          prof.flops[MFGPU_KC_TRSM] += M * kb * kb;
+          prof.flops[MFGPU_KC_SYRK] += M * M * kb;
+        }
+      }
+      prof.begin(MFGPU_KC_POTRF, stream);
+      mfgpu::launch_potrf(fl, (int)L.nf, d_fr, F, k, d_err, stream);
+      ck(cudaGetLastError(), "launch panel Cholesky (k_potrf)");
+      prof.end(stream);
+      prof.begin(MFGPU_KC_TRSM, stream);
+      mfgpu::launch_trsm(fl, (int)L.nf, d_fr, F, k, L.maxN, stream);
+      ck(cudaGetLastError(), "launch panel solve (k_trsm)");
+      prof.end(stream);
+      prof.begin(MFGPU_KC_SYRK, stream);
+      mfgpu::launch_syrk(fl, (int)L.nf, d_fr, F, k, L.maxN, stream);
+      ck(cudaGetLastError(), "launch trailing update (k_syrk)");
+      prof.end(stream);
+    }
+  }
+
+  void runPlan(const Plan& P) {
+    if (mixed) runPlanT<float>(P);
+    else runPlanT<double>(P);
+  }
+
+  // Replace the matrix values (same pattern) and refactor a plan.  The mixed
+  // path's diagonal scaling is recomputed only with a full factorization and
+  // kept through localized updates, so fronts that an update leaves alone stay
+  // consistent with the ones it recomputes.
+  void factorWith(const double* val, bool device, const Plan& P, bool full) {
     if (val)
       ck(cudaMemcpyAsync(d_val, val, nnz * sizeof(double),
                          device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream),
          "upload values");
+    if (mixed && full) {
+      mfgpu::launch_diag_scale(d_rp, d_ci, d_val, n, d_scale, d_iscale, stream);
+      ck(cudaGetLastError(), "launch diagonal scaling");
+    }
     runPlan(P);
   }
 
@@ -413,26 +520,32 @@ struct mfgpu_handle {
     }
   }
 
+  // ---- solve / apply buffers ----
+  template <class P>
+  void growBuf(P*& p, size_t& cap, size_t need, const char* what) {
+    if (need <= cap) return;
+    cudaFree(p);
+    p = nullptr;
+    p = dalloc<P>(need, what);
+    cap = need;
+  }
+
   void ensureWork(int nrhs) {
-    size_t needW = (size_t)woffTotal * nrhs;
-    if (needW > capW) {
-      cudaFree(d_W);
-      d_W = nullptr;
-      d_W = dalloc<double>(needW, "alloc solve workspace");
-      capW = needW;
-    }
-    size_t needX = (size_t)n * nrhs;
-    if (needX > capX) {
-      cudaFree(d_X);
-      cudaFree(d_T);
-      d_X = d_T = nullptr;
-      d_X = dalloc<double>(needX, "alloc rhs buffer");
-      d_T = dalloc<double>(needX, "alloc apply buffer");
-      capX = needX;
+    growBuf(d_Wd, capW, (size_t)woffTotal * nrhs * esz / sizeof(double) + 1, "alloc solve workspace");
+    growBuf(d_X, capX, (size_t)n * nrhs, "alloc rhs buffer");
+    growBuf(d_Td, capT, (size_t)n * nrhs * esz / sizeof(double) + 1, "alloc apply buffer");
+    if (mixed) {
+      const size_t v = (size_t)n * nrhs;
+      growBuf(d_B, capB, v, "alloc refinement buffer");
+      growBuf(d_R, capR, v, "alloc refinement buffer");
+      growBuf(d_P, capP, v, "alloc refinement buffer");
+      growBuf(d_Q, capQ, v, "alloc refinement buffer");
+      growBuf(d_Z, capZ, v, "alloc refinement buffer");
+      growBuf(d_x32, cap32, v, "alloc refinement buffer");
+      growBuf(d_dotp, capDot, mfgpu::dot_scratch_elems(nrhs), "alloc dot scratch");
     }
   }
 
-  // Solve in place on device data X (n x nrhs, ld = ldx), nrhs <= 16.
   // MFGPU_VERBOSE: per-level marks inside the solve (class SOLVE, level tag).
   void vmark(bool begin, int level) {
     if (!prof.verbose) return;
@@ -444,71 +557,201 @@ struct mfgpu_handle {
     }
   }
 
-  void solveChunk(double* X, int64_t ldx, int nrhs) {
+  // Forward / backward sweeps of the factorization in precision T, in place on
+  // X (n x nrhs, ld ldx, nrhs <= 16) with per-front workspace W
+  // (src/DE/mf2d.cpp:976-1054).
+  bool coopSweep(int ell) const {
+    return solveCoopMinN > 0 && lvMaxN[ell] >= solveCoopMinN &&
+           S->lv[ell].nbox <= mfgpu::solve_coop_max_fronts();
+  }
+
+  template <class T>
+  void sweepLevel(bool forward, int ell, T* X, int64_t ldx, int nrhs, T* W) {
     const Schedule& s = *S;
-    for (int ell = s.levels - 1; ell >= 1; ell--) {
-      const int f0 = s.lv[ell].front0, s0 = s.lv[ell].sep0;
-      vmark(true, ell);
-      mfgpu::launch_solve_fwd(d_all + f0, s.lv[ell].nbox, lvMaxN[ell], d_fr, d_F, d_dofs, X, ldx, nrhs, d_W,
-                              d_woff, stream);
-      vmark(false, ell);
+    const T* F = (const T*)d_F;
+    const int* fl = d_all + s.lv[ell].front0;
+    const int nf = s.lv[ell].nbox;
+    if (coopSweep(ell)) {
+      ck(mfgpu::launch_solve_coop<T>(forward, fl, nf, lvMaxn[ell], d_fr, F, d_dofs, X, ldx, nrhs, W,
+                                     d_woff, stream),
+         forward ? "launch cooperative forward sweep (k_solve_coop_fwd)"
+                 : "launch cooperative backward sweep (k_solve_coop_bwd)");
+    } else if (forward) {
+      mfgpu::launch_solve_fwd<T>(fl, nf, lvMaxN[ell], d_fr, F, d_dofs, X, ldx, nrhs, W, d_woff,
+                                 stream);
       ck(cudaGetLastError(), "launch forward sweep (k_solve_fwd)");
-      mfgpu::launch_sep_gather(d_all + s.fronts.size() + s0, s.lv[ell].nsep, d_sp, d_dofs, X, ldx,
-                               nrhs, d_W, d_woff, d_fr, stream);
+    } else {
+      mfgpu::launch_solve_bwd<T>(fl, nf, lvMaxN[ell], d_fr, F, d_dofs, X, ldx, nrhs, W, d_woff,
+                                 stream);
+      ck(cudaGetLastError(), "launch backward sweep (k_solve_bwd)");
+    }
+  }
+
+  // Forward / backward sweeps of the factorization in precision T, in place on
+  // X (n x nrhs, ld ldx, nrhs <= 16) with per-front workspace W
+  // (src/DE/mf2d.cpp:976-1054).
+  template <class T>
+  void sweeps(T* X, int64_t ldx, int nrhs, T* W) {
+    const Schedule& s = *S;
+    const T* F = (const T*)d_F;
+    for (int ell = s.levels - 1; ell >= 1; ell--) {
+      const int s0 = s.lv[ell].sep0;
+      vmark(true, ell);
+      sweepLevel<T>(true, ell, X, ldx, nrhs, W);
+      vmark(false, ell);
+      mfgpu::launch_sep_gather<T>(d_all + s.fronts.size() + s0, s.lv[ell].nsep, d_sp, d_dofs, X, ldx,
+                                  nrhs, W, d_woff, d_fr, stream);
       ck(cudaGetLastError(), "launch separator gather (k_sep_gather)");
     }
     vmark(true, 0);
-    mfgpu::launch_root_solve(0, s.fronts[0].N, d_fr, d_F, d_dofs, X, ldx, nrhs, d_W, d_woff, stream);
+    if (coopSweep(0)) {
+      sweepLevel<T>(true, 0, X, ldx, nrhs, W);
+      sweepLevel<T>(false, 0, X, ldx, nrhs, W);
+    } else {
+      mfgpu::launch_root_solve<T>(0, s.fronts[0].N, d_fr, F, d_dofs, X, ldx, nrhs, W, d_woff, stream);
+      ck(cudaGetLastError(), "launch root solve (k_root_solve)");
+    }
     vmark(false, 0);
-    ck(cudaGetLastError(), "launch root solve (k_root_solve)");
     for (int ell = 1; ell < s.levels; ell++) {
       vmark(true, 100 + ell);
-      mfgpu::launch_solve_bwd(d_all + s.lv[ell].front0, s.lv[ell].nbox, lvMaxN[ell], d_fr, d_F, d_dofs, X, ldx,
-                              nrhs, d_W, d_woff, stream);
+      sweepLevel<T>(false, ell, X, ldx, nrhs, W);
       vmark(false, 100 + ell);
-      ck(cudaGetLastError(), "launch backward sweep (k_solve_bwd)");
     }
-    ck(cudaGetLastError(), "solve launch");
   }
 
-  // The same sweeps as solveChunk, with the per-front workspace at W (used
-  // by the no-allocation entry point, which passes its static scratch).
-  void solveChunkScratch(double* X, int64_t ldx, int nrhs, double* W) {
+  // Factored-operator application in precision T (src/DE/mf2d.cpp:904-974).
+  template <class T>
+  void applySweeps(T* X, int64_t ldx, int nrhs, T* W, T* Tb) {
     const Schedule& s = *S;
+    const T* F = (const T*)d_F;
     for (int ell = s.levels - 1; ell >= 1; ell--) {
-      const int f0 = s.lv[ell].front0, s0 = s.lv[ell].sep0;
-      mfgpu::launch_solve_fwd(d_all + f0, s.lv[ell].nbox, lvMaxN[ell], d_fr, d_F, d_dofs, X, ldx, nrhs, W,
-                              d_woff, stream);
-      ck(cudaGetLastError(), "launch forward sweep (k_solve_fwd)");
-      mfgpu::launch_sep_gather(d_all + s.fronts.size() + s0, s.lv[ell].nsep, d_sp, d_dofs, X, ldx,
-                               nrhs, W, d_woff, d_fr, stream);
-      ck(cudaGetLastError(), "launch separator gather (k_sep_gather)");
-    }
-    mfgpu::launch_root_solve(0, s.fronts[0].N, d_fr, d_F, d_dofs, X, ldx, nrhs, W, d_woff, stream);
-    ck(cudaGetLastError(), "launch root solve (k_root_solve)");
-    for (int ell = 1; ell < s.levels; ell++) {
-      mfgpu::launch_solve_bwd(d_all + s.lv[ell].front0, s.lv[ell].nbox, lvMaxN[ell], d_fr, d_F, d_dofs, X, ldx,
-                              nrhs, W, d_woff, stream);
-      ck(cudaGetLastError(), "launch backward sweep (k_solve_bwd)");
-    }
-    ck(cudaGetLastError(), "solve launch");
-  }
-
-  void applyChunk(double* X, int64_t ldx, int nrhs) {
-    const Schedule& s = *S;
-    for (int ell = s.levels - 1; ell >= 1; ell--)
-      mfgpu::launch_apply_up(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, d_F, d_dofs, X, ldx,
-                             nrhs, d_W, d_woff, d_T, stream);
+      mfgpu::launch_apply_up<T>(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, F, d_dofs, X, ldx,
+                                nrhs, W, d_woff, Tb, stream);
       ck(cudaGetLastError(), "launch apply up (k_apply_up)");
-    mfgpu::launch_root_apply(0, d_fr, d_F, d_dofs, X, ldx, nrhs, d_W, d_woff, stream);
+    }
+    mfgpu::launch_root_apply<T>(0, d_fr, F, d_dofs, X, ldx, nrhs, W, d_woff, stream);
     ck(cudaGetLastError(), "launch root apply (k_root_apply)");
     for (int ell = 1; ell < s.levels; ell++) {
-      mfgpu::launch_apply_down(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, d_F, d_dofs, ldx,
-                               nrhs, d_W, d_woff, d_T, stream);
+      mfgpu::launch_apply_down<T>(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, F, d_dofs, ldx,
+                                  nrhs, W, d_woff, Tb, stream);
       ck(cudaGetLastError(), "launch apply down (k_apply_down)");
-      mfgpu::launch_sep_gather(d_all + s.fronts.size() + s.lv[ell].sep0, s.lv[ell].nsep, d_sp, d_dofs,
-                               X, ldx, nrhs, d_W, d_woff, d_fr, stream);
+      mfgpu::launch_sep_gather<T>(d_all + s.fronts.size() + s.lv[ell].sep0, s.lv[ell].nsep, d_sp,
+                                  d_dofs, X, ldx, nrhs, W, d_woff, d_fr, stream);
       ck(cudaGetLastError(), "launch separator gather (k_sep_gather)");
+    }
+  }
+
+  // z = M^{-1} r with the scaled FP32 factorization: z = s .* (S^{-1} (s .* r)).
+  void precond(const double* r, double* z, int nc) {
+    mfgpu::launch_scale_to<float>(r, n, d_x32, n, d_scale, n, nc, stream);
+    sweeps<float>(d_x32, n, nc, (float*)d_Wd);
+    mfgpu::launch_scale_from<float>(d_x32, n, z, n, d_scale, n, nc, stream);
+  }
+
+  void dots(const double* x, const double* y, int nc, double* out) {
+    mfgpu::launch_dot(x, n, y, n, n, nc, d_dotp, out, stream);
+  }
+
+  // Mixed precision: conjugate gradients on A x = b in FP64 (residuals from the
+  // FP64 CSR matrix), preconditioned by the FP32 factorization, until
+  // ||b - A x|| <= tol ||b|| for every column.  XB holds b on entry, x on exit
+  // (n x nc, ld n).
+  void pcg(double* XB, int nc) {
+    const double tol = opt.refine_tol > 0 ? opt.refine_tol : 1e-10;
+    const int maxit = opt.refine_maxit > 0 ? opt.refine_maxit : 50;
+    const size_t vb = (size_t)n * nc * sizeof(double);
+    double* sc = d_sc;   // rz_a | rz_b | pq | rr | bb, 16 each
+    double* rzA = sc;
+    double* rzB = sc + 16;
+    double* pq = sc + 32;
+    double* rr = sc + 48;
+    double* bb = sc + 64;
+    ck(cudaMemcpyAsync(d_B, XB, vb, cudaMemcpyDeviceToDevice, stream), "copy rhs");
+    dots(d_B, d_B, nc, bb);
+    precond(d_B, XB, nc);   // x0 = M^{-1} b
+    mfgpu::launch_residual(d_rp, d_ci, d_val, n, d_B, n, XB, n, d_R, n, nc, stream);
+    double hb[16], hr[16];
+    int act[16];
+    ck(cudaMemcpyAsync(hb, bb, nc * sizeof(double), cudaMemcpyDeviceToHost, stream), "read norms");
+    int it = 0, restarts = 0;
+    bool first = true;
+    double worst = 0;
+    while (true) {
+      dots(d_R, d_R, nc, rr);
+      ck(cudaMemcpyAsync(hr, rr, nc * sizeof(double), cudaMemcpyDeviceToHost, stream), "read norms");
+      ck(cudaStreamSynchronize(stream), "refinement");
+      int nact = 0;
+      worst = 0;
+      for (int c = 0; c < nc; c++) {
+        const double rel = hb[c] > 0 ? std::sqrt(hr[c] / hb[c]) : std::sqrt(hr[c]);
+        worst = std::max(worst, rel);
+        act[c] = rel > tol;
+        nact += act[c];
+      }
+      if (nact == 0) {
+        // confirm with the true residual; restart from it if the recursive one drifted
+        mfgpu::launch_residual(d_rp, d_ci, d_val, n, d_B, n, XB, n, d_R, n, nc, stream);
+        dots(d_R, d_R, nc, rr);
+        ck(cudaMemcpyAsync(hr, rr, nc * sizeof(double), cudaMemcpyDeviceToHost, stream), "read norms");
+        ck(cudaStreamSynchronize(stream), "refinement");
+        worst = 0;
+        for (int c = 0; c < nc; c++) {
+          const double rel = hb[c] > 0 ? std::sqrt(hr[c] / hb[c]) : std::sqrt(hr[c]);
+          worst = std::max(worst, rel);
+          act[c] = rel > tol;
+          nact += act[c];
+        }
+        if (nact == 0 || restarts >= 3) break;
+        restarts++;
+        first = true;
+      }
+      if (it >= maxit) break;
+      ck(cudaMemcpyAsync(d_active, act, nc * sizeof(int), cudaMemcpyHostToDevice, stream), "flags");
+      precond(d_R, d_Z, nc);
+      dots(d_R, d_Z, nc, rzB);
+      mfgpu::launch_pcg_p(d_P, d_Z, n, n, nc, rzB, rzA, d_active, first ? 1 : 0, stream);
+      mfgpu::launch_spmv(d_rp, d_ci, d_val, n, d_P, n, d_Q, n, nc, stream);
+      dots(d_P, d_Q, nc, pq);
+      mfgpu::launch_pcg_xr(XB, d_R, d_P, d_Q, n, n, nc, rzB, pq, d_active, stream);
+      ck(cudaGetLastError(), "refinement launch");
+      std::swap(rzA, rzB);   // rz of this iteration becomes the previous one
+      first = false;
+      it++;
+    }
+    stats.iterations = std::max(stats.iterations, it);
+    stats.residual = std::max(stats.residual, worst);
+    if (worst > tol) {
+      char buf[160];
+      snprintf(buf, sizeof buf,
+               "refinement stopped after %d iterations at relative residual %.3e (target %.1e)", it,
+               worst, tol);
+      throw CudaError(buf, MFGPU_ERR_NOT_CONVERGED);
+    }
+  }
+
+  // Solve in place on device data X (n x nrhs, ld = n), nrhs <= 16.
+  void solveChunk(double* X, int nrhs) {
+    if (mixed) pcg(X, nrhs);
+    else sweeps<double>(X, n, nrhs, (double*)d_Wd);
+    ck(cudaGetLastError(), "solve launch");
+  }
+
+  // The FP64 sweeps with the per-front workspace at W (used by the
+  // no-allocation entry point, which passes its static scratch).
+  void solveChunkScratch(double* X, int64_t ldx, int nrhs, double* W) {
+    sweeps<double>(X, ldx, nrhs, W);
+    ck(cudaGetLastError(), "solve launch");
+  }
+
+  // b = (factored A) x in place on X (n x nrhs, ld n).  The mixed path applies
+  // the scaled FP32 factorization: A ~ D^{1/2} L L^T D^{1/2}, D^{1/2} = 1/s.
+  void applyChunk(double* X, int nrhs) {
+    if (!mixed) {
+      applySweeps<double>(X, n, nrhs, (double*)d_Wd, (double*)d_Td);
+    } else {
+      mfgpu::launch_scale_to<float>(X, n, d_x32, n, d_iscale, n, nrhs, stream);
+      applySweeps<float>(d_x32, n, nrhs, (float*)d_Wd, (float*)d_Td);
+      mfgpu::launch_scale_from<float>(d_x32, n, X, n, d_iscale, n, nrhs, stream);
     }
     ck(cudaGetLastError(), "apply launch");
   }
@@ -591,6 +834,10 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n
   mfgpu_default_options(&h->opt);
   if (opts) h->opt = *opts;
   h->device = h->opt.device;
+  if (h->opt.precision != MFGPU_FP64 && h->opt.precision != MFGPU_MIXED) {
+    g_create_error = "unknown precision";
+    return MFGPU_ERR_ARG;
+  }
   try {
     h->S.reset(new Schedule(dim, nx, ny, nz, width, max_side));
   } catch (const std::invalid_argument& e) {
@@ -610,6 +857,9 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n
   h->nnz = row_ptr[n];
   if (const char* e = getenv("MFGPU_STEPPED")) h->stepped = e[0] == '1';
   if (const char* e = getenv("MFGPU_VERBOSE")) h->prof.verbose = e[0] == '1';
+  if (const char* e = getenv("MFGPU_TC_MIN_N")) h->tcMinN = atoi(e);
+  if (const char* e = getenv("MFGPU_SOLVE_COOP_MIN_N")) h->solveCoopMinN = atoi(e);
+  if (const char* e = getenv("MFGPU_TC_SPLIT")) h->tcSplit = atoi(e) == 1 ? 1 : 3;
   h->h_rowptr.assign(row_ptr, row_ptr + n + 1);
   h->h_colind.assign(col_ind, col_ind + h->nnz);
   int st = guarded(h.get(), [&]() {
@@ -618,8 +868,16 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n
     H.stream = H.own;
     ck(cudaEventCreate(&H.ev0), "event");
     ck(cudaEventCreate(&H.ev1), "event");
-    H.d_F = dalloc<double>(s.front_elems, "alloc front arena");
-    H.d_Sep = dalloc<double>(s.sep_elems, "alloc separator arena");
+    H.mixed = H.opt.precision == MFGPU_MIXED;
+    H.esz = H.mixed ? sizeof(float) : sizeof(double);
+    H.d_F = dalloc<unsigned char>(s.front_elems * H.esz, "alloc front arena");
+    H.d_Sep = dalloc<unsigned char>(s.sep_elems * H.esz, "alloc separator arena");
+    if (H.mixed) {
+      H.d_scale = dalloc<double>(n, "alloc scaling");
+      H.d_iscale = dalloc<double>(n, "alloc scaling");
+      H.d_sc = dalloc<double>(80, "alloc refinement scalars");
+      H.d_active = dalloc<int>(16, "alloc refinement flags");
+    }
     H.d_val = dalloc<double>(H.nnz, "alloc CSR values");
     H.d_rp = dalloc<int>(n + 1, "alloc CSR rows");
     H.d_ci = dalloc<int>(H.nnz, "alloc CSR cols");
@@ -633,7 +891,11 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n
     }
     H.woffTotal = woff.back();
     H.lvMaxN.assign(s.levels, 0);
-    for (const mfgpu::Front& f : s.fronts) H.lvMaxN[f.level] = std::max(H.lvMaxN[f.level], f.N);
+    H.lvMaxn.assign(s.levels, 0);
+    for (const mfgpu::Front& f : s.fronts) {
+      H.lvMaxN[f.level] = std::max(H.lvMaxN[f.level], f.N);
+      H.lvMaxn[f.level] = std::max(H.lvMaxn[f.level], f.n);
+    }
     std::vector<SepDev> sp(s.seps.size());
     for (size_t i = 0; i < s.seps.size(); i++) {
       const mfgpu::Sep& e = s.seps[i];
@@ -646,7 +908,7 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n
     H.d_sp = dalloc<SepDev>(std::max<size_t>(1, sp.size()), "alloc seps");
     H.d_woff = dalloc<int64_t>(woff.size(), "alloc woff");
     H.d_err = dalloc<DevError>(1, "alloc error word");
-    H.d_slots = dalloc<double>(mfgpu::coop_slot_doubles(), "alloc diagonal slots");
+    H.d_slots = dalloc<unsigned char>(mfgpu::coop_slot_elems() * H.esz, "alloc diagonal slots");
     H.d_all = dalloc<int>(all.size(), "alloc id list");
     ck(cudaMemcpy(H.d_val, val, H.nnz * sizeof(double), cudaMemcpyHostToDevice), "upload val");
     ck(cudaMemcpy(H.d_rp, row_ptr, (n + 1) * sizeof(int), cudaMemcpyHostToDevice), "upload rows");
@@ -661,8 +923,8 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n
     std::vector<char> dirty(s.fronts.size(), 1);
     H.buildPlan(H.full, dirty);
     H.full.upload(H.stream);
-    H.device_bytes = (int64_t)(s.front_elems + s.sep_elems + H.nnz) * 8 + (H.nnz + n + 1) * 4 +
-                     (int64_t)s.dofs.size() * 4;
+    H.device_bytes = (int64_t)(s.front_elems + s.sep_elems) * (int64_t)H.esz + H.nnz * 8 +
+                     (H.nnz + n + 1) * 4 + (int64_t)s.dofs.size() * 4;
   });
   if (st != MFGPU_OK) {
     g_create_error = h->err;
@@ -679,7 +941,7 @@ static int factorImpl(mfgpu_handle* h, const double* val, int64_t nnz, bool devi
   return guarded(h, [&]() {
     h->factored = false;
     ck(cudaEventRecord(h->ev0, h->stream), "event");
-    h->factorWith(val, device, h->full);
+    h->factorWith(val, device, h->full, true);
     ck(cudaEventRecord(h->ev1, h->stream), "event");
     h->checkDevError();
     float ms = 0;
@@ -722,7 +984,7 @@ static int updateImpl(mfgpu_handle* h, const double* val, int64_t nnz, const int
       P = &h->upd;
     }
     h->factored = false;
-    h->factorWith(val, device, *P);
+    h->factorWith(val, device, *P, P == &h->full);
     ck(cudaEventRecord(h->ev1, h->stream), "event");
     h->checkDevError();
     h->factored = true;
@@ -772,6 +1034,8 @@ static int solveOrApply(mfgpu_handle* h, const double* in, double* out, int nrhs
   if (nrhs == 0) return MFGPU_OK;
   return guarded(h, [&]() {
     const int chunk = 16;
+    h->stats.iterations = 0;
+    h->stats.residual = 0;
     ck(cudaEventRecord(h->ev0, h->stream), "event");
     for (int c0 = 0; c0 < nrhs; c0 += chunk) {
       const int nc = std::min(chunk, nrhs - c0);
@@ -782,8 +1046,8 @@ static int solveOrApply(mfgpu_handle* h, const double* in, double* out, int nrhs
                            device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream),
            "copy rhs in");
       if (!h->prof.verbose) h->prof.begin(apply ? MFGPU_KC_APPLY : MFGPU_KC_SOLVE, h->stream);
-      if (apply) h->applyChunk(X, h->n, nc);
-      else h->solveChunk(X, h->n, nc);
+      if (apply) h->applyChunk(X, nc);
+      else h->solveChunk(X, nc);
       if (!h->prof.verbose) h->prof.end(h->stream);
       if (h->prof.on) {
         // L11 (lower) and L21 are read once forward and once backward; the
@@ -791,8 +1055,8 @@ static int solveOrApply(mfgpu_handle* h, const double* in, double* out, int nrhs
         double fl = 0, by = 0;
         for (const mfgpu::Front& f : h->S->fronts) {
           fl += 2.0 * ((double)f.n * f.n + 2.0 * f.n * f.m) * nc;
-          by += 2.0 * 8.0 * ((double)f.n * (f.n + 1) / 2 + (double)f.n * f.m) +
-                8.0 * 4.0 * f.N * nc;
+          by += 2.0 * h->esz * ((double)f.n * (f.n + 1) / 2 + (double)f.n * f.m) +
+                h->esz * 4.0 * f.N * nc;
         }
         const int kc = apply ? MFGPU_KC_APPLY : MFGPU_KC_SOLVE;
         h->prof.flops[kc] += fl;
@@ -864,6 +1128,10 @@ double* noallocScratch(int dev) {
 int mfgpu_solve_device_noalloc(mfgpu_handle* h, const double* d_b, double* d_x, int nrhs,
                                int64_t ld) {
   if (!h) return MFGPU_ERR_ARG;
+  if (h->mixed)
+    return fail(h, MFGPU_ERR_ARG,
+                "mfgpu_solve_device_noalloc supports FP64 handles only (mixed precision refines "
+                "with allocated work vectors); use mfgpu_solve_device");
   const int64_t per_rhs = h->woffTotal;   // workspace doubles one right-hand side needs
   if (per_rhs > (int64_t)kNoAllocScratchDoubles) {
     char buf[256];
@@ -914,8 +1182,8 @@ int mfgpu_get_info(const mfgpu_handle* h, mfgpu_info* info) {
   for (int a = 0; a < 3; a++) info->leaf_box[a] = s.bw[a];
   for (const mfgpu::Front& f : s.fronts) info->max_front = std::max(info->max_front, f.N);
   info->factor_flops = s.total_flops();
-  info->front_bytes = s.front_elems * 8;
-  info->sep_bytes = s.sep_elems * 8;
+  info->front_bytes = s.front_elems * (int64_t)h->esz;
+  info->sep_bytes = s.sep_elems * (int64_t)h->esz;
   info->device_bytes = h->device_bytes;
   return MFGPU_OK;
 }
