@@ -50,6 +50,9 @@ WORKLOADS = {
     # the 3D workload (log-uniform [0.1, 100], leaf parameter 4, one RHS)
     "3d-127": dict(dim=3, N=(127, 127, 127), max_side=4, lo=0.1, hi=100.0, nrhs=1, patch=9,
                    factor=10.0, seed=SEED0 + 3),
+    # a smaller 3D case of the same kind (profiling captures, quick checks)
+    "3d-63": dict(dim=3, N=(63, 63, 63), max_side=4, lo=0.1, hi=100.0, nrhs=1, patch=5,
+                  factor=10.0, seed=SEED0 + 4),
 }
 
 
@@ -375,24 +378,32 @@ def main():
     P = prof[dom]
     roof = None
     if rank == 0:
-        if dom in ("potrf", "trsm", "syrk", "front"):
+        kern = KERNEL_OF.get(dom, dom)
+        common = {"kernel": kern, "class": dom, "launches": P["launches"],
+                  "avg_launch_ms": P["ms"] / max(1, P["launches"]),
+                  "traffic": traffic_for(kern, args.workload, args.precision)}
+        ach = P["flops"] / (P["ms"] * 1e-3) / 1e12
+        if dom == "tc":
+            split = int(os.environ.get("MFGPU_TC_SPLIT", "3"))
+            pk = float(peaks["bf16_tflops"]) / 2.0
+            roof = dict(common, bound="tensor", achieved=ach, peak=pk, unit="TFLOP/s", frac=ach / pk,
+                        achieved_executed=ach * split,
+                        peak_source=f"{peak_src} bf16_tflops / 2 (MEASURED_PEAKS.json): the dense "
+                                    "TF32 rate is half the BF16 rate; achieved counts the "
+                                    f"algorithmic flops once, the kernel executes {split} TF32 "
+                                    "products per flop")
+        elif dom in ("potrf", "trsm", "syrk", "front", "coop"):
             dt, nm = (torch.float32, "SGEMM (float32") if args.precision == "mixed" else \
                 (torch.float64, "DGEMM (float64")
             pk = measured_gemm_peak(torch, dt)
-            ach = P["flops"] / (P["ms"] * 1e-3) / 1e12
-            roof = {"bound": "tensor", "kernel": dom, "achieved": ach, "peak": pk,
-                    "unit": "TFLOP/s", "frac": ach / pk, "traffic": traffic_for(dom),
-                    "peak_source": f"measured cuBLAS {nm} matmul 8192^3, TF32 off) on this "
-                                   "GPU; the factor's precision has no entry in "
-                                   "MEASURED_PEAKS.json",
-                    "launches": P["launches"], "avg_launch_ms": P["ms"] / max(1, P["launches"])}
+            roof = dict(common, bound="tensor", achieved=ach, peak=pk, unit="TFLOP/s", frac=ach / pk,
+                        peak_source=f"measured cuBLAS {nm} matmul 8192^3, TF32 off) on this GPU; "
+                                    "the factor's precision has no entry in MEASURED_PEAKS.json")
         else:
             ach = P["bytes"] / (P["ms"] * 1e-3) / 1e9
             pk = float(peaks["hbm_gbs"])
-            roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": pk, "unit": "GB/s",
-                    "frac": ach / pk, "traffic": traffic_for(dom),
-                    "peak_source": f"{peak_src} hbm_gbs (MEASURED_PEAKS.json)",
-                    "launches": P["launches"], "avg_launch_ms": P["ms"] / max(1, P["launches"])}
+            roof = dict(common, bound="hbm", achieved=ach, peak=pk, unit="GB/s", frac=ach / pk,
+                        peak_source=f"{peak_src} hbm_gbs (MEASURED_PEAKS.json)")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -440,13 +451,20 @@ def main():
     return 0
 
 
-def traffic_for(kernel):
-    """DRAM bytes per launch from the committed ncu summary, when one exists."""
+# profiling class -> the kernel it times
+KERNEL_OF = {"front": "k_front_small", "coop": "k_level_coop", "tc": "k_trail_tc",
+             "assemble": "k_tasks", "solve": "k_solve_*", "apply": "k_apply_*",
+             "potrf": "k_potrf", "trsm": "k_trsm", "syrk": "k_syrk"}
+
+
+def traffic_for(kernel, workload, precision):
+    """DRAM bytes (read + write) per launch of `kernel` in this workload, from
+    the ncu capture summarised in profiles/traffic.json, when one exists."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.isfile(p):
         with open(p) as f:
             d = json.load(f)
-        v = d.get(kernel)
+        v = d.get(f"{kernel}/{workload}/{precision}")
         if isinstance(v, dict):
             return v.get("dram_bytes_per_launch")
     return None

@@ -444,13 +444,15 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_bwd(const int* __restrict__ 
   }
 }
 
+// One CTA per SM: a step's work (at most a few hundred row or column blocks)
+// needs no more, and a smaller grid makes each grid barrier cheaper.
 template <class K>
 int coopGrid(K kern) {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, SCT, 0);
-  return sms * (per > 0 ? per : 1);
+  return per > 0 ? sms : 1;
 }
 
 template <class T, int NR>

@@ -247,6 +247,7 @@ struct mfgpu_handle {
   bool mixed = false;
   int tcMinN = 4096;               // mixed: smallest level maxN run on the tensor cores (0 = never)
   int tcSplit = 3;                 // mixed: 3 = three-term TF32 products, 1 = plain TF32
+  int fusedMinFronts = 148;        // fewest fronts for the one-CTA-per-front kernel
   size_t esz = sizeof(double);     // bytes per factor element
   double* d_scale = nullptr;       // s = 1/sqrt(diag(A)) of the last full factorization
   double* d_iscale = nullptr;      // 1/s
@@ -344,7 +345,7 @@ struct mfgpu_handle {
       L.sadd0 = P.addGroup(s.sep_add_tasks, s.sep_task_ptr, sl, 0);
       L.sadd1 = P.addGroup(s.sep_add_tasks, s.sep_task_ptr, sl, 1);
       L.cpref0 = (int64_t)P.cpref.size();
-      if (!fl.empty() && !mfgpu::small_front_fits(L.maxN, (int)esz) && mfgpu::coop_fits((int)fl.size())) {
+      if (!fl.empty() && !useFused((int)fl.size(), L.maxN) && mfgpu::coop_fits((int)fl.size())) {
         std::vector<int> nn, NN;
         for (int f : fl) {
           nn.push_back(s.fronts[f].n);
@@ -394,25 +395,29 @@ struct mfgpu_handle {
       prof.level = ell;
       runGroup<T>(P, L.sbase, groupBytes(P, L.sbase));
       runGroup<T>(P, L.ftask, groupBytes(P, L.ftask));
-      const bool fused = L.nf > 0 && mfgpu::small_front_fits(L.maxN, (int)sizeof(T));
+      const bool fused = L.nf > 0 && useFused((int)L.nf, L.maxN);
       const bool coop = L.nf > 0 && !fused && mfgpu::coop_fits((int)L.nf) &&
                         (!stepped || sizeof(T) != sizeof(double));
       if (fused || coop) {
+        double fl = 0;
         if (prof.on)
-          for (int64_t i = L.f0; i < L.f0 + L.nf; i++)
-            prof.flops[MFGPU_KC_FRONT] += s.front_flops(s.fronts[P.ids[i]]);
-        prof.begin(MFGPU_KC_FRONT, stream);
+          for (int64_t i = L.f0; i < L.f0 + L.nf; i++) fl += s.front_flops(s.fronts[P.ids[i]]);
         if (fused) {
+          prof.flops[MFGPU_KC_FRONT] += fl;
+          prof.begin(MFGPU_KC_FRONT, stream);
           mfgpu::launch_front_small<T>(P.d_ids + L.f0, (int)L.nf, L.maxN, d_fr, F, d_err, stream);
           ck(cudaGetLastError(), "launch fused front factorization (k_front_small)");
+          prof.end(stream);
         } else if (sizeof(T) == sizeof(float) && tcLevel(L)) {
-          runTensorLevel(P, L);
+          runTensorLevel(P, L, fl);
         } else {
+          prof.flops[MFGPU_KC_COOP] += fl;
+          prof.begin(MFGPU_KC_COOP, stream);
           ck(mfgpu::launch_level_coop<T>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, F, d_err,
                                          (T*)d_slots, P.d_cpref + L.cpref0, stream),
              "launch cooperative level factorization (k_level_coop)");
+          prof.end(stream);
         }
-        prof.end(stream);
       } else if (L.nf > 0) {
         if (sizeof(T) != sizeof(double))
           throw CudaError("no single-precision path for this level", MFGPU_ERR_ARG);
@@ -424,6 +429,14 @@ struct mfgpu_handle {
     ck(cudaGetLastError(), "factor launch");
   }
 
+  // One CTA per front (k_front_small) when the level has enough fronts to fill
+  // the GPU and each front's staged panel fits in shared memory; otherwise the
+  // cooperative kernel spreads every front of the level over all SMs (a
+  // localized update often leaves one or two fronts per level).
+  bool useFused(int nf, int maxN) const {
+    return mfgpu::small_front_fits(maxN, (int)esz) && (nf >= fusedMinFronts || maxN <= 64);
+  }
+
   // Mixed path: levels of large fronts run the cooperative kernel one outer
   // panel at a time (diagonal blocks, panel solves and in-panel updates) and
   // the trailing update of each panel on the tensor cores.
@@ -431,7 +444,10 @@ struct mfgpu_handle {
     return tcMinN > 0 && L.maxN >= tcMinN && L.nf <= mfgpu::tc_max_fronts();
   }
 
-  void runTensorLevel(const Plan& P, const Plan::Level& L) {
+  // Profile attribution: the trailing updates' algorithmic flops,
+  // sum (N - k1)^2 (k1 - K), go to MFGPU_KC_TC, the rest of the level's flops
+  // (diagonal blocks, panel solves, in-panel updates) to MFGPU_KC_COOP.
+  void runTensorLevel(const Plan& P, const Plan::Level& L, double level_flops) {
     const Schedule& s = *S;
     std::vector<int> nn(L.nf), NN(L.nf);
     for (int64_t i = 0; i < L.nf; i++) {
@@ -440,17 +456,30 @@ struct mfgpu_handle {
     }
     const int outer = mfgpu::coop_outer();
     int phase0 = 0;
+    double tc_fl = 0;
     for (int K = 0; K < L.maxn; K += outer) {
+      prof.begin(MFGPU_KC_COOP, stream);
       ck(mfgpu::launch_level_coop<float>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, (float*)d_F,
                                          d_err, (float*)d_slots, P.d_cpref + L.cpref0, stream, K,
                                          K + outer, phase0, 0),
          "launch cooperative panel factorization (k_level_coop)");
+      prof.end(stream);
       phase0 += mfgpu::coop_phases(K, L.maxn);
       const int64_t nt = mfgpu::tc_tiles(nn, NN, K);
+      if (prof.on)
+        for (int64_t i = 0; i < L.nf; i++)
+          if (K < nn[i]) {
+            const double k1 = std::min(K + outer, nn[i]), r = NN[i] - k1;
+            tc_fl += r * r * (k1 - K);
+          }
+      prof.begin(MFGPU_KC_TC, stream);
       ck(mfgpu::launch_trail_tc(P.d_ids + L.f0, (int)L.nf, nt, d_fr, (float*)d_F, K, tcSplit, d_err,
                                 stream),
          "launch tensor-core trailing update (k_trail_tc)");
+      prof.end(stream);
     }
+    prof.flops[MFGPU_KC_TC] += tc_fl;
+    prof.flops[MFGPU_KC_COOP] += std::max(0.0, level_flops - tc_fl);
   }
 
   // FP64 per-step launches (MFGPU_STEPPED=1, or levels no cooperative launch takes).
@@ -859,6 +888,7 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n
   if (const char* e = getenv("MFGPU_VERBOSE")) h->prof.verbose = e[0] == '1';
   if (const char* e = getenv("MFGPU_TC_MIN_N")) h->tcMinN = atoi(e);
   if (const char* e = getenv("MFGPU_SOLVE_COOP_MIN_N")) h->solveCoopMinN = atoi(e);
+  if (const char* e = getenv("MFGPU_FUSED_MIN_FRONTS")) h->fusedMinFronts = atoi(e);
   if (const char* e = getenv("MFGPU_TC_SPLIT")) h->tcSplit = atoi(e) == 1 ? 1 : 3;
   h->h_rowptr.assign(row_ptr, row_ptr + n + 1);
   h->h_colind.assign(col_ind, col_ind + h->nnz);

@@ -33,7 +33,7 @@ EXPORTED = [
     "mfgpu_symbolic_dirty",
 ]
 
-KERNEL_CLASSES = ["assemble", "potrf", "trsm", "syrk", "solve", "apply", "front"]
+KERNEL_CLASSES = ["assemble", "potrf", "trsm", "syrk", "solve", "apply", "front", "coop", "tc"]
 
 
 class Options(C.Structure):
