@@ -81,6 +81,24 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side_length
                  const int* row_ptr, const int* col_ind, const double* val,
                  const mfgpu_options* opts, mfgpu_handle** out);
 
+/* Batch of independent problems in one handle (no reference counterpart; the
+ * reference factors one problem per MF2D/MF3D object).  Problem p has the
+ * geometry (dim[p], nx[p], ny[p], nz[p], width[p], max_side[p]); the matrix is
+ * the block-diagonal CSR of the problems (n = sum of their DOFs, global column
+ * indices), problem p owning rows offs[p] .. offs[p+1]-1 (mfgpu_batch_info).
+ * Every tree level of every problem is factored and solved by the same
+ * launches (levels aligned at the leaves).  All other calls work on the
+ * stacked vectors; mixed-precision refinement, its scalars and its tolerance
+ * are per problem and per right-hand side. */
+int mfgpu_batch_create(int count, const int* dim, const int* nx, const int* ny, const int* nz,
+                       const int* width, const int* max_side, int n, const int* row_ptr,
+                       const int* col_ind, const double* val, const mfgpu_options* opts,
+                       mfgpu_handle** out);
+
+/* Number of problems in the handle (1 for mfgpu_create) and, when dof_offsets
+ * is not null, their count + 1 row offsets. */
+int mfgpu_batch_info(const mfgpu_handle* h, int* count, int64_t* dof_offsets);
+
 /* void Factor() — include/DE/mf.hpp:84, src/DE/mf2d.cpp:449-500. */
 int mfgpu_factor(mfgpu_handle* h);
 
@@ -175,6 +193,10 @@ void mfgpu_destroy(mfgpu_handle* h);
  * AddNew*Interactions_ (src/DE/mf2d.cpp:755-901). */
 int mfgpu_symbolic_create(int dim, int nx, int ny, int nz, int width, int max_side_length,
                           mfgpu_symbolic** out);
+/* The forest schedule of a batch (see mfgpu_batch_create), host only. */
+int mfgpu_symbolic_batch_create(int count, const int* dim, const int* nx, const int* ny,
+                                const int* nz, const int* width, const int* max_side,
+                                mfgpu_symbolic** out);
 void mfgpu_symbolic_destroy(mfgpu_symbolic* s);
 const char* mfgpu_symbolic_error(void);
 /* levels, n_fronts, n_seps, ndof */

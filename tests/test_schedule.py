@@ -197,3 +197,75 @@ def test_update_marks_root_paths(dim, N, ms, side, lib):
         O.marked_boxes = {O._parent(bx, ell) for e in seps for bx in O._nbor_boxes(e, ell)}
     ref |= {(0, 0)}
     assert got <= ref
+
+
+def _model_solve_forest(S, E, b):
+    """Algorithm model for a batch: every level, roots included, through the
+    generic forward sweep, then the generic backward sweep."""
+    for ell in range(S.levels - 1, -1, -1):
+        fl, sl = E.level_fronts(ell), E.level_seps(ell)
+        E.run(E.stasks, sl)
+        E.run(E.ftasks, fl)
+        for f in fl:
+            n = E.fronts[f]["n"]
+            M = E.block(f)
+            L11 = np.linalg.cholesky(M[:n, :n])
+            L21 = sla.solve_triangular(L11, M[n:, :n].T, lower=True).T
+            M[:n, :n], M[n:, :n] = L11, L21
+            M[n:, n:] -= L21 @ L21.T
+            E.set_block(f, M)
+        E.run(E.atasks[0::2], sl)
+        E.run(E.atasks[1::2], sl)
+    X, W, Fr = b.copy(), {}, E.fronts
+    for ell in range(S.levels - 1, -1, -1):
+        for f in E.level_fronts(ell):
+            n, d, M = Fr[f]["n"], Fr[f]["dofs"], np.tril(E.block(f))
+            y = sla.solve_triangular(M[:n, :n], X[d[:n]], lower=True)
+            X[d[:n]] = y
+            W[f] = -(M[n:, :n] @ y)
+        for k in E.level_seps(ell):
+            s = E.seps[k]
+            (b0, b1), (r0, r1) = s["boxes"], s["rows"]
+            d, n0, n1 = s["dofs"], Fr[b0]["n"], Fr[b1]["n"]
+            X[d] = (X[d] + W[b0][r0 - n0:r0 - n0 + len(d)]) + W[b1][r1 - n1:r1 - n1 + len(d)]
+    for ell in range(0, S.levels):
+        for f in E.level_fronts(ell):
+            n, d, M = Fr[f]["n"], Fr[f]["dofs"], np.tril(E.block(f))
+            X[d[:n]] = sla.solve_triangular(M[:n, :n], X[d[:n]] - M[n:, :n].T @ X[d[n:]],
+                                            lower=True, trans=1)
+    return X
+
+
+def test_batch_forest_model_matches_oracle(lib):
+    # three problems of different depth and dimension in one forest schedule:
+    # levels aligned at the leaves, fronts renumbered, DOFs shifted
+    import scipy.sparse as sp
+    batch = [(2, (31, 31), 1, 4), (2, (63, 63), 1, 4), (3, (13, 17, 11), 1, 3)]
+    mats, rhs, xs = [], [], []
+    for i, (dim, N, w, ms) in enumerate(batch):
+        A = stencil.build_laplacian(stencil.loguniform_coefficients(N, 0.1, 10.0, 20 + i)).to_scipy()
+        b = stencil.uniform_rhs(A.shape[0], 1, 30 + i)[0]
+        O = mf_oracle.MFOracle(A, N, w, ms)
+        O.factor()
+        mats.append(A)
+        rhs.append(b)
+        xs.append(O.solve(b))
+    S = Symbolic(0, (0, 0), batch=batch)
+    singles = [Symbolic(dim, N, w, ms) for dim, N, w, ms in batch]
+    assert S.levels == max(q.levels for q in singles)
+    assert S.n_fronts == sum(q.n_fronts for q in singles)
+    assert S.ndof == sum(q.ndof for q in singles)
+    x = _model_solve_forest(S, taskemu.Emu(S, sp.block_diag(mats, format="csr")),
+                            np.concatenate(rhs))
+    off = 0
+    for b, xo in zip(rhs, xs):
+        assert np.linalg.norm(x[off:off + len(b)] - xo) <= 1e-13 * np.linalg.norm(xo)
+        off += len(b)
+    # dirty marking stays inside the touched problem
+    dirty, _ = S.dirty([singles[0].ndof + 5])
+    fronts = [S.front(f) for f in range(S.n_fronts)]
+    lo, hi = singles[0].ndof, singles[0].ndof + singles[1].ndof
+    assert dirty.any()
+    for f in np.flatnonzero(dirty):
+        d = fronts[f]["dofs"]
+        assert len(d) == 0 or (lo <= d.min() and d.max() < hi)

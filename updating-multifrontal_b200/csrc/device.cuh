@@ -134,18 +134,26 @@ void launch_spmv(const int* rp, const int* ci, const double* va, int n, const do
 void launch_residual(const int* rp, const int* ci, const double* va, int n, const double* b,
                      int64_t ldb, const double* x, int64_t ldx, double* r, int64_t ldr, int nrhs,
                      cudaStream_t st);
-size_t dot_scratch_elems(int nrhs);
-void launch_dot(const double* x, int64_t ldx, const double* y, int64_t ldy, int n, int nrhs,
-                double* part, double* out, cudaStream_t st);
+// Segmented deterministic dots: dot_plan cuts each segment [seg_row[g],
+// seg_row[g+1]) into fixed chunks; launch_dot writes out[g + nseg * c].
+void dot_plan(const std::vector<int64_t>& seg_row, std::vector<int>& chunk_row,
+              std::vector<int>& seg_chunk);
+void launch_dot(const double* x, int64_t ldx, const double* y, int64_t ldy, int nrhs,
+                const int* chunk_row, int nchunks, const int* seg_chunk, int nseg, double* part,
+                double* out, cudaStream_t st);
 template <class T>
 void launch_scale_to(const double* src, int64_t lds, T* dst, int64_t ldd, const double* s, int n,
                      int nrhs, cudaStream_t st);
 template <class T>
 void launch_scale_from(const T* src, int64_t lds, double* dst, int64_t ldd, const double* s, int n,
                        int nrhs, cudaStream_t st);
+// PCG updates with per-(segment, column) scalars; seg_row holds the nseg + 1
+// segment boundaries (rows) on the device.
 void launch_pcg_xr(double* x, double* r, const double* p, const double* q, int64_t ld, int n,
-                   int nrhs, const double* rz, const double* pq, const int* active, cudaStream_t st);
+                   int nrhs, const double* rz, const double* pq, const int* active,
+                   const int* seg_row, int nseg, cudaStream_t st);
 void launch_pcg_p(double* p, const double* z, int64_t ld, int n, int nrhs, const double* rz_new,
-                  const double* rz_old, const int* active, int first, cudaStream_t st);
+                  const double* rz_old, const int* active, int first, const int* seg_row, int nseg,
+                  cudaStream_t st);
 
 }  // namespace mfgpu

@@ -59,9 +59,12 @@ __global__ void k_residual(const int* __restrict__ rp, const int* __restrict__ c
   r[i + c * ldr] = b[i + c * ldb] - s;
 }
 
-// Deterministic dot products: fixed partition into kDotBlocks chunks, fixed
-// reduction tree in each, partials summed in order by one block per column.
-constexpr int kDotBlocks = 256;
+// Deterministic, segmented dot products.  The vector is a concatenation of
+// segments (the problems of a batch; one segment otherwise); each segment is
+// cut into chunks of kDotChunk elements starting at the segment's first row,
+// each chunk reduced by a fixed tree, and a segment's chunk sums added in
+// order.  A segment's result therefore depends only on its own data.
+constexpr int kDotChunk = 8192;
 
 __device__ double block_sum(double v) {
   __shared__ double red[VT / 32];
@@ -78,25 +81,39 @@ __device__ double block_sum(double v) {
   return t;   // valid in thread 0
 }
 
+// chunk_row[k] = first row of chunk k; chunk_row[nchunks] = n.
 __global__ void k_dot_part(const double* __restrict__ x, int64_t ldx, const double* __restrict__ y,
-                           int64_t ldy, int n, double* __restrict__ part) {
-  const int c = blockIdx.y;
-  const int chunk = (n + kDotBlocks - 1) / kDotBlocks;
-  const int lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
+                           int64_t ldy, const int* __restrict__ chunk_row, int nchunks,
+                           double* __restrict__ part) {
+  const int k = blockIdx.x, c = blockIdx.y;
+  const int lo = chunk_row[k], hi = chunk_row[k + 1];
   const double* xc = x + c * ldx;
   const double* yc = y + c * ldy;
   double s = 0.0;
   for (int i = lo + threadIdx.x; i < hi; i += VT) s = fma(xc[i], yc[i], s);
   s = block_sum(s);
-  if (threadIdx.x == 0) part[c * kDotBlocks + blockIdx.x] = s;
+  if (threadIdx.x == 0) part[(int64_t)c * nchunks + k] = s;
 }
 
-__global__ void k_dot_final(const double* __restrict__ part, double* __restrict__ out) {
-  const int c = blockIdx.x;
+// out[seg + nseg * c] = sum of the segment's chunk partials, in order.
+__global__ void k_dot_final(const double* __restrict__ part, const int* __restrict__ seg_chunk,
+                            int nseg, int nchunks, double* __restrict__ out) {
+  const int g = blockIdx.x, c = blockIdx.y;
+  const int lo = seg_chunk[g], hi = seg_chunk[g + 1];
   double s = 0.0;
-  for (int i = threadIdx.x; i < kDotBlocks; i += VT) s += part[c * kDotBlocks + i];
+  for (int i = lo + threadIdx.x; i < hi; i += VT) s += part[(int64_t)c * nchunks + i];
   s = block_sum(s);
-  if (threadIdx.x == 0) out[c] = s;
+  if (threadIdx.x == 0) out[g + nseg * c] = s;
+}
+
+__device__ __forceinline__ int seg_of(const int* __restrict__ seg_row, int nseg, int i) {
+  int lo = 0, hi = nseg - 1;   // largest g with seg_row[g] <= i
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (seg_row[mid] <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
 }
 
 // dst(T) = s .* src(double)   (s may be null)
@@ -121,27 +138,34 @@ __global__ void k_scale_from(const T* __restrict__ src, int64_t lds, double* __r
   dst[i + c * ldd] = s ? s[i] * v : v;
 }
 
-// x_c += a_c p_c ; r_c -= a_c q_c with a_c = rz_c / pq_c, for active columns.
+// x += a p ; r -= a q with a = rz / pq of the row's (segment, column), for
+// active (segment, column) pairs.
 __global__ void k_pcg_xr(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
                          const double* __restrict__ q, int64_t ld, int n,
                          const double* __restrict__ rz, const double* __restrict__ pq,
-                         const int* __restrict__ active) {
+                         const int* __restrict__ active, const int* __restrict__ seg_row, int nseg) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int c = blockIdx.y;
-  if (i >= n || !active[c]) return;
-  const double a = rz[c] / pq[c];
+  if (i >= n) return;
+  const int g = seg_of(seg_row, nseg, i) + nseg * c;
+  if (!active[g]) return;
+  const double a = rz[g] / pq[g];
   x[i + c * ld] = fma(a, p[i + c * ld], x[i + c * ld]);
   r[i + c * ld] = fma(-a, q[i + c * ld], r[i + c * ld]);
 }
 
-// p_c = z_c + b_c p_c with b_c = rz_new_c / rz_old_c (first iteration: p = z).
+// p = z + b p with b = rz_new / rz_old of the row's (segment, column) (first
+// iteration: p = z).
 __global__ void k_pcg_p(double* __restrict__ p, const double* __restrict__ z, int64_t ld, int n,
                         const double* __restrict__ rz_new, const double* __restrict__ rz_old,
-                        const int* __restrict__ active, int first) {
+                        const int* __restrict__ active, int first, const int* __restrict__ seg_row,
+                        int nseg) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int c = blockIdx.y;
-  if (i >= n || !active[c]) return;
-  const double b = first ? 0.0 : rz_new[c] / rz_old[c];
+  if (i >= n) return;
+  const int g = seg_of(seg_row, nseg, i) + nseg * c;
+  if (!active[g]) return;
+  const double b = first ? 0.0 : rz_new[g] / rz_old[g];
   p[i + c * ld] = fma(b, p[i + c * ld], z[i + c * ld]);
 }
 
@@ -168,12 +192,22 @@ void launch_residual(const int* rp, const int* ci, const double* va, int n, cons
   g_launches++;
 }
 
-size_t dot_scratch_elems(int nrhs) { return (size_t)kDotBlocks * nrhs; }
+void dot_plan(const std::vector<int64_t>& seg_row, std::vector<int>& chunk_row,
+              std::vector<int>& seg_chunk) {
+  chunk_row.clear();
+  seg_chunk.assign(1, 0);
+  for (size_t g = 0; g + 1 < seg_row.size(); g++) {
+    for (int64_t r = seg_row[g]; r < seg_row[g + 1]; r += kDotChunk) chunk_row.push_back((int)r);
+    seg_chunk.push_back((int)chunk_row.size());
+  }
+  chunk_row.push_back((int)seg_row.back());
+}
 
-void launch_dot(const double* x, int64_t ldx, const double* y, int64_t ldy, int n, int nrhs,
-                double* part, double* out, cudaStream_t st) {
-  k_dot_part<<<dim3(kDotBlocks, nrhs), VT, 0, st>>>(x, ldx, y, ldy, n, part);
-  k_dot_final<<<nrhs, VT, 0, st>>>(part, out);
+void launch_dot(const double* x, int64_t ldx, const double* y, int64_t ldy, int nrhs,
+                const int* chunk_row, int nchunks, const int* seg_chunk, int nseg, double* part,
+                double* out, cudaStream_t st) {
+  k_dot_part<<<dim3(nchunks, nrhs), VT, 0, st>>>(x, ldx, y, ldy, chunk_row, nchunks, part);
+  k_dot_final<<<dim3(nseg, nrhs), VT, 0, st>>>(part, seg_chunk, nseg, nchunks, out);
   g_launches += 2;
 }
 
@@ -192,14 +226,16 @@ void launch_scale_from(const T* src, int64_t lds, double* dst, int64_t ldd, cons
 }
 
 void launch_pcg_xr(double* x, double* r, const double* p, const double* q, int64_t ld, int n,
-                   int nrhs, const double* rz, const double* pq, const int* active, cudaStream_t st) {
-  k_pcg_xr<<<vgrid(n, nrhs), VT, 0, st>>>(x, r, p, q, ld, n, rz, pq, active);
+                   int nrhs, const double* rz, const double* pq, const int* active,
+                   const int* seg_row, int nseg, cudaStream_t st) {
+  k_pcg_xr<<<vgrid(n, nrhs), VT, 0, st>>>(x, r, p, q, ld, n, rz, pq, active, seg_row, nseg);
   g_launches++;
 }
 
 void launch_pcg_p(double* p, const double* z, int64_t ld, int n, int nrhs, const double* rz_new,
-                  const double* rz_old, const int* active, int first, cudaStream_t st) {
-  k_pcg_p<<<vgrid(n, nrhs), VT, 0, st>>>(p, z, ld, n, rz_new, rz_old, active, first);
+                  const double* rz_old, const int* active, int first, const int* seg_row, int nseg,
+                  cudaStream_t st) {
+  k_pcg_p<<<vgrid(n, nrhs), VT, 0, st>>>(p, z, ld, n, rz_new, rz_old, active, first, seg_row, nseg);
   g_launches++;
 }
 

@@ -257,8 +257,14 @@ struct mfgpu_handle {
   size_t cap32 = 0;
   double* d_dotp = nullptr;
   size_t capDot = 0;
-  double* d_sc = nullptr;          // refinement scalars
-  int* d_active = nullptr;         // refinement: columns still iterating
+  double* d_sc = nullptr;          // refinement scalars, 5 x nseg x 16
+  int* d_active = nullptr;         // refinement: (segment, column) pairs still iterating
+  // segments of the solution vector: the problems of a batch (one otherwise);
+  // the refinement's dots, scalars and convergence test are per segment
+  int nseg = 1, nchunks = 0;
+  int* d_segrow = nullptr;         // nseg + 1 segment boundaries (rows)
+  int* d_chunkrow = nullptr;       // nchunks + 1 dot chunk boundaries (rows)
+  int* d_segchunk = nullptr;       // nseg + 1: first dot chunk of each segment
   int* d_all = nullptr;      // every front id then every separator id, level order
   int64_t woffTotal = 0;     // sum over fronts of 2N
   Plan full, upd;
@@ -299,6 +305,9 @@ struct mfgpu_handle {
     cudaFree(d_dotp);
     cudaFree(d_sc);
     cudaFree(d_active);
+    cudaFree(d_segrow);
+    cudaFree(d_chunkrow);
+    cudaFree(d_segchunk);
     cudaFree(d_all);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -571,7 +580,7 @@ struct mfgpu_handle {
       growBuf(d_Q, capQ, v, "alloc refinement buffer");
       growBuf(d_Z, capZ, v, "alloc refinement buffer");
       growBuf(d_x32, cap32, v, "alloc refinement buffer");
-      growBuf(d_dotp, capDot, mfgpu::dot_scratch_elems(nrhs), "alloc dot scratch");
+      growBuf(d_dotp, capDot, (size_t)nchunks * nrhs, "alloc dot scratch");
     }
   }
 
@@ -633,7 +642,7 @@ struct mfgpu_handle {
       ck(cudaGetLastError(), "launch separator gather (k_sep_gather)");
     }
     vmark(true, 0);
-    if (coopSweep(0)) {
+    if (coopSweep(0) || s.lv[0].nbox > 1) {   // several roots (a batch): generic sweeps
       sweepLevel<T>(true, 0, X, ldx, nrhs, W);
       sweepLevel<T>(false, 0, X, ldx, nrhs, W);
     } else {
@@ -658,8 +667,14 @@ struct mfgpu_handle {
                                 nrhs, W, d_woff, Tb, stream);
       ck(cudaGetLastError(), "launch apply up (k_apply_up)");
     }
-    mfgpu::launch_root_apply<T>(0, d_fr, F, d_dofs, X, ldx, nrhs, W, d_woff, stream);
-    ck(cudaGetLastError(), "launch root apply (k_root_apply)");
+    if (s.lv[0].nbox > 1) {   // several roots (a batch)
+      mfgpu::launch_apply_up<T>(d_all, s.lv[0].nbox, d_fr, F, d_dofs, X, ldx, nrhs, W, d_woff, Tb,
+                                stream);
+      ck(cudaGetLastError(), "launch apply up (k_apply_up)");
+    } else {
+      mfgpu::launch_root_apply<T>(0, d_fr, F, d_dofs, X, ldx, nrhs, W, d_woff, stream);
+      ck(cudaGetLastError(), "launch root apply (k_root_apply)");
+    }
     for (int ell = 1; ell < s.levels; ell++) {
       mfgpu::launch_apply_down<T>(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, F, d_dofs, ldx,
                                   nrhs, W, d_woff, Tb, stream);
@@ -678,7 +693,7 @@ struct mfgpu_handle {
   }
 
   void dots(const double* x, const double* y, int nc, double* out) {
-    mfgpu::launch_dot(x, n, y, n, n, nc, d_dotp, out, stream);
+    mfgpu::launch_dot(x, n, y, n, nc, d_chunkrow, nchunks, d_segchunk, nseg, d_dotp, out, stream);
   }
 
   // Mixed precision: conjugate gradients on A x = b in FP64 (residuals from the
@@ -689,59 +704,57 @@ struct mfgpu_handle {
     const double tol = opt.refine_tol > 0 ? opt.refine_tol : 1e-10;
     const int maxit = opt.refine_maxit > 0 ? opt.refine_maxit : 50;
     const size_t vb = (size_t)n * nc * sizeof(double);
-    double* sc = d_sc;   // rz_a | rz_b | pq | rr | bb, 16 each
-    double* rzA = sc;
-    double* rzB = sc + 16;
-    double* pq = sc + 32;
-    double* rr = sc + 48;
-    double* bb = sc + 64;
+    const int G = nseg * nc;            // (segment, column) pairs
+    double* rzA = d_sc;                 // rz_a | rz_b | pq | rr | bb, nseg * 16 each
+    double* rzB = d_sc + 16 * nseg;
+    double* pq = d_sc + 32 * nseg;
+    double* rr = d_sc + 48 * nseg;
+    double* bb = d_sc + 64 * nseg;
     ck(cudaMemcpyAsync(d_B, XB, vb, cudaMemcpyDeviceToDevice, stream), "copy rhs");
     dots(d_B, d_B, nc, bb);
     precond(d_B, XB, nc);   // x0 = M^{-1} b
     mfgpu::launch_residual(d_rp, d_ci, d_val, n, d_B, n, XB, n, d_R, n, nc, stream);
-    double hb[16], hr[16];
-    int act[16];
-    ck(cudaMemcpyAsync(hb, bb, nc * sizeof(double), cudaMemcpyDeviceToHost, stream), "read norms");
+    std::vector<double> hb(G), hr(G);
+    std::vector<int> act(G);
+    ck(cudaMemcpyAsync(hb.data(), bb, G * sizeof(double), cudaMemcpyDeviceToHost, stream),
+       "read norms");
     int it = 0, restarts = 0;
     bool first = true;
     double worst = 0;
-    while (true) {
+    // relative residual of every (segment, column); returns how many miss tol
+    auto check = [&]() {
       dots(d_R, d_R, nc, rr);
-      ck(cudaMemcpyAsync(hr, rr, nc * sizeof(double), cudaMemcpyDeviceToHost, stream), "read norms");
+      ck(cudaMemcpyAsync(hr.data(), rr, G * sizeof(double), cudaMemcpyDeviceToHost, stream),
+         "read norms");
       ck(cudaStreamSynchronize(stream), "refinement");
       int nact = 0;
       worst = 0;
-      for (int c = 0; c < nc; c++) {
-        const double rel = hb[c] > 0 ? std::sqrt(hr[c] / hb[c]) : std::sqrt(hr[c]);
+      for (int g = 0; g < G; g++) {
+        const double rel = hb[g] > 0 ? std::sqrt(hr[g] / hb[g]) : std::sqrt(hr[g]);
         worst = std::max(worst, rel);
-        act[c] = rel > tol;
-        nact += act[c];
+        act[g] = rel > tol;
+        nact += act[g];
       }
-      if (nact == 0) {
+      return nact;
+    };
+    while (true) {
+      if (check() == 0) {
         // confirm with the true residual; restart from it if the recursive one drifted
         mfgpu::launch_residual(d_rp, d_ci, d_val, n, d_B, n, XB, n, d_R, n, nc, stream);
-        dots(d_R, d_R, nc, rr);
-        ck(cudaMemcpyAsync(hr, rr, nc * sizeof(double), cudaMemcpyDeviceToHost, stream), "read norms");
-        ck(cudaStreamSynchronize(stream), "refinement");
-        worst = 0;
-        for (int c = 0; c < nc; c++) {
-          const double rel = hb[c] > 0 ? std::sqrt(hr[c] / hb[c]) : std::sqrt(hr[c]);
-          worst = std::max(worst, rel);
-          act[c] = rel > tol;
-          nact += act[c];
-        }
-        if (nact == 0 || restarts >= 3) break;
+        if (check() == 0 || restarts >= 3) break;
         restarts++;
         first = true;
       }
       if (it >= maxit) break;
-      ck(cudaMemcpyAsync(d_active, act, nc * sizeof(int), cudaMemcpyHostToDevice, stream), "flags");
+      ck(cudaMemcpyAsync(d_active, act.data(), G * sizeof(int), cudaMemcpyHostToDevice, stream),
+         "flags");
       precond(d_R, d_Z, nc);
       dots(d_R, d_Z, nc, rzB);
-      mfgpu::launch_pcg_p(d_P, d_Z, n, n, nc, rzB, rzA, d_active, first ? 1 : 0, stream);
+      mfgpu::launch_pcg_p(d_P, d_Z, n, n, nc, rzB, rzA, d_active, first ? 1 : 0, d_segrow, nseg,
+                          stream);
       mfgpu::launch_spmv(d_rp, d_ci, d_val, n, d_P, n, d_Q, n, nc, stream);
       dots(d_P, d_Q, nc, pq);
-      mfgpu::launch_pcg_xr(XB, d_R, d_P, d_Q, n, n, nc, rzB, pq, d_active, stream);
+      mfgpu::launch_pcg_xr(XB, d_R, d_P, d_Q, n, n, nc, rzB, pq, d_active, d_segrow, nseg, stream);
       ck(cudaGetLastError(), "refinement launch");
       std::swap(rzA, rzB);   // rz of this iteration becomes the previous one
       first = false;
@@ -844,6 +857,34 @@ const char* mfgpu_status_string(int s) {
   return "unknown status";
 }
 
+namespace {
+
+// Schedule of one problem; the reference's constructor exceptions become
+// status codes (src/DE/mf2d.cpp:38-43 recursion depth, :60-66 leaf math).
+int makeSchedule(int dim, int nx, int ny, int nz, int width, int max_side,
+                 std::unique_ptr<Schedule>& out) {
+  if (width != 1) {
+    g_create_error = "only separator width 1 (5-/7-point stencils) is supported";
+    return MFGPU_ERR_ARG;
+  }
+  try {
+    out.reset(new Schedule(dim, nx, ny, nz, width, max_side));
+  } catch (const std::invalid_argument& e) {
+    g_create_error = e.what();
+    return MFGPU_ERR_ARG;
+  } catch (const std::runtime_error& e) {
+    g_create_error = e.what();
+    return std::string(e.what()).find("recursion depth") != std::string::npos ? MFGPU_ERR_DEPTH
+                                                                                : MFGPU_ERR_LEAF;
+  }
+  return MFGPU_OK;
+}
+
+int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const int* col_ind,
+               const double* val, const mfgpu_options* opts, mfgpu_handle** out);
+
+}  // namespace
+
 int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n,
                  const int* row_ptr, const int* col_ind, const double* val,
                  const mfgpu_options* opts, mfgpu_handle** out) {
@@ -854,10 +895,63 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n
     g_create_error = "null CSR pointer";
     return MFGPU_ERR_ARG;
   }
-  if (width != 1) {
-    g_create_error = "only separator width 1 (5-/7-point stencils) is supported";
+  std::unique_ptr<Schedule> sched;
+  const int st = makeSchedule(dim, nx, ny, nz, width, max_side, sched);
+  if (st != MFGPU_OK) return st;
+  return createFrom(std::move(sched), n, row_ptr, col_ind, val, opts, out);
+}
+
+int mfgpu_batch_create(int count, const int* dim, const int* nx, const int* ny, const int* nz,
+                       const int* width, const int* max_side, int n, const int* row_ptr,
+                       const int* col_ind, const double* val, const mfgpu_options* opts,
+                       mfgpu_handle** out) {
+  if (!out) return MFGPU_ERR_ARG;
+  *out = nullptr;
+  g_create_error.clear();
+  if (count <= 0 || !dim || !nx || !ny || !nz || !width || !max_side || !row_ptr || !col_ind ||
+      !val) {
+    g_create_error = "bad batch arguments";
     return MFGPU_ERR_ARG;
   }
+  std::vector<Schedule> parts;
+  parts.reserve(count);
+  for (int p = 0; p < count; p++) {
+    std::unique_ptr<Schedule> one;
+    const int st = makeSchedule(dim[p], nx[p], ny[p], nz[p], width[p], max_side[p], one);
+    if (st != MFGPU_OK) {
+      g_create_error = "batch member " + std::to_string(p) + ": " + g_create_error;
+      return st;
+    }
+    parts.push_back(std::move(*one));
+  }
+  std::unique_ptr<Schedule> sched;
+  try {
+    sched.reset(new Schedule(std::move(parts)));
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    return MFGPU_ERR_ARG;
+  }
+  return createFrom(std::move(sched), n, row_ptr, col_ind, val, opts, out);
+}
+
+int mfgpu_batch_info(const mfgpu_handle* h, int* count, int64_t* dof_offsets) {
+  if (!h) return MFGPU_ERR_ARG;
+  const Schedule& s = *h->S;
+  const int c = s.forest() ? (int)s.parts.size() : 1;
+  if (count) *count = c;
+  if (dof_offsets) {
+    if (s.forest())
+      for (int p = 0; p <= c; p++) dof_offsets[p] = s.dof_base[p];
+    else
+      dof_offsets[0] = 0, dof_offsets[1] = s.ndof;
+  }
+  return MFGPU_OK;
+}
+
+namespace {
+
+int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const int* col_ind,
+               const double* val, const mfgpu_options* opts, mfgpu_handle** out) {
   std::unique_ptr<mfgpu_handle> h(new (std::nothrow) mfgpu_handle());
   if (!h) return MFGPU_ERR_OOM;
   mfgpu_default_options(&h->opt);
@@ -867,16 +961,7 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n
     g_create_error = "unknown precision";
     return MFGPU_ERR_ARG;
   }
-  try {
-    h->S.reset(new Schedule(dim, nx, ny, nz, width, max_side));
-  } catch (const std::invalid_argument& e) {
-    g_create_error = e.what();
-    return MFGPU_ERR_ARG;
-  } catch (const std::runtime_error& e) {
-    g_create_error = e.what();
-    return std::string(e.what()).find("recursion depth") != std::string::npos ? MFGPU_ERR_DEPTH
-                                                                                : MFGPU_ERR_LEAF;
-  }
+  h->S = std::move(sched);
   const Schedule& s = *h->S;
   if ((int64_t)n != s.ndof || row_ptr[0] != 0) {
     g_create_error = "matrix dimension does not match the grid";
@@ -903,10 +988,24 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n
     H.d_F = dalloc<unsigned char>(s.front_elems * H.esz, "alloc front arena");
     H.d_Sep = dalloc<unsigned char>(s.sep_elems * H.esz, "alloc separator arena");
     if (H.mixed) {
+      std::vector<int64_t> segrow = s.forest() ? s.dof_base : std::vector<int64_t>{0, s.ndof};
+      H.nseg = (int)segrow.size() - 1;
+      std::vector<int> chunkrow, segchunk, segrow32(segrow.begin(), segrow.end());
+      mfgpu::dot_plan(segrow, chunkrow, segchunk);
+      H.nchunks = (int)chunkrow.size() - 1;
       H.d_scale = dalloc<double>(n, "alloc scaling");
       H.d_iscale = dalloc<double>(n, "alloc scaling");
-      H.d_sc = dalloc<double>(80, "alloc refinement scalars");
-      H.d_active = dalloc<int>(16, "alloc refinement flags");
+      H.d_sc = dalloc<double>(80 * (size_t)H.nseg, "alloc refinement scalars");
+      H.d_active = dalloc<int>(16 * (size_t)H.nseg, "alloc refinement flags");
+      H.d_segrow = dalloc<int>(segrow32.size(), "alloc segments");
+      H.d_chunkrow = dalloc<int>(chunkrow.size(), "alloc dot chunks");
+      H.d_segchunk = dalloc<int>(segchunk.size(), "alloc dot chunks");
+      ck(cudaMemcpy(H.d_segrow, segrow32.data(), segrow32.size() * sizeof(int),
+                    cudaMemcpyHostToDevice), "upload segments");
+      ck(cudaMemcpy(H.d_chunkrow, chunkrow.data(), chunkrow.size() * sizeof(int),
+                    cudaMemcpyHostToDevice), "upload dot chunks");
+      ck(cudaMemcpy(H.d_segchunk, segchunk.data(), segchunk.size() * sizeof(int),
+                    cudaMemcpyHostToDevice), "upload dot chunks");
     }
     H.d_val = dalloc<double>(H.nnz, "alloc CSR values");
     H.d_rp = dalloc<int>(n + 1, "alloc CSR rows");
@@ -963,6 +1062,8 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n
   *out = h.release();
   return MFGPU_OK;
 }
+
+}  // namespace
 
 static int factorImpl(mfgpu_handle* h, const double* val, int64_t nnz, bool device) {
   if (!h) return MFGPU_ERR_ARG;
@@ -1248,6 +1349,33 @@ int mfgpu_symbolic_create(int dim, int nx, int ny, int nz, int width, int max_si
   try {
     std::unique_ptr<mfgpu_symbolic> s(new mfgpu_symbolic());
     s->S.reset(new Schedule(dim, nx, ny, nz, width, max_side));
+    *out = s.release();
+    return MFGPU_OK;
+  } catch (const std::invalid_argument& e) {
+    g_sym_error = e.what();
+    return MFGPU_ERR_ARG;
+  } catch (const std::runtime_error& e) {
+    g_sym_error = e.what();
+    return std::string(e.what()).find("recursion depth") != std::string::npos ? MFGPU_ERR_DEPTH
+                                                                                : MFGPU_ERR_LEAF;
+  } catch (const std::bad_alloc&) {
+    return MFGPU_ERR_OOM;
+  }
+}
+
+int mfgpu_symbolic_batch_create(int count, const int* dim, const int* nx, const int* ny,
+                                const int* nz, const int* width, const int* max_side,
+                                mfgpu_symbolic** out) {
+  if (!out || count <= 0 || !dim || !nx || !ny || !nz || !width || !max_side) return MFGPU_ERR_ARG;
+  *out = nullptr;
+  g_sym_error.clear();
+  try {
+    std::vector<Schedule> parts;
+    parts.reserve(count);
+    for (int p = 0; p < count; p++)
+      parts.emplace_back(dim[p], nx[p], ny[p], nz[p], width[p], max_side[p]);
+    std::unique_ptr<mfgpu_symbolic> s(new mfgpu_symbolic());
+    s->S.reset(new Schedule(std::move(parts)));
     *out = s.release();
     return MFGPU_OK;
   } catch (const std::invalid_argument& e) {

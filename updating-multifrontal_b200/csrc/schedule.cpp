@@ -1,6 +1,10 @@
 #include "schedule.hpp"
 
 #include <algorithm>
+#include <array>
+#include <climits>
+
+#include <algorithm>
 #include <cmath>
 #include <set>
 #include <stdexcept>
@@ -659,7 +663,149 @@ void Schedule::buildTasks() {
   }
 }
 
+Schedule::Schedule(std::vector<Schedule>&& batch) {
+  if (batch.empty()) throw std::invalid_argument("empty batch");
+  parts = std::move(batch);
+  const int P = (int)parts.size();
+  const Schedule& p0 = parts[0];
+  dim = p0.dim;
+  width = p0.width;
+  for (int a = 0; a < 3; a++) {
+    N[a] = p0.N[a];
+    bw[a] = p0.bw[a];
+  }
+  levels = 0;
+  for (const Schedule& q : parts) levels = std::max(levels, q.levels);
+  auto shift = [&](int p) { return levels - parts[p].levels; };
+  dof_base.assign(P + 1, 0);
+  std::vector<int64_t> fbase(P + 1, 0), sbase(P + 1, 0), tbase(P + 1, 0);
+  for (int p = 0; p < P; p++) {
+    dof_base[p + 1] = dof_base[p] + parts[p].ndof;
+    fbase[p + 1] = fbase[p] + parts[p].front_elems;
+    sbase[p + 1] = sbase[p] + parts[p].sep_elems;
+    tbase[p + 1] = tbase[p] + (int64_t)parts[p].dofs.size();
+  }
+  ndof = dof_base[P];
+  if (ndof > 0x7fffffffLL) throw std::invalid_argument("more than 2^31-1 DOFs in the batch");
+  if (tbase[P] > 0x7fffffffLL) throw std::invalid_argument("DOF table too large for the batch");
+  front_elems = fbase[P];
+  sep_elems = sbase[P];
+  // levels and renumbering: level by level, part by part, local order inside
+  lv.assign(levels, LevelInfo{0, 0, 0, 0});
+  for (int ml = 0; ml < levels; ml++)
+    for (int p = 0; p < P; p++) {
+      const int pl = ml - shift(p);
+      if (pl < 0) continue;
+      lv[ml].nbox += parts[p].lv[pl].nbox;
+      lv[ml].nsep += parts[p].lv[pl].nsep;
+    }
+  int nf = 0, ns = 0;
+  for (int ml = 0; ml < levels; ml++) {
+    lv[ml].front0 = nf;
+    lv[ml].sep0 = ns;
+    nf += lv[ml].nbox;
+    ns += lv[ml].nsep;
+  }
+  front_map.resize(P);
+  sep_map.resize(P);
+  std::vector<std::pair<int, int>> fsrc(nf), ssrc(ns);   // id here -> (part, local id)
+  for (int p = 0; p < P; p++) {
+    front_map[p].assign(parts[p].fronts.size(), -1);
+    sep_map[p].assign(parts[p].seps.size(), -1);
+  }
+  for (int ml = 0; ml < levels; ml++) {
+    int fc = lv[ml].front0, sc = lv[ml].sep0;
+    for (int p = 0; p < P; p++) {
+      const int pl = ml - shift(p);
+      if (pl < 0) continue;
+      const LevelInfo& L = parts[p].lv[pl];
+      for (int b = 0; b < L.nbox; b++) {
+        front_map[p][L.front0 + b] = fc;
+        fsrc[fc++] = {p, L.front0 + b};
+      }
+      for (int e = 0; e < L.nsep; e++) {
+        sep_map[p][L.sep0 + e] = sc;
+        ssrc[sc++] = {p, L.sep0 + e};
+      }
+    }
+  }
+  fronts.resize(nf);
+  seps.resize(ns);
+  dofs.reserve((size_t)tbase[P]);
+  // per part: (old table offset, new table offset, length), sorted by old offset
+  std::vector<std::vector<std::array<int64_t, 3>>> tmap(P);
+  for (int i = 0; i < nf; i++) {
+    const int p = fsrc[i].first;
+    Front f = parts[p].fronts[fsrc[i].second];
+    tmap[p].push_back({f.dof_off, (int64_t)dofs.size(), f.N});
+    for (int k = 0; k < f.N; k++)
+      dofs.push_back((int32_t)(parts[p].dofs[f.dof_off + k] + dof_base[p]));
+    f.level += shift(p);
+    f.off += fbase[p];
+    f.dof_off = tmap[p].back()[1];
+    f.parent = f.parent >= 0 ? front_map[p][f.parent] : -1;
+    fronts[i] = f;
+  }
+  for (int i = 0; i < ns; i++) {
+    const int p = ssrc[i].first;
+    Sep q = parts[p].seps[ssrc[i].second];
+    tmap[p].push_back({q.dof_off, (int64_t)dofs.size(), q.s});
+    for (int k = 0; k < q.s; k++)
+      dofs.push_back((int32_t)(parts[p].dofs[q.dof_off + k] + dof_base[p]));
+    q.level += shift(p);
+    q.off += sbase[p];
+    q.dof_off = tmap[p].back()[1];
+    q.box[0] = front_map[p][q.box[0]];
+    q.box[1] = front_map[p][q.box[1]];
+    seps[i] = q;
+  }
+  for (auto& m : tmap) std::sort(m.begin(), m.end());
+  auto tpos = [&](int p, int64_t old) -> int32_t {   // old table index of part p -> new
+    const auto& m = tmap[p];
+    auto it = std::upper_bound(m.begin(), m.end(),
+                               std::array<int64_t, 3>{old, INT64_MAX, INT64_MAX});
+    if (it == m.begin()) throw std::logic_error("DOF table index outside every list");
+    --it;
+    if (old >= (*it)[0] + std::max<int64_t>((*it)[2], 1))
+      throw std::logic_error("DOF table index outside every list");
+    return (int32_t)((*it)[1] + (old - (*it)[0]));
+  };
+  auto remap = [&](Task t, int p, bool front_owner) {
+    t.dst_off += t.dst_arena == AR_FRONT ? fbase[p] : sbase[p];
+    t.src_off += t.src_arena == AR_FRONT ? fbase[p] : sbase[p];
+    if (t.kind == TK_SPARSE) {
+      t.row_dof = t.rows > 0 ? tpos(p, t.row_dof) : 0;
+      t.col_dof = t.cols > 0 ? tpos(p, t.col_dof) : 0;
+    }
+    t.owner = front_owner ? front_map[p][t.owner] : sep_map[p][t.owner];
+    return t;
+  };
+  front_task_ptr.assign(nf + 1, 0);
+  for (int i = 0; i < nf; i++) {
+    const Schedule& q = parts[fsrc[i].first];
+    const int lf = fsrc[i].second;
+    for (int64_t k = q.front_task_ptr[lf]; k < q.front_task_ptr[lf + 1]; k++)
+      front_tasks.push_back(remap(q.front_tasks[k], fsrc[i].first, true));
+    front_task_ptr[i + 1] = (int64_t)front_tasks.size();
+  }
+  sep_task_ptr.assign(ns + 1, 0);
+  for (int i = 0; i < ns; i++) {
+    const Schedule& q = parts[ssrc[i].first];
+    const int ls = ssrc[i].second;
+    for (int64_t k = q.sep_task_ptr[ls]; k < q.sep_task_ptr[ls + 1]; k++)
+      sep_tasks.push_back(remap(q.sep_tasks[k], ssrc[i].first, false));
+    sep_task_ptr[i + 1] = (int64_t)sep_tasks.size();
+    for (int k = 0; k < 2; k++)
+      sep_add_tasks.push_back(remap(q.sep_add_tasks[2 * (size_t)ls + k], ssrc[i].first, false));
+  }
+}
+
 int Schedule::leaf_of_dof(int dof) const {
+  if (forest()) {
+    const int p = (int)(std::upper_bound(dof_base.begin(), dof_base.end(), (int64_t)dof) -
+                        dof_base.begin()) - 1;
+    return front_map[p][parts[p].leaf_of_dof((int)(dof - dof_base[p]))];
+  }
   int bps = 1 << (levels - 1);
   int c[3];
   int64_t d = dof;
@@ -685,6 +831,26 @@ int Schedule::leaf_of_dof(int dof) const {
 size_t Schedule::dirty_fronts(const int* mod, int nmod, std::vector<char>& dirty) const {
   dirty.assign(fronts.size(), 0);
   size_t nd = 0;
+  if (forest()) {
+    // each touched problem refactors its own root paths (and its root)
+    std::vector<std::vector<int>> local(parts.size());
+    for (int i = 0; i < nmod; i++) {
+      const int p = (int)(std::upper_bound(dof_base.begin(), dof_base.end(), (int64_t)mod[i]) -
+                          dof_base.begin()) - 1;
+      local[p].push_back((int)(mod[i] - dof_base[p]));
+    }
+    for (size_t p = 0; p < parts.size(); p++) {
+      if (local[p].empty()) continue;
+      std::vector<char> d;
+      parts[p].dirty_fronts(local[p].data(), (int)local[p].size(), d);
+      for (size_t f = 0; f < d.size(); f++)
+        if (d[f]) {
+          dirty[front_map[p][f]] = 1;
+          nd++;
+        }
+    }
+    return nd;
+  }
   for (int i = 0; i < nmod; i++) {
     int f = leaf_of_dof(mod[i]);
     while (f >= 0 && !dirty[f]) {

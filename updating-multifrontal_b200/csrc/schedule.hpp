@@ -72,6 +72,21 @@ class Schedule {
   // Throws std::runtime_error with the reference's messages on bad parameters.
   Schedule(int dim, int nx, int ny, int nz, int width, int max_side);
 
+  // A batch of independent problems as one forest over their block-diagonal
+  // matrix.  Levels are aligned at the leaves: part p's level l is level
+  // l + (levels - parts[p].levels) here, so one launch per level covers the
+  // fronts of every problem at that height.  Fronts and separators are
+  // renumbered level by level (part by part inside a level), DOFs of part p
+  // are shifted by dof_base[p], arena offsets by the parts' arena sizes, and
+  // the DOF table keeps the single-problem layout (all fronts, then all
+  // separators).
+  explicit Schedule(std::vector<Schedule>&& batch);
+
+  std::vector<Schedule> parts;        // the batch members (empty for one problem)
+  std::vector<int64_t> dof_base;      // parts.size() + 1 DOF offsets
+  std::vector<std::vector<int>> front_map, sep_map;   // part-local id -> id here
+  bool forest() const { return !parts.empty(); }
+
   int dim, N[3], width, levels;
   int bw[3];                        // leaf box widths
   int64_t ndof;

@@ -18,8 +18,8 @@ from . import _lib
 from ._lib import MFGPU_FP64, MFGPU_MIXED, TASK_DTYPE
 from .stencil import CSR, build_laplacian
 
-__all__ = ["MF2D", "MF3D", "Symbolic", "CSR", "build_laplacian", "MFGPU_FP64", "MFGPU_MIXED",
-           "MFError"]
+__all__ = ["MF2D", "MF3D", "MFBatch", "Symbolic", "CSR", "build_laplacian", "MFGPU_FP64",
+           "MFGPU_MIXED", "MFError"]
 
 
 class MFError(RuntimeError):
@@ -170,6 +170,85 @@ class _MFBase:
         return {f: getattr(s, f) for f, _ in _lib.Stats._fields_}
 
 
+class MFBatch(_MFBase):
+    """Independent problems factored and solved together (mfgpu_batch_create).
+
+    `problems` is a list of (A, N, width, maxSideLength) with N = (Nx, Ny) or
+    (Nx, Ny, Nz).  The handle works on the block-diagonal matrix: vectors are
+    the problems' vectors stacked (row offsets in `self.offsets`); `join` and
+    `split` convert.  Update(A_list, mods) takes the new matrices (None keeps a
+    problem unchanged) and the per-problem modified DOFs (local numbering).
+    """
+
+    def __init__(self, problems, precision=MFGPU_FP64, device=0, refine_tol=1e-10,
+                 refine_maxit=50):
+        lib = _lib.load()
+        mats, geo = [], []
+        for A, N, width, ms in problems:
+            if not isinstance(A, CSR):
+                A = CSR(A.indptr, A.indices, A.data, A.shape[0])
+            N = tuple(int(x) for x in N)
+            mats.append(A)
+            geo.append((len(N), N[0], N[1], N[2] if len(N) == 3 else 1, int(width), int(ms)))
+        self.mats = mats
+        self.A = _block_diag(mats)
+        cols = [np.ascontiguousarray([g[k] for g in geo], np.int32) for k in range(6)]
+        opts = _lib.default_options(precision, device, refine_tol, refine_maxit)
+        h = C.c_void_p()
+        st = lib.mfgpu_batch_create(len(problems), *[_lib._ptr(c) for c in cols], int(self.A.n),
+                                    _lib._ptr(self.A.row_ptr), _lib._ptr(self.A.col_ind),
+                                    _lib._ptr(self.A.val), C.byref(opts), C.byref(h))
+        if st != _lib.MFGPU_OK:
+            _raise(st, lib.mfgpu_last_error(None).decode())
+        self._h = h
+        self._lib = lib
+        cnt = C.c_int()
+        offs = np.zeros(len(problems) + 1, np.int64)
+        self._check(lib.mfgpu_batch_info(h, C.byref(cnt),
+                                         offs.ctypes.data_as(C.POINTER(C.c_int64))))
+        self.offsets = offs
+        self.N = None
+
+    def join(self, vecs, nrhs=None):
+        """Stack per-problem right-hand sides ((n_p,) or (n_p, k_p)) into (n, nrhs),
+        zero-padding problems with fewer columns."""
+        vs = [np.asarray(v, np.float64).reshape(len(v), -1) for v in vecs]
+        k = nrhs or max(v.shape[1] for v in vs)
+        out = np.zeros((int(self.offsets[-1]), k), order="F")
+        for p, v in enumerate(vs):
+            out[self.offsets[p]:self.offsets[p + 1], :v.shape[1]] = v
+        return out
+
+    def split(self, X):
+        return [X[self.offsets[p]:self.offsets[p + 1]] for p in range(len(self.offsets) - 1)]
+
+    def Update(self, A_list, mods):
+        """A_list[p]: new matrix of problem p (same pattern) or None; mods[p]: its
+        modified DOFs (local numbering)."""
+        mats = [self.mats[p] if A is None else (A if isinstance(A, CSR) else
+                CSR(A.indptr, A.indices, A.data, A.shape[0])) for p, A in enumerate(A_list)]
+        allmod = []
+        for p, m in enumerate(mods):
+            allmod.extend(int(d) + int(self.offsets[p]) for d in (m if m is not None else ()))
+        B = _block_diag(mats)
+        mod = np.ascontiguousarray(sorted(set(allmod)), np.int32)
+        self._check(self._lib.mfgpu_update(self._h, _lib._ptr(B.val), B.nnz, _lib._ptr(mod),
+                                           len(mod)))
+        self.mats, self.A = mats, B
+
+
+def _block_diag(mats):
+    rp, ci, va = [np.zeros(1, np.int32)], [], []
+    rows = nnz = 0
+    for A in mats:
+        rp.append((A.row_ptr[1:].astype(np.int64) + nnz).astype(np.int32))
+        ci.append((A.col_ind.astype(np.int64) + rows).astype(np.int32))
+        va.append(A.val)
+        rows += A.n
+        nnz += A.nnz
+    return CSR(np.concatenate(rp), np.concatenate(ci), np.concatenate(va), rows)
+
+
 class MF2D(_MFBase):
     """MF2D(A, Nx, Ny, width=1, maxSideLength=4)."""
     _dim = 2
@@ -189,11 +268,19 @@ class MF3D(_MFBase):
 class Symbolic:
     """Host-only view of the schedule: DOF lists and assembly tasks."""
 
-    def __init__(self, dim, N, width=1, max_side_length=4):
+    def __init__(self, dim, N, width=1, max_side_length=4, batch=None):
+        """One problem, or with batch=[(dim, N, width, maxSideLength), ...] the
+        forest schedule of a batch (dim, N, width, max_side_length ignored)."""
         lib = _lib.load()
         h = C.c_void_p()
-        Nz = N[2] if dim == 3 else 1
-        st = lib.mfgpu_symbolic_create(dim, N[0], N[1], Nz, width, max_side_length, C.byref(h))
+        if batch is not None:
+            cols = [np.ascontiguousarray(c, np.int32) for c in zip(
+                *[(d, n[0], n[1], n[2] if d == 3 else 1, w, m) for d, n, w, m in batch])]
+            st = lib.mfgpu_symbolic_batch_create(len(batch), *[_lib._ptr(c) for c in cols],
+                                                 C.byref(h))
+        else:
+            Nz = N[2] if dim == 3 else 1
+            st = lib.mfgpu_symbolic_create(dim, N[0], N[1], Nz, width, max_side_length, C.byref(h))
         if st != _lib.MFGPU_OK:
             _raise(st, lib.mfgpu_symbolic_error().decode())
         self._h, self._lib = h, lib

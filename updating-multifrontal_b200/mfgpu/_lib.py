@@ -30,7 +30,8 @@ EXPORTED = [
     "mfgpu_symbolic_sizes", "mfgpu_symbolic_front", "mfgpu_symbolic_sep", "mfgpu_symbolic_tasks",
     "mfgpu_symbolic_layout", "mfgpu_update_device", "mfgpu_refactor", "mfgpu_refactor_device",
     "mfgpu_profile_enable", "mfgpu_profile_reset", "mfgpu_profile_read", "mfgpu_kernel_launches",
-    "mfgpu_symbolic_dirty",
+    "mfgpu_symbolic_dirty", "mfgpu_batch_create", "mfgpu_batch_info",
+    "mfgpu_symbolic_batch_create",
 ]
 
 KERNEL_CLASSES = ["assemble", "potrf", "trsm", "syrk", "solve", "apply", "front", "coop", "tc"]
@@ -82,6 +83,11 @@ def load(path=None):
     lib.mfgpu_create.argtypes = [C.c_int] * 7 + [C.c_void_p, C.c_void_p, C.c_void_p,
                                                  C.POINTER(Options), C.POINTER(P)]
     lib.mfgpu_create.restype = C.c_int
+    lib.mfgpu_batch_create.argtypes = [C.c_int] + [C.c_void_p] * 6 + [
+        C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Options), C.POINTER(P)]
+    lib.mfgpu_batch_create.restype = C.c_int
+    lib.mfgpu_batch_info.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int64)]
+    lib.mfgpu_batch_info.restype = C.c_int
     lib.mfgpu_factor.argtypes = [P]
     lib.mfgpu_factor.restype = C.c_int
     lib.mfgpu_update.argtypes = [P, C.c_void_p, C.c_int64, C.c_void_p, C.c_int]
@@ -116,6 +122,8 @@ def load(path=None):
     lib.mfgpu_destroy.restype = None
     lib.mfgpu_symbolic_create.argtypes = [C.c_int] * 6 + [C.POINTER(P)]
     lib.mfgpu_symbolic_create.restype = C.c_int
+    lib.mfgpu_symbolic_batch_create.argtypes = [C.c_int] + [C.c_void_p] * 6 + [C.POINTER(P)]
+    lib.mfgpu_symbolic_batch_create.restype = C.c_int
     lib.mfgpu_symbolic_destroy.argtypes = [P]
     lib.mfgpu_symbolic_destroy.restype = None
     lib.mfgpu_symbolic_error.argtypes = []
