@@ -50,6 +50,9 @@ WORKLOADS = {
     # the 3D workload (log-uniform [0.1, 100], leaf parameter 4, one RHS)
     "3d-127": dict(dim=3, N=(127, 127, 127), max_side=4, lo=0.1, hi=100.0, nrhs=1, patch=9,
                    factor=10.0, seed=SEED0 + 3),
+    # 256 independent 2D problems in one handle (sides 63..511, 1-8 RHS each)
+    "batch256": dict(batch=True, count=256, sides=(63, 127, 255, 511), max_side=4, lo=0.1, hi=10.0,
+                     max_nrhs=8, seed=SEED0 + 5),
     # a smaller 3D case of the same kind (profiling captures, quick checks)
     "3d-63": dict(dim=3, N=(63, 63, 63), max_side=4, lo=0.1, hi=100.0, nrhs=1, patch=5,
                   factor=10.0, seed=SEED0 + 4),
@@ -188,6 +191,8 @@ def run_reference_arm(args, w):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if w.get("batch"):
+        return run_reference_arm_batch(args, w)
     a1, a2, A1, A2, mod, b = make_problem(w)
     fl = front_sizes(w)
     factor_fl = sum(n ** 3 / 3.0 + n * n * m + n * m * m for n, m in fl)
@@ -226,6 +231,59 @@ def run_reference_arm(args, w):
     return 0
 
 
+def run_reference_arm_batch(args, w):
+    """Reference arm of a batch workload: the reference factors and solves one
+    problem per object, so each sample runs the batch's members one at a time
+    (from the first) for about 20 s; value = their algorithmic flops / time."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refio
+    from mfgpu import Symbolic
+    if not refio.have_reference():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference harness oracle/_ref/ref_harness not built"}))
+        return 0
+    members = make_batch(w)
+    threads = os.cpu_count() or 1
+    cache = {}
+    samples = []
+    for rep in range(1 + max(1, args.steps)):
+        t_tot, fl_tot, used = 0.0, 0.0, 0
+        for dim, N, ms, a, A, b in members:
+            if t_tot > 20.0:
+                break
+            with tempfile.TemporaryDirectory() as d:
+                res = refio.time_reference(d, dim, N, 1, ms, a, None, b, reps=1, solve_reps=1,
+                                           threads=threads)
+            t_tot += res["factor_s"][0] + res["solve_s"][0]
+            if N not in cache:
+                Sp = Symbolic(dim, N, 1, ms)
+                cache[N] = [(Sp.front(f)["n"], Sp.front(f)["m"]) for f in range(Sp.n_fronts)]
+            fr = cache[N]
+            fl_tot += sum(n ** 3 / 3.0 + n * n * m + n * m * m for n, m in fr)
+            fl_tot += solve_flops(fr, b.shape[0])
+            used += 1
+        if rep > 0:
+            samples.append((t_tot, fl_tot, used))
+    vals = [fl / t / 1e12 for t, fl, _ in samples]
+    value = statistics.median(vals)
+    model, _ = cpu_info()
+    t_med = statistics.median([t for t, _, _ in samples])
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s",
+        "n_gpus": args.gpus, "steps": len(samples), "warmup": 1, "ms_per_step": t_med * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded coefficients and right-hand sides)",
+        "config": {"workload": args.workload, "precision": args.precision,
+                   "sample": f"first {samples[0][2]} of {len(members)} problems per step"},
+        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": threads, "kind": "reference",
+                         "sample": f"factor + solve of the first {samples[0][2]} batch members, "
+                                   f"one at a time, OPENBLAS_NUM_THREADS={threads}", "cpu": model},
+        "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def update_flops(w, mod):
     """Flops of the fronts a localized update refactors (root paths of dirty leaves)."""
     from mfgpu import Symbolic
@@ -243,6 +301,192 @@ def config_of(w, args):
             "grid": list(w["N"]), "max_side_length": w["max_side"], "nrhs": w["nrhs"],
             "precision": args.precision, "parallelism": f"replicas x{args.gpus}",
             "l2": "inputs larger than L2 (front arena > 126 MB)"}
+
+
+class SingleWork:
+    """One problem: step = full factorization + localized update + solve."""
+
+    def __init__(self, w, rank, local, prec):
+        from mfgpu import MF2D, MF3D
+        self.w = w
+        self.a1, self.a2, self.A1, self.A2, self.mod, self.b = make_problem(w, rank)
+        self.n, self.nnz, self.nrhs = self.A1.n, self.A1.nnz, w["nrhs"]
+        N = w["N"]
+        if w["dim"] == 2:
+            self.F = MF2D(self.A1, N[0], N[1], 1, w["max_side"], device=local, precision=prec)
+        else:
+            self.F = MF3D(self.A1, N[0], N[1], N[2], 1, w["max_side"], device=local,
+                          precision=prec)
+        self.fl = front_sizes(w)
+        self.upd_fl = update_flops(w, self.mod)
+
+    def to_device(self, torch):
+        self.dv1 = torch.from_numpy(self.A1.val).to("cuda")
+        self.dv2 = torch.from_numpy(self.A2.val).to("cuda")
+        self.db = torch.from_numpy(np.ascontiguousarray(self.b)).to("cuda")   # column-major n x nrhs
+        self.dx = torch.empty_like(self.db)
+
+    def step(self):
+        F = self.F
+        F.refactor_device(self.dv1.data_ptr(), self.nnz)
+        F.update_device(self.dv2.data_ptr(), self.nnz, self.mod)
+        F.solve_device(self.db.data_ptr(), self.dx.data_ptr(), self.nrhs, self.n)
+
+    def resid(self):
+        x = self.dx.cpu().numpy()
+        return max(float(np.linalg.norm(self.A2.matvec(x[r]) - self.b[r]) /
+                         np.linalg.norm(self.b[r])) for r in range(self.nrhs))
+
+    def flops_breakdown(self):
+        return {"factor": self.F.info()["factor_flops"], "update": self.upd_fl,
+                "solve": solve_flops(self.fl, self.nrhs)}
+
+    def step_flops(self):
+        return sum(self.flops_breakdown().values())
+
+    def e2e_setup(self, torch):
+        self.hv1 = torch.from_numpy(self.A1.val).pin_memory()
+        self.hv2 = torch.from_numpy(self.A2.val).pin_memory()
+        self.hb = torch.from_numpy(np.ascontiguousarray(self.b)).pin_memory()
+        self.hx = torch.empty_like(self.hb).pin_memory()
+        self.mod32 = np.ascontiguousarray(self.mod, np.int32)
+
+    def e2e_step(self):
+        F = self.F
+        F.refactor_host_ptr(self.hv1.data_ptr(), self.nnz)
+        F.update_host_ptr(self.hv2.data_ptr(), self.nnz, self.mod32)
+        F.solve_host_ptr(self.hb.data_ptr(), self.hx.data_ptr(), self.nrhs, self.n)
+
+    def e2e_bytes(self):
+        return (2 * self.nnz * 8 + self.n * self.nrhs * 8 + self.mod32.size * 4,
+                self.n * self.nrhs * 8)
+
+    def config(self, args):
+        return config_of(self.w, args)
+
+    def cpu_baseline(self, threads):
+        res = reference_time(self.w, self.a1, self.a2, self.b, threads, reps=1, solve_reps=1)
+        if res is None:
+            return None
+        tcpu = res["factor_s"][0] + res["update_s"][0] + res["solve_s"][0]
+        model, _ = cpu_info()
+        return {"value": self.step_flops() / tcpu / 1e12, "unit": "TFLOP/s", "cores": threads,
+                "kind": "reference",
+                "sample": f"1 x (factor + update + {self.nrhs}-RHS solve) of the full workload "
+                          f"({tcpu:.2f} s), OPENBLAS_NUM_THREADS={threads}", "cpu": model}
+
+
+def make_batch(w, rank=0):
+    """The batch members: (dim, N, maxSideLength, coefficients, CSR, rhs (k, n))."""
+    seed = w["seed"] + 1000 * rank
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sides = rng.choice(np.asarray(w["sides"]), size=w["count"])
+    ks = rng.integers(1, w["max_nrhs"] + 1, size=w["count"])
+    out = []
+    for i, (side, k) in enumerate(zip(sides, ks)):
+        N = (int(side), int(side))
+        a = stencil.loguniform_coefficients(N, w["lo"], w["hi"], seed + 1 + i)
+        A = stencil.build_laplacian(a)
+        b = stencil.uniform_rhs(A.n, int(k), seed + 100000 + i)
+        out.append((2, N, w["max_side"], a, A, b))
+    return out
+
+
+class BatchWork:
+    """Independent problems in one handle: step = factorization of every
+    problem + one solve with every problem's right-hand sides."""
+
+    def __init__(self, w, rank, local, prec):
+        from mfgpu import MFBatch, Symbolic
+        self.w = w
+        self.members = make_batch(w, rank)
+        self.F = MFBatch([(A, N, 1, ms) for dim, N, ms, a, A, b in self.members], device=local,
+                         precision=prec)
+        self.A = self.F.A
+        self.n, self.nnz = self.A.n, self.A.nnz
+        self.nrhs = max(b.shape[0] for *_, b in self.members)
+        self.B = self.F.join([b.T for *_, b in self.members], self.nrhs)
+        self.factor_fl = self.F.info()["factor_flops"]
+        self.solve_fl = 0.0
+        cache = {}
+        for dim, N, ms, a, A, b in self.members:
+            if N not in cache:
+                Sp = Symbolic(dim, N, 1, ms)
+                cache[N] = [(Sp.front(f)["n"], Sp.front(f)["m"]) for f in range(Sp.n_fronts)]
+            self.solve_fl += solve_flops(cache[N], b.shape[0])
+        self.sizes = cache
+
+    def to_device(self, torch):
+        self.dv = torch.from_numpy(self.A.val).to("cuda")
+        self.db = torch.from_numpy(np.ascontiguousarray(self.B.T)).to("cuda")   # (nrhs, n)
+        self.dx = torch.empty_like(self.db)
+
+    def step(self):
+        self.F.refactor_device(self.dv.data_ptr(), self.nnz)
+        self.F.solve_device(self.db.data_ptr(), self.dx.data_ptr(), self.nrhs, self.n)
+
+    def resid(self):
+        X = self.dx.cpu().numpy().T
+        worst = 0.0
+        for (dim, N, ms, a, A, b), x in zip(self.members, self.F.split(X)):
+            for c in range(b.shape[0]):
+                worst = max(worst, float(np.linalg.norm(A.matvec(x[:, c]) - b[c]) /
+                                         np.linalg.norm(b[c])))
+        return worst
+
+    def flops_breakdown(self):
+        return {"factor": self.factor_fl, "update": 0.0, "solve": self.solve_fl}
+
+    def step_flops(self):
+        return self.factor_fl + self.solve_fl
+
+    def e2e_setup(self, torch):
+        self.hv = torch.from_numpy(self.A.val).pin_memory()
+        self.hb = torch.from_numpy(np.ascontiguousarray(self.B.T)).pin_memory()
+        self.hx = torch.empty_like(self.hb).pin_memory()
+
+    def e2e_step(self):
+        self.F.refactor_host_ptr(self.hv.data_ptr(), self.nnz)
+        self.F.solve_host_ptr(self.hb.data_ptr(), self.hx.data_ptr(), self.nrhs, self.n)
+
+    def e2e_bytes(self):
+        return self.nnz * 8 + self.n * self.nrhs * 8, self.n * self.nrhs * 8
+
+    def config(self, args):
+        sides = [N[0] for _, N, *_ in self.members]
+        return {"workload": f"{args.workload} ({self.w['count']} 2D 5-point problems, sides from "
+                            f"{sorted(set(self.w['sides']))}, a log-U[{self.w['lo']},{self.w['hi']}], "
+                            f"maxSideLength {self.w['max_side']}, 1-{self.w['max_nrhs']} RHS each; "
+                            "step = factor + solve of every problem)",
+                "problems": len(self.members), "ndof": self.n,
+                "sides_count": {str(s): sides.count(s) for s in sorted(set(sides))},
+                "nrhs_total": int(sum(b.shape[0] for *_, b in self.members)),
+                "precision": args.precision, "parallelism": f"replicas x{args.gpus}",
+                "l2": "inputs larger than L2 (front arena > 126 MB)"}
+
+    def cpu_baseline(self, threads):
+        # the reference on the batch's first members, one at a time, about 20 s
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import refio
+        if not refio.have_reference():
+            return None
+        t_tot, fl_tot, used = 0.0, 0.0, 0
+        for dim, N, ms, a, A, b in self.members:
+            if t_tot > 20.0:
+                break
+            with tempfile.TemporaryDirectory() as d:
+                res = refio.time_reference(d, dim, N, 1, ms, a, None, b, reps=1, solve_reps=1,
+                                           threads=threads)
+            t_tot += res["factor_s"][0] + res["solve_s"][0]
+            fr = self.sizes[N]
+            fl_tot += sum(n ** 3 / 3.0 + n * n * m + n * m * m for n, m in fr)
+            fl_tot += solve_flops(fr, b.shape[0])
+            used += 1
+        model, _ = cpu_info()
+        return {"value": fl_tot / t_tot / 1e12, "unit": "TFLOP/s", "cores": threads,
+                "kind": "reference",
+                "sample": f"factor + solve of the first {used} batch members one at a time "
+                          f"({t_tot:.2f} s), OPENBLAS_NUM_THREADS={threads}", "cpu": model}
 
 
 def main():
@@ -273,37 +517,19 @@ def main():
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    a1, a2, A1, A2, mod, b = make_problem(w, rank)
-    n, nnz, nrhs = A1.n, A1.nnz, w["nrhs"]
-    if w["dim"] == 2:
-        F = MF2D(A1, w["N"][0], w["N"][1], 1, w["max_side"], device=local, precision=prec)
-    else:
-        F = MF3D(A1, w["N"][0], w["N"][1], w["N"][2], 1, w["max_side"], device=local,
-                 precision=prec)
+    work = (BatchWork if w.get("batch") else SingleWork)(w, rank, local, prec)
+    F = work.F
     stream = torch.cuda.Stream()
     F.set_stream(stream.cuda_stream)
-    dv1 = torch.from_numpy(A1.val).to("cuda")
-    dv2 = torch.from_numpy(A2.val).to("cuda")
-    db = torch.from_numpy(np.ascontiguousarray(b)).to("cuda")      # (nrhs, n): column-major n x nrhs
-    dx = torch.empty_like(db)
+    work.to_device(torch)
     torch.cuda.synchronize()
-
-    def step():
-        F.refactor_device(dv1.data_ptr(), nnz)
-        F.update_device(dv2.data_ptr(), nnz, mod)
-        F.solve_device(db.data_ptr(), dx.data_ptr(), nrhs, n)
+    step = work.step
 
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
-    # correctness of what is timed: residual of the updated system in FP64
-    x = dx.cpu().numpy()
-    resid = max(float(np.linalg.norm(A2.matvec(x[r]) - b[r]) / np.linalg.norm(b[r]))
-                for r in range(nrhs))
-    info = F.info()
-    fl = front_sizes(w)
-    upd_fl = update_flops(w, mod)
-    step_fl = info["factor_flops"] + upd_fl + solve_flops(fl, nrhs)
+    resid = work.resid()      # correctness of what is timed, in FP64 on the host
+    step_fl = work.step_flops()
 
     if world > 1:
         dist.barrier()
@@ -343,25 +569,15 @@ def main():
     value = world * args.steps * step_fl / (ms_max * 1e-3) / 1e12
 
     # end to end through the public API with pinned host buffers
-    hv1 = torch.from_numpy(A1.val).pin_memory()
-    hv2 = torch.from_numpy(A2.val).pin_memory()
-    hb = torch.from_numpy(np.ascontiguousarray(b)).pin_memory()
-    hx = torch.empty_like(hb).pin_memory()
-    mod32 = np.ascontiguousarray(mod, np.int32)
+    work.e2e_setup(torch)
     F.set_stream(stream.cuda_stream)
-
-    def e2e_step():
-        F.refactor_host_ptr(hv1.data_ptr(), nnz)
-        F.update_host_ptr(hv2.data_ptr(), nnz, mod32)
-        F.solve_host_ptr(hb.data_ptr(), hx.data_ptr(), nrhs, n)
-
-    e2e_step()
+    work.e2e_step()
     torch.cuda.synchronize()
     ee0 = torch.cuda.Event(enable_timing=True)
     ee1 = torch.cuda.Event(enable_timing=True)
     ee0.record(stream)
     for _ in range(args.steps):
-        e2e_step()
+        work.e2e_step()
     ee1.record(stream)
     ee1.synchronize()
     e2e_ms = ee0.elapsed_time(ee1)
@@ -369,8 +585,7 @@ def main():
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = world * args.steps * step_fl / (float(te.item()) * 1e-3) / 1e12
-    h2d = 2 * nnz * 8 + n * nrhs * 8 + mod32.size * 4
-    d2h = n * nrhs * 8
+    h2d, d2h = work.e2e_bytes()
 
     # roofline of the dominant kernel class in the timed region
     peaks, peak_src = measured_peaks()
@@ -407,15 +622,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        res = reference_time(w, a1, a2, b, threads, reps=1, solve_reps=1)
-        if res is not None:
-            tcpu = res["factor_s"][0] + res["update_s"][0] + res["solve_s"][0]
-            model, _ = cpu_info()
-            cpu = {"value": step_fl / tcpu / 1e12, "unit": "TFLOP/s", "cores": threads,
-                   "kind": "reference",
-                   "sample": f"1 x (factor + update + {nrhs}-RHS solve) of the full workload "
-                             f"({tcpu:.2f} s), OPENBLAS_NUM_THREADS={threads}", "cpu": model}
+        cpu = work.cpu_baseline(os.cpu_count() or 1)
 
     if rank == 0:
         line = {
@@ -424,13 +631,12 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32 factor + f64 refinement",
             "data": "synthetic (seeded coefficients and right-hand sides)",
-            "config": config_of(w, args),
+            "config": work.config(args),
             "step_ms_p50": statistics.median(step_ms),
             "step_ms_p99": float(np.percentile(step_ms, 99)),
             "resid": resid,
             "refine_iterations": F.stats()["iterations"] if args.precision == "mixed" else 0,
-            "flops_per_step": {"factor": info["factor_flops"], "update": upd_fl,
-                               "solve": solve_flops(fl, nrhs)},
+            "flops_per_step": work.flops_breakdown(),
             "kernel_classes": {k: {"launches": v["launches"], "ms": v["ms"]} for k, v in prof.items()},
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
