@@ -81,6 +81,23 @@ int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side_length
                  const int* row_ptr, const int* col_ind, const double* val,
                  const mfgpu_options* opts, mfgpu_handle** out);
 
+/* Stencil assembly on the device (no reference counterpart; restates the
+ * reference fixture test_include/DE/buildLaplacian.hpp:10-132, 244-391 for
+ * width 1, bit for bit).  d_coef: node coefficients, (nx+2) x (ny+2)
+ * [x (nz+2)] doubles, C order with x slowest; hxyz: grid spacings (null = 1).
+ * Writes every CSR value of the handle's pattern into d_val (nnz doubles). */
+int mfgpu_stencil_assemble_device(mfgpu_handle* h, const double* d_coef, const double* hxyz,
+                                  double* d_val);
+
+/* After the coefficients of the cells in the box [box_lo, box_hi) changed
+ * (d_coef holds the new array), recompute the affected rows of d_val in place
+ * and return the modified DOFs (rows with a changed entry, sorted: the set the
+ * reference's test computes on the host, test_src/DE/testMF2D.cpp:143-150),
+ * ready for mfgpu_update_device. */
+int mfgpu_stencil_update_device(mfgpu_handle* h, const double* d_coef, const double* hxyz,
+                                const int* box_lo, const int* box_hi, double* d_val,
+                                int* modified_dofs, int capacity, int* n_modified);
+
 /* Batch of independent problems in one handle (no reference counterpart; the
  * reference factors one problem per MF2D/MF3D object).  Problem p has the
  * geometry (dim[p], nx[p], ny[p], nz[p], width[p], max_side[p]); the matrix is

@@ -95,6 +95,15 @@ cudaError_t launch_solve_coop(bool forward, const int* flist, int nf, int maxn, 
                               const T* F, const int* dofs, T* X, int64_t ldx, int nrhs, T* W,
                               const int64_t* woff, cudaStream_t st);
 
+// Stencil assembly (width 1): recompute the CSR values of the rows of the
+// cells in [lo, hi) from the node coefficients; with `flag`, record which rows
+// changed; launch_collect_rows appends the flagged rows to `out`.
+cudaError_t launch_stencil_rows(int dim, int nx, int ny, int nz, const double h[3], const double* a,
+                                const int* rp, double* val, const int lo[3], const int hi[3],
+                                int* flag, cudaStream_t st);
+cudaError_t launch_collect_rows(int dim, int nx, int ny, const int lo[3], const int hi[3],
+                                const int* flag, int* out, int cap, int* count, cudaStream_t st);
+
 // Number of kernels this library has launched since it was loaded.
 long long launches_total();
 

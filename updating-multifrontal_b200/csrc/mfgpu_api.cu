@@ -265,6 +265,10 @@ struct mfgpu_handle {
   int* d_segrow = nullptr;         // nseg + 1 segment boundaries (rows)
   int* d_chunkrow = nullptr;       // nchunks + 1 dot chunk boundaries (rows)
   int* d_segchunk = nullptr;       // nseg + 1: first dot chunk of each segment
+  // device stencil assembly: per-row change flags (+ a counter) and the rows found
+  int* d_flag = nullptr;
+  int* d_modbuf = nullptr;
+  size_t capMod = 0;
   int* d_all = nullptr;      // every front id then every separator id, level order
   int64_t woffTotal = 0;     // sum over fronts of 2N
   Plan full, upd;
@@ -308,6 +312,8 @@ struct mfgpu_handle {
     cudaFree(d_segrow);
     cudaFree(d_chunkrow);
     cudaFree(d_segchunk);
+    cudaFree(d_flag);
+    cudaFree(d_modbuf);
     cudaFree(d_all);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -1289,6 +1295,73 @@ int mfgpu_solve_device_noalloc(mfgpu_handle* h, const double* d_b, double* d_x, 
       h->solveChunkScratch(X, ld, nc, W);
     }
     ck(cudaStreamSynchronize(h->stream), "solve");
+  });
+}
+
+// ---- stencil assembly on the device ----
+
+int mfgpu_stencil_assemble_device(mfgpu_handle* h, const double* d_coef, const double* hxyz,
+                                  double* d_val) {
+  if (!h) return MFGPU_ERR_ARG;
+  const Schedule& s = *h->S;
+  if (s.forest() || s.width != 1 || !d_coef || !d_val)
+    return fail(h, MFGPU_ERR_ARG,
+                "stencil assembly needs one problem of width 1 and non-null pointers");
+  const double hh[3] = {hxyz ? hxyz[0] : 1.0, hxyz ? hxyz[1] : 1.0, hxyz ? hxyz[2] : 1.0};
+  return guarded(h, [&]() {
+    const int lo[3] = {0, 0, 0}, hi[3] = {s.N[0], s.N[1], s.dim == 3 ? s.N[2] : 1};
+    ck(mfgpu::launch_stencil_rows(s.dim, s.N[0], s.N[1], s.N[2], hh, d_coef, h->d_rp, d_val, lo,
+                                  hi, nullptr, h->stream),
+       "launch stencil assembly (k_stencil_rows)");
+    ck(cudaStreamSynchronize(h->stream), "stencil assembly");
+  });
+}
+
+int mfgpu_stencil_update_device(mfgpu_handle* h, const double* d_coef, const double* hxyz,
+                                const int* box_lo, const int* box_hi, double* d_val,
+                                int* modified_dofs, int capacity, int* n_modified) {
+  if (!h) return MFGPU_ERR_ARG;
+  const Schedule& s = *h->S;
+  if (s.forest() || s.width != 1 || !d_coef || !d_val || !box_lo || !box_hi || !n_modified)
+    return fail(h, MFGPU_ERR_ARG,
+                "stencil update needs one problem of width 1 and non-null pointers");
+  const double hh[3] = {hxyz ? hxyz[0] : 1.0, hxyz ? hxyz[1] : 1.0, hxyz ? hxyz[2] : 1.0};
+  // rows whose stencil reads a node of the changed cells: the box grown by one
+  int lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+  int64_t cells = 1;
+  for (int a = 0; a < s.dim; a++) {
+    lo[a] = std::max(0, box_lo[a] - 1);
+    hi[a] = std::min(s.N[a], box_hi[a] + 1);
+    if (hi[a] <= lo[a]) {
+      *n_modified = 0;
+      return MFGPU_OK;
+    }
+    cells *= hi[a] - lo[a];
+  }
+  return guarded(h, [&]() {
+    if (!h->d_flag) h->d_flag = dalloc<int>((size_t)h->n + 1, "alloc row flags");
+    h->growBuf(h->d_modbuf, h->capMod, (size_t)cells, "alloc modified rows");
+    int* d_count = h->d_flag + h->n;
+    ck(cudaMemsetAsync(d_count, 0, sizeof(int), h->stream), "clear count");
+    ck(mfgpu::launch_stencil_rows(s.dim, s.N[0], s.N[1], s.N[2], hh, d_coef, h->d_rp, d_val, lo,
+                                  hi, h->d_flag, h->stream),
+       "launch stencil update (k_stencil_rows)");
+    ck(mfgpu::launch_collect_rows(s.dim, s.N[0], s.N[1], lo, hi, h->d_flag, h->d_modbuf,
+                                  (int)cells, d_count, h->stream),
+       "launch modified-row collection (k_collect)");
+    int cnt = 0;
+    ck(cudaMemcpyAsync(&cnt, d_count, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "read count");
+    ck(cudaStreamSynchronize(h->stream), "stencil update");
+    std::vector<int> rows(cnt);
+    if (cnt)
+      ck(cudaMemcpy(rows.data(), h->d_modbuf, cnt * sizeof(int), cudaMemcpyDeviceToHost),
+         "read modified rows");
+    std::sort(rows.begin(), rows.end());
+    *n_modified = cnt;
+    if (modified_dofs) {
+      if (cnt > capacity) throw CudaError("modified-DOF buffer too small", MFGPU_ERR_ARG);
+      std::copy(rows.begin(), rows.end(), modified_dofs);
+    }
   });
 }
 

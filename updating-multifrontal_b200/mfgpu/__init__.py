@@ -155,6 +155,29 @@ class _MFBase:
         self._check(self._lib.mfgpu_apply_device(self._h, C.c_void_p(x_ptr), C.c_void_p(b_ptr),
                                                  nrhs, ld))
 
+    def stencil_assemble_device(self, coef_ptr, val_ptr, h=(1.0, 1.0, 1.0)):
+        """CSR values of the handle's stencil from device coefficients (bit-exact
+        with stencil.build_laplacian) into the device array at val_ptr."""
+        hh = np.ascontiguousarray(h, np.float64)
+        self._check(self._lib.mfgpu_stencil_assemble_device(self._h, C.c_void_p(coef_ptr),
+                                                            _lib._ptr(hh), C.c_void_p(val_ptr)))
+
+    def stencil_update_device(self, coef_ptr, lo, hi, val_ptr, h=(1.0, 1.0, 1.0)):
+        """Recompute the rows touched by the cell box [lo, hi) in place; returns
+        the modified DOFs (sorted int32 array)."""
+        hh = np.ascontiguousarray(h, np.float64)
+        lo3 = np.ascontiguousarray(list(lo) + [0] * (3 - len(lo)), np.int32)
+        hi3 = np.ascontiguousarray(list(hi) + [1] * (3 - len(hi)), np.int32)
+        cnt = C.c_int()
+        self._check(self._lib.mfgpu_stencil_update_device(
+            self._h, C.c_void_p(coef_ptr), _lib._ptr(hh), _lib._ptr(lo3), _lib._ptr(hi3),
+            C.c_void_p(val_ptr), None, 0, C.byref(cnt)))
+        out = np.zeros(max(1, cnt.value), np.int32)
+        self._check(self._lib.mfgpu_stencil_update_device(
+            self._h, C.c_void_p(coef_ptr), _lib._ptr(hh), _lib._ptr(lo3), _lib._ptr(hi3),
+            C.c_void_p(val_ptr), _lib._ptr(out), len(out), C.byref(cnt)))
+        return out[:cnt.value]
+
     def set_stream(self, stream_ptr):
         self._check(self._lib.mfgpu_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
 

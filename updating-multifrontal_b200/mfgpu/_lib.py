@@ -31,7 +31,7 @@ EXPORTED = [
     "mfgpu_symbolic_layout", "mfgpu_update_device", "mfgpu_refactor", "mfgpu_refactor_device",
     "mfgpu_profile_enable", "mfgpu_profile_reset", "mfgpu_profile_read", "mfgpu_kernel_launches",
     "mfgpu_symbolic_dirty", "mfgpu_batch_create", "mfgpu_batch_info",
-    "mfgpu_symbolic_batch_create",
+    "mfgpu_symbolic_batch_create", "mfgpu_stencil_assemble_device", "mfgpu_stencil_update_device",
 ]
 
 KERNEL_CLASSES = ["assemble", "potrf", "trsm", "syrk", "solve", "apply", "front", "coop", "tc"]
@@ -124,6 +124,12 @@ def load(path=None):
     lib.mfgpu_symbolic_create.restype = C.c_int
     lib.mfgpu_symbolic_batch_create.argtypes = [C.c_int] + [C.c_void_p] * 6 + [C.POINTER(P)]
     lib.mfgpu_symbolic_batch_create.restype = C.c_int
+    lib.mfgpu_stencil_assemble_device.argtypes = [P, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.mfgpu_stencil_assemble_device.restype = C.c_int
+    lib.mfgpu_stencil_update_device.argtypes = [P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_void_p, C.c_void_p, C.c_int,
+                                                C.POINTER(C.c_int)]
+    lib.mfgpu_stencil_update_device.restype = C.c_int
     lib.mfgpu_symbolic_destroy.argtypes = [P]
     lib.mfgpu_symbolic_destroy.restype = None
     lib.mfgpu_symbolic_error.argtypes = []
