@@ -168,11 +168,14 @@ class _MFBase:
         hh = np.ascontiguousarray(h, np.float64)
         lo3 = np.ascontiguousarray(list(lo) + [0] * (3 - len(lo)), np.int32)
         hi3 = np.ascontiguousarray(list(hi) + [1] * (3 - len(hi)), np.int32)
+        # at most every row of the box grown by one cell changes; one call
+        # (the values are updated in place, so a second call would find nothing)
+        cap = 1
+        for d in range(len(lo)):
+            cap *= max(0, int(hi[d]) + 1 - max(int(lo[d]) - 1, 0))
+        cap = max(1, min(cap, self.A.n))
+        out = np.zeros(cap, np.int32)
         cnt = C.c_int()
-        self._check(self._lib.mfgpu_stencil_update_device(
-            self._h, C.c_void_p(coef_ptr), _lib._ptr(hh), _lib._ptr(lo3), _lib._ptr(hi3),
-            C.c_void_p(val_ptr), None, 0, C.byref(cnt)))
-        out = np.zeros(max(1, cnt.value), np.int32)
         self._check(self._lib.mfgpu_stencil_update_device(
             self._h, C.c_void_p(coef_ptr), _lib._ptr(hh), _lib._ptr(lo3), _lib._ptr(hi3),
             C.c_void_p(val_ptr), _lib._ptr(out), len(out), C.byref(cnt)))
