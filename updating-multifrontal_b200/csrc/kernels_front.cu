@@ -30,81 +30,93 @@ std::atomic<long long> g_launches{0};
 
 namespace {
 
-__device__ __forceinline__ double sparse_at(const int* __restrict__ rp, const int* __restrict__ ci,
-                                            const double* __restrict__ va, int r, int c) {
-  // Sparse<Scalar>::operator()(i, j) (src/LinAlg/sparse.cpp:80-92): scan row r.
-  int p = rp[r], e = rp[r + 1];
-  double v = 0.0;
-  for (; p < e; p++)
-    if (ci[p] == c) v = va[p];
-  return v;
-}
+// One warp per 32 x 32 tile of a task, kTaskWarps tiles per CTA.
+constexpr int kTaskWarps = 4;
 
 template <class T>
-__global__ void __launch_bounds__(256) k_tasks(const Task* __restrict__ tasks,
-                                               const int64_t* __restrict__ tstart, int ntasks,
-                                               T* __restrict__ F, T* __restrict__ SA,
-                                               const int* __restrict__ rp,
-                                               const int* __restrict__ ci,
-                                               const double* __restrict__ va,
-                                               const int* __restrict__ dofs,
-                                               const double* __restrict__ scale) {
-  __shared__ T sm[kTaskTile][kTaskTile + 1];
-  __shared__ int s_task;
-  const int64_t tile = (int64_t)blockIdx.x + (int64_t)blockIdx.y * gridDim.x;
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
+__global__ void __launch_bounds__(32 * kTaskWarps) k_tasks(const Task* __restrict__ tasks,
+                                                           const int64_t* __restrict__ tstart,
+                                                           int ntasks, int64_t ntiles,
+                                                           T* __restrict__ F, T* __restrict__ SA,
+                                                           const int* __restrict__ rp,
+                                                           const int* __restrict__ ci,
+                                                           const double* __restrict__ va,
+                                                           const int* __restrict__ dofs,
+                                                           const double* __restrict__ scale) {
+  __shared__ T sm[kTaskWarps][kTaskTile][kTaskTile + 1];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t tile = ((int64_t)blockIdx.x + (int64_t)blockIdx.y * gridDim.x) * kTaskWarps + w;
+  if (tile >= ntiles) return;
+  int t = 0;
+  if (lane == 0) {
     int lo = 0, hi = ntasks - 1;   // last t with tstart[t] <= tile
     while (lo < hi) {
-      int mid = (lo + hi + 1) >> 1;
+      const int mid = (lo + hi + 1) >> 1;
       if (tstart[mid] <= tile) lo = mid;
       else hi = mid - 1;
     }
-    s_task = lo;
+    t = lo;
   }
-  __syncthreads();
-  if (tile >= tstart[ntasks]) return;
-  const Task Tk = tasks[s_task];
-  const int64_t local = tile - tstart[s_task];
+  t = __shfl_sync(0xffffffffu, t, 0);
+  const Task Tk = tasks[t];
+  const int64_t local = tile - tstart[t];
   const int tr = (Tk.rows + kTaskTile - 1) / kTaskTile;
   const int i0 = (int)(local % tr) * kTaskTile;
   const int j0 = (int)(local / tr) * kTaskTile;
   if (Tk.lower && i0 + kTaskTile - 1 < j0) return;
   T* dst = (Tk.dst_arena == AR_FRONT ? F : SA) + Tk.dst_off;
   const T* src = (Tk.src_arena == AR_FRONT ? F : SA) + Tk.src_off;
-  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int rows = min(kTaskTile, Tk.rows - i0), cols = min(kTaskTile, Tk.cols - j0);
+  T(*tb)[kTaskTile + 1] = sm[w];
+  const int i = i0 + lane;   // this lane's row of the tile in the column-major writes
   if (Tk.kind == TK_COPY && Tk.trans) {
-    // dst(i, j) = src[j + i*ld]: stage through shared memory so both sides coalesce
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      int ii = i0 + ty + 8 * q, jj = j0 + tx;
-      if (ii < Tk.rows && jj < Tk.cols) sm[ty + 8 * q][tx] = src[jj + (int64_t)ii * Tk.src_ld];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      int i = i0 + tx, j = j0 + ty + 8 * q;
-      if (i < Tk.rows && j < Tk.cols && (!Tk.lower || i >= j))
-        dst[i + (int64_t)j * Tk.dst_ld] = sm[tx][ty + 8 * q];
-    }
+    // dst(i, j) = src[j + i*ld]: read src rows with lanes along j, write dst
+    // columns with lanes along i, through the warp's shared-memory tile
+    for (int ii = 0; ii < rows; ii++)
+      if (lane < cols) tb[ii][lane] = src[(j0 + lane) + (int64_t)(i0 + ii) * Tk.src_ld];
+    __syncwarp();
+    if (lane < rows)
+      for (int jj = 0; jj < cols; jj++)
+        if (!Tk.lower || i >= j0 + jj) dst[i + (int64_t)(j0 + jj) * Tk.dst_ld] = tb[lane][jj];
     return;
   }
+  if (Tk.kind == TK_SPARSE) {
+    // A(r, c) for the tile (Sparse::operator(), src/LinAlg/sparse.cpp:80-92):
+    // lane j holds column DOF c_j; every row's CSR entries are read once (all
+    // lanes load the same addresses) and matched against the lanes' columns
+    const int cj = lane < cols ? dofs[Tk.col_dof + j0 + lane] : -1;
+    const double sc = (scale && lane < cols) ? scale[cj] : 1.0;
+    // row DOFs, row extents and row scales of the tile, one per lane
+    const int rl = lane < rows ? dofs[Tk.row_dof + i0 + lane] : 0;
+    const int pl0 = lane < rows ? rp[rl] : 0, pl1 = lane < rows ? rp[rl + 1] : 0;
+    const double srl = (scale && lane < rows) ? scale[rl] : 1.0;
+#pragma unroll 4
+    for (int ii = 0; ii < rows; ii++) {
+      const int p0 = __shfl_sync(0xffffffffu, pl0, ii), p1 = __shfl_sync(0xffffffffu, pl1, ii);
+      const double sr = __shfl_sync(0xffffffffu, srl, ii);
+      double v = 0.0;
 #pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const int i = i0 + tx, j = j0 + ty + 8 * q;
-    if (i >= Tk.rows || j >= Tk.cols || (Tk.lower && i < j)) continue;
-    T* d = dst + i + (int64_t)j * Tk.dst_ld;
-    switch (Tk.kind) {
-      case TK_ZERO: *d = T(0); break;
-      case TK_COPY: *d = src[i + (int64_t)j * Tk.src_ld]; break;
-      case TK_ADD: *d = *d + src[i + (int64_t)j * Tk.src_ld]; break;
-      case TK_SPARSE: {
-        const int r = dofs[Tk.row_dof + i], c = dofs[Tk.col_dof + j];
-        double v = sparse_at(rp, ci, va, r, c);
-        if (scale) v = v * scale[r] * scale[c];   // symmetric diagonal scaling
-        *d = (T)v;
-        break;
-      }
+      for (int q = 0; q < 8; q++)   // stencil rows are short: independent loads
+        if (p0 + q < p1 && ci[p0 + q] == cj) v = va[p0 + q];
+      for (int p = p0 + 8; p < p1; p++)
+        if (ci[p] == cj) v = va[p];
+      if (scale) v = v * sr * sc;   // symmetric diagonal scaling
+      tb[ii][lane] = (T)v;
     }
+    __syncwarp();
+    if (lane < rows)
+      for (int jj = 0; jj < cols; jj++)
+        if (!Tk.lower || i >= j0 + jj) dst[i + (int64_t)(j0 + jj) * Tk.dst_ld] = tb[lane][jj];
+    return;
+  }
+  if (lane >= rows) return;
+  for (int jj = 0; jj < cols; jj++) {
+    const int j = j0 + jj;
+    if (Tk.lower && i < j) continue;
+    T* d = dst + i + (int64_t)j * Tk.dst_ld;
+    if (Tk.kind == TK_ZERO) *d = T(0);
+    else if (Tk.kind == TK_COPY) *d = src[i + (int64_t)j * Tk.src_ld];
+    else *d = *d + src[i + (int64_t)j * Tk.src_ld];   // TK_ADD
   }
 }
 
@@ -1128,10 +1140,11 @@ void launch_tasks(const Task* tasks, const int64_t* tstart, int ntasks, int64_t 
                   T* seps, const int* rp, const int* ci, const double* va, const int* dofs,
                   const double* scale, cudaStream_t st) {
   if (ntasks <= 0 || ntiles <= 0) return;
-  const int64_t gx = ntiles < 65535 * 32 ? ntiles : 65535 * 32;
-  const int64_t gy = (ntiles + gx - 1) / gx;
-  k_tasks<T><<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(tasks, tstart, ntasks, fronts,
-                                                                         seps, rp, ci, va, dofs, scale);
+  const int64_t blocks = (ntiles + kTaskWarps - 1) / kTaskWarps;
+  const int64_t gx = blocks < 65535 * 32 ? blocks : 65535 * 32;
+  const int64_t gy = (blocks + gx - 1) / gx;
+  k_tasks<T><<<dim3((unsigned)gx, (unsigned)gy), 32 * kTaskWarps, 0, st>>>(
+      tasks, tstart, ntasks, ntiles, fronts, seps, rp, ci, va, dofs, scale);
   g_launches++;
 }
 
@@ -1273,6 +1286,7 @@ void launch_solve_fwd(const int* flist, int nf, int maxN, const FrontDev* fr, co
   } while (0)
   if (nrhs == 1) MFGPU_FWD(1);
   else if (nrhs <= 4) MFGPU_FWD(4);
+  else if (nrhs <= 8) MFGPU_FWD(8);
   else MFGPU_FWD(16);
 #undef MFGPU_FWD
   g_launches++;
@@ -1294,6 +1308,7 @@ void launch_solve_bwd(const int* flist, int nf, int maxN, const FrontDev* fr, co
   } while (0)
   if (nrhs == 1) MFGPU_BWD(1);
   else if (nrhs <= 4) MFGPU_BWD(4);
+  else if (nrhs <= 8) MFGPU_BWD(8);
   else MFGPU_BWD(16);
 #undef MFGPU_BWD
   g_launches++;
@@ -1313,6 +1328,7 @@ void launch_root_solve(int f, int N, const FrontDev* fr, const T* F, const int* 
   } while (0)
   if (nrhs == 1) MFGPU_ROOT(1);
   else if (nrhs <= 4) MFGPU_ROOT(4);
+  else if (nrhs <= 8) MFGPU_ROOT(8);
   else MFGPU_ROOT(16);
 #undef MFGPU_ROOT
   g_launches++;

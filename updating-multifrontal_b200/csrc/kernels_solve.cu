@@ -490,6 +490,8 @@ cudaError_t launch_solve_coop(bool forward, const int* flist, int nf, int maxn, 
     return launchCoopSolve<T, 1>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, st);
   if (nrhs <= 4)
     return launchCoopSolve<T, 4>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, st);
+  if (nrhs <= 8)
+    return launchCoopSolve<T, 8>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, st);
   return launchCoopSolve<T, 16>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, st);
 }
 
