@@ -28,11 +28,44 @@ static_assert(sizeof(SepDev) == 32, "SepDev layout");
 
 // Error word written by kernels: first failing front, column and code.
 struct DevError {
-  int code;     // 0 ok, 1 non-positive pivot
+  int code;     // 0 ok, 1 non-positive pivot, 2 tensor-core wait, 3 grid barrier timed out
   int front;
   int col;
   int pad;
 };
+
+// Grid-wide barrier of the cooperative kernels, with a bounded wait.  `count`
+// (one unsigned per launch, zeroed before the launch on the launch's stream)
+// counts arrivals; `target` is private to each thread and advances by the grid
+// size at every barrier.  A wait that gives up records error code 3 in the
+// error word; every later barrier of any CTA then passes at once, so the
+// launch always ends.  The fences follow the usual grid-barrier pattern: the
+// CTA's writes are ordered before thread 0's arrival, and thread 0's
+// observation of the last arrival before the CTA's later reads.
+constexpr unsigned kBarrierSpin = 1u << 25;
+__device__ __forceinline__ void grid_barrier(unsigned* count, unsigned& target, DevError* err) {
+  __syncthreads();
+  target += gridDim.x;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    __threadfence();
+    atomicAdd(count, 1u);
+    volatile unsigned* c = count;
+    volatile int* code = err ? &err->code : nullptr;
+    unsigned it = 0;
+    while (*c < target) {
+      if ((++it & 1023u) == 0) {
+        if (code && *code == 3) break;              // another CTA gave up
+        if (it > kBarrierSpin) {
+          if (err) atomicCAS(&err->code, 0, 3);
+          break;
+        }
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
 
 constexpr int kTaskTile = 32;   // assembly tile edge
 constexpr int kPanel = 32;      // panel width of the partial Cholesky
@@ -70,10 +103,12 @@ size_t coop_slot_elems();
 std::vector<int> coop_phase_prefix(const std::vector<int>& n, const std::vector<int>& N, int maxn);
 // K0/K1/phase0/trailing restrict the launch to the outer panels [K0, K1)
 // (K1 < 0: to the end) and optionally leave the last trailing update out.
+// gbar: one unsigned of device memory for the launch's grid barrier.
 template <class T>
 cudaError_t launch_level_coop(const int* flist, int nf, int maxn, const FrontDev* fr, T* F,
-                              DevError* err, T* slots, const int* phase_pref, cudaStream_t st,
-                              int K0 = 0, int K1 = -1, int phase0 = 0, int trailing = 1);
+                              DevError* err, T* slots, const int* phase_pref, unsigned* gbar,
+                              cudaStream_t st, int K0 = 0, int K1 = -1, int phase0 = 0,
+                              int trailing = 1);
 int coop_outer();                   // outer panel width of the cooperative kernel
 int coop_phases(int K, int maxn);   // phases of outer panel K in the prefix table
 
@@ -93,7 +128,7 @@ int solve_coop_max_fronts();
 template <class T>
 cudaError_t launch_solve_coop(bool forward, const int* flist, int nf, int maxn, const FrontDev* fr,
                               const T* F, const int* dofs, T* X, int64_t ldx, int nrhs, T* W,
-                              const int64_t* woff, cudaStream_t st);
+                              const int64_t* woff, unsigned* gbar, DevError* err, cudaStream_t st);
 
 // Stencil assembly (width 1): recompute the CSR values of the rows of the
 // cells in [lo, hi) from the node coefficients; with `flag`, record which rows

@@ -670,8 +670,9 @@ __global__ void __launch_bounds__(kCT) k_level_coop(const int* __restrict__ flis
                                                     T* __restrict__ F, DevError* err, int maxn,
                                                     T* __restrict__ slots,
                                                     const int* __restrict__ phase_pref, int K0,
-                                                    int K1, int phase0, int trailing) {
-  cg::grid_group grid = cg::this_grid();
+                                                    int K1, int phase0, int trailing,
+                                                    unsigned* gbar) {
+  unsigned gtarget = 0;
   __shared__ T Ls[kPanel][kPanel + 1];
   __shared__ T Li[kPanel * kLi];
   __shared__ T Dinv[kPanel];
@@ -705,7 +706,7 @@ __global__ void __launch_bounds__(kCT) k_level_coop(const int* __restrict__ flis
       coop_factor_publish(F + d.off, d.ld, K0, min(kPanel, d.n - K0), slots + (int64_t)i * kDiagSlot,
                           Ls, Li, Dinv, err, f);
   }
-  grid.sync();
+  grid_barrier(gbar, gtarget, err);
   for (int K = K0; K < K1 && K < maxn; K += kOuter) {
     for (int k = K; k < K + kOuter && k < maxn; k += kPanel) {
       // ---- phase A: rows below the (already factored) diagonal block ----
@@ -727,7 +728,7 @@ __global__ void __launch_bounds__(kCT) k_level_coop(const int* __restrict__ flis
         __syncthreads();
         warp_trsm_block(Rows, (tid >> 5) * 32, (const T*)Li, kb, A, d.ld, rbase, k, Mi, tid & 31);
       }
-      grid.sync();
+      grid_barrier(gbar, gtarget, err);
       // ---- phase B: update the outer panel's remaining columns; the CTA that
       // updates the next diagonal block factors and publishes it ----
       load_phase();
@@ -751,7 +752,7 @@ __global__ void __launch_bounds__(kCT) k_level_coop(const int* __restrict__ flis
           coop_factor_publish(A, d.ld, c0, min(kPanel, d.n - c0), slots + (int64_t)i * kDiagSlot, Ls,
                               Li, Dinv, err, f);
       }
-      grid.sync();
+      grid_barrier(gbar, gtarget, err);
     }
     // ---- phase C: trailing update with the outer panel ----
     if (!trailing && K + kOuter >= K1) break;
@@ -768,7 +769,7 @@ __global__ void __launch_bounds__(kCT) k_level_coop(const int* __restrict__ flis
         coop_factor_publish(F + d.off, d.ld, k1, min(kPanel, d.n - k1), slots + (int64_t)i * kDiagSlot,
                             Ls, Li, Dinv, err, f);
     }
-    grid.sync();
+    grid_barrier(gbar, gtarget, err);
   }
 }
 
@@ -1226,9 +1227,11 @@ int coop_phases(int K, int maxn) {
 
 template <class T>
 cudaError_t launch_level_coop(const int* flist, int nf, int maxn, const FrontDev* fr, T* F,
-                              DevError* err, T* slots, const int* phase_pref, cudaStream_t st,
-                              int K0, int K1, int phase0, int trailing) {
+                              DevError* err, T* slots, const int* phase_pref, unsigned* gbar,
+                              cudaStream_t st, int K0, int K1, int phase0, int trailing) {
   if (nf <= 0) return cudaSuccess;
+  cudaError_t me = cudaMemsetAsync(gbar, 0, sizeof(unsigned), st);
+  if (me != cudaSuccess) return me;
   if (K1 < 0) K1 = maxn;
   const size_t sm = 2 * 64 * kPS * sizeof(T) + (size_t)(kMaxCoopFronts + 1) * sizeof(int);
   static int grid = 0;   // co-resident CTAs of this instantiation on this device
@@ -1242,7 +1245,8 @@ cudaError_t launch_level_coop(const int* flist, int nf, int maxn, const FrontDev
   }
   void* args[] = {(void*)&flist, (void*)&nf,    (void*)&fr,         (void*)&F,
                   (void*)&err,   (void*)&maxn,  (void*)&slots,      (void*)&phase_pref,
-                  (void*)&K0,    (void*)&K1,    (void*)&phase0,     (void*)&trailing};
+                  (void*)&K0,    (void*)&K1,    (void*)&phase0,     (void*)&trailing,
+                  (void*)&gbar};
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_level_coop<T>, dim3(grid), dim3(kCT),
                                               args, sm, st);
   g_launches++;
@@ -1368,7 +1372,8 @@ void launch_sep_gather(const int* slist, int ns, const SepDev* sp, const int* do
   template void launch_tasks<T>(const Task*, const int64_t*, int, int64_t, T*, T*, const int*,     \
                                 const int*, const double*, const int*, const double*, cudaStream_t); \
   template cudaError_t launch_level_coop<T>(const int*, int, int, const FrontDev*, T*, DevError*,  \
-                                            T*, const int*, cudaStream_t, int, int, int, int);      \
+                                            T*, const int*, unsigned*, cudaStream_t, int, int, int, \
+                                            int);                                                   \
   template void launch_front_small<T>(const int*, int, int, const FrontDev*, T*, DevError*,        \
                                       cudaStream_t);                                                \
   template void launch_solve_fwd<T>(const int*, int, int, const FrontDev*, const T*, const int*,   \

@@ -193,8 +193,8 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_fwd(const int* __restrict__ 
                                                         const int* __restrict__ dofs, T* X,
                                                         int64_t ldx, int nrhs, T* Wb,
                                                         const int64_t* __restrict__ woff,
-                                                        int maxnb) {
-  cg::grid_group grid = cg::this_grid();
+                                                        int maxnb, unsigned* gbar, DevError* err) {
+  unsigned gtarget = 0;
   __shared__ int pre[kMaxSolveCoopFronts + 1];
   __shared__ int wt[SCT / 32];
   __shared__ T ys[SB][NR + 1];
@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_fwd(const int* __restrict__ 
       W[idx] = r < d.n ? X[dl[r] + (int64_t)c * ldx] : T(0);
     }
   }
-  grid.sync();
+  grid_barrier(gbar, gtarget, err);
   for (int i = blockIdx.x; i < nf; i += gridDim.x) {
     const int f = flist[i];
     const FrontDev d = fr[f];
@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_fwd(const int* __restrict__ 
       diag_lower_solve<T, NR>(F + d.off, d.ld, Wb + woff[f] * nrhs, d.N, 0, min(SB, d.n), nrhs, Ls,
                               xs);
   }
-  grid.sync();
+  grid_barrier(gbar, gtarget, err);
   for (int j = 0; j < maxnb; j++) {
     int cnt = 0;
     if (tid < nf) {
@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_fwd(const int* __restrict__ 
         diag_lower_solve<T, NR>(A, d.ld, W, d.N, k + kb, min(SB, d.n - k - kb), nrhs, Ls, xs);
       }
     }
-    grid.sync();
+    grid_barrier(gbar, gtarget, err);
   }
   // pivots back to X; the boundary part stays in W for the separator gather
   for (int i = 0; i < nf; i++) {
@@ -304,8 +304,8 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_bwd(const int* __restrict__ 
                                                         const int* __restrict__ dofs, T* X,
                                                         int64_t ldx, int nrhs, T* Wb,
                                                         const int64_t* __restrict__ woff,
-                                                        int maxnb) {
-  cg::grid_group grid = cg::this_grid();
+                                                        int maxnb, unsigned* gbar, DevError* err) {
+  unsigned gtarget = 0;
   __shared__ int pre[kMaxSolveCoopFronts + 1];
   __shared__ int wt[SCT / 32];
   __shared__ T xj[SB][NR + 1];
@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_bwd(const int* __restrict__ 
       W[idx] = X[dl[r] + (int64_t)c * ldx];
     }
   }
-  grid.sync();
+  grid_barrier(gbar, gtarget, err);
   // r = y - L21^T x_bd, one column block per item; the CTA with the last
   // block then solves it
   {
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_bwd(const int* __restrict__ 
         diag_upper_solve<T, NR>(A, d.ld, W, d.N, k, kb, nrhs, Ls, xs);
       }
     }
-    grid.sync();
+    grid_barrier(gbar, gtarget, err);
   }
   // step t: front i works on its block j = nb_i - 1 - t
   for (int t = 0; t < maxnb - 1; t++) {
@@ -430,7 +430,7 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_bwd(const int* __restrict__ 
         diag_upper_solve<T, NR>(A, d.ld, W, d.N, k, SB, nrhs, Ls, xs);
       }
     }
-    grid.sync();
+    grid_barrier(gbar, gtarget, err);
   }
   for (int i = 0; i < nf; i++) {
     const int f = flist[i];
@@ -458,7 +458,9 @@ int coopGrid(K kern) {
 template <class T, int NR>
 cudaError_t launchCoopSolve(bool fwd, const int* flist, int nf, int maxn, const FrontDev* fr,
                             const T* F, const int* dofs, T* X, int64_t ldx, int nrhs, T* W,
-                            const int64_t* woff, cudaStream_t st) {
+                            const int64_t* woff, unsigned* gbar, DevError* err, cudaStream_t st) {
+  cudaError_t me = cudaMemsetAsync(gbar, 0, sizeof(unsigned), st);
+  if (me != cudaSuccess) return me;
   static int gf = 0, gb = 0;
   if (gf == 0) {
     gf = coopGrid(k_solve_coop_fwd<T, NR>);
@@ -467,7 +469,7 @@ cudaError_t launchCoopSolve(bool fwd, const int* flist, int nf, int maxn, const 
   int maxnb = cdiv(maxn, SB);
   void* args[] = {(void*)&flist, (void*)&nf,   (void*)&fr,   (void*)&F,
                   (void*)&dofs,  (void*)&X,    (void*)&ldx,  (void*)&nrhs,
-                  (void*)&W,     (void*)&woff, (void*)&maxnb};
+                  (void*)&W,     (void*)&woff, (void*)&maxnb, (void*)&gbar, (void*)&err};
   g_launches++;
   if (fwd)
     return cudaLaunchCooperativeKernel((const void*)k_solve_coop_fwd<T, NR>, dim3(gf), dim3(SCT),
@@ -483,23 +485,24 @@ int solve_coop_max_fronts() { return kMaxSolveCoopFronts; }
 template <class T>
 cudaError_t launch_solve_coop(bool forward, const int* flist, int nf, int maxn, const FrontDev* fr,
                               const T* F, const int* dofs, T* X, int64_t ldx, int nrhs, T* W,
-                              const int64_t* woff, cudaStream_t st) {
+                              const int64_t* woff, unsigned* gbar, DevError* err, cudaStream_t st) {
   if (nf <= 0) return cudaSuccess;
   if (nf > kMaxSolveCoopFronts || nrhs > 16) return cudaErrorInvalidValue;
   if (nrhs == 1)
-    return launchCoopSolve<T, 1>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, st);
+    return launchCoopSolve<T, 1>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, gbar, err, st);
   if (nrhs <= 4)
-    return launchCoopSolve<T, 4>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, st);
+    return launchCoopSolve<T, 4>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, gbar, err, st);
   if (nrhs <= 8)
-    return launchCoopSolve<T, 8>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, st);
-  return launchCoopSolve<T, 16>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, st);
+    return launchCoopSolve<T, 8>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, gbar, err, st);
+  return launchCoopSolve<T, 16>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, gbar, err, st);
 }
 
 template cudaError_t launch_solve_coop<double>(bool, const int*, int, int, const FrontDev*,
                                                const double*, const int*, double*, int64_t, int,
-                                               double*, const int64_t*, cudaStream_t);
+                                               double*, const int64_t*, unsigned*, DevError*,
+                                               cudaStream_t);
 template cudaError_t launch_solve_coop<float>(bool, const int*, int, int, const FrontDev*,
                                               const float*, const int*, float*, int64_t, int, float*,
-                                              const int64_t*, cudaStream_t);
+                                              const int64_t*, unsigned*, DevError*, cudaStream_t);
 
 }  // namespace mfgpu

@@ -236,6 +236,7 @@ struct mfgpu_handle {
   int64_t* d_woff = nullptr;
   DevError* d_err = nullptr;
   void* d_slots = nullptr;     // diagonal-block hand-off slots of the cooperative kernel
+  unsigned* d_gbar = nullptr;  // grid-barrier arrival counter of the cooperative kernels
   // solve workspaces (d_Wd / d_Td hold elements of the factor's precision)
   double* d_Wd = nullptr;
   size_t capW = 0;
@@ -295,6 +296,7 @@ struct mfgpu_handle {
     cudaFree(d_woff);
     cudaFree(d_err);
     cudaFree(d_slots);
+    cudaFree(d_gbar);
     cudaFree(d_Wd);
     cudaFree(d_X);
     cudaFree(d_Td);
@@ -429,7 +431,7 @@ struct mfgpu_handle {
           prof.flops[MFGPU_KC_COOP] += fl;
           prof.begin(MFGPU_KC_COOP, stream);
           ck(mfgpu::launch_level_coop<T>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, F, d_err,
-                                         (T*)d_slots, P.d_cpref + L.cpref0, stream),
+                                         (T*)d_slots, P.d_cpref + L.cpref0, d_gbar, stream),
              "launch cooperative level factorization (k_level_coop)");
           prof.end(stream);
         }
@@ -475,8 +477,8 @@ struct mfgpu_handle {
     for (int K = 0; K < L.maxn; K += outer) {
       prof.begin(MFGPU_KC_COOP, stream);
       ck(mfgpu::launch_level_coop<float>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, (float*)d_F,
-                                         d_err, (float*)d_slots, P.d_cpref + L.cpref0, stream, K,
-                                         K + outer, phase0, 0),
+                                         d_err, (float*)d_slots, P.d_cpref + L.cpref0, d_gbar,
+                                         stream, K, K + outer, phase0, 0),
          "launch cooperative panel factorization (k_level_coop)");
       prof.end(stream);
       phase0 += mfgpu::coop_phases(K, L.maxn);
@@ -553,6 +555,11 @@ struct mfgpu_handle {
     DevError e;
     ck(cudaMemcpyAsync(&e, d_err, sizeof(e), cudaMemcpyDeviceToHost, stream), "read error word");
     ck(cudaStreamSynchronize(stream), "factor");
+    if (e.code == 2 || e.code == 3) {
+      throw CudaError(e.code == 2 ? "a tensor-core pipeline wait gave up (k_trail_tc)"
+                                  : "a cooperative kernel's grid barrier gave up",
+                      MFGPU_ERR_TIMEOUT);
+    }
     if (e.code == 1) {
       const mfgpu::Front& f = S->fronts[e.front];
       char buf[256];
@@ -617,7 +624,7 @@ struct mfgpu_handle {
     const int nf = s.lv[ell].nbox;
     if (coopSweep(ell)) {
       ck(mfgpu::launch_solve_coop<T>(forward, fl, nf, lvMaxn[ell], d_fr, F, d_dofs, X, ldx, nrhs, W,
-                                     d_woff, stream),
+                                     d_woff, d_gbar, d_err, stream),
          forward ? "launch cooperative forward sweep (k_solve_coop_fwd)"
                  : "launch cooperative backward sweep (k_solve_coop_bwd)");
     } else if (forward) {
@@ -1044,6 +1051,7 @@ int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const
     H.d_woff = dalloc<int64_t>(woff.size(), "alloc woff");
     H.d_err = dalloc<DevError>(1, "alloc error word");
     H.d_slots = dalloc<unsigned char>(mfgpu::coop_slot_elems() * H.esz, "alloc diagonal slots");
+    H.d_gbar = dalloc<unsigned>(1, "alloc grid barrier");
     H.d_all = dalloc<int>(all.size(), "alloc id list");
     ck(cudaMemcpy(H.d_val, val, H.nnz * sizeof(double), cudaMemcpyHostToDevice), "upload val");
     ck(cudaMemcpy(H.d_rp, row_ptr, (n + 1) * sizeof(int), cudaMemcpyHostToDevice), "upload rows");
@@ -1173,6 +1181,7 @@ static int solveOrApply(mfgpu_handle* h, const double* in, double* out, int nrhs
     const int chunk = 16;
     h->stats.iterations = 0;
     h->stats.residual = 0;
+    ck(cudaMemsetAsync(h->d_err, 0, sizeof(DevError), h->stream), "clear error word");
     ck(cudaEventRecord(h->ev0, h->stream), "event");
     for (int c0 = 0; c0 < nrhs; c0 += chunk) {
       const int nc = std::min(chunk, nrhs - c0);
@@ -1207,6 +1216,7 @@ static int solveOrApply(mfgpu_handle* h, const double* in, double* out, int nrhs
     }
     ck(cudaEventRecord(h->ev1, h->stream), "event");
     ck(cudaEventSynchronize(h->ev1), "solve");
+    h->checkDevError();
     h->prof.collect();
     float ms = 0;
     ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "elapsed");
