@@ -26,6 +26,7 @@ extern "C" {
 
 typedef struct mfgpu_handle mfgpu_handle;
 typedef struct mfgpu_symbolic mfgpu_symbolic;
+typedef struct mfgpu_server mfgpu_server;
 
 enum mfgpu_status {
   MFGPU_OK = 0,
@@ -97,6 +98,41 @@ int mfgpu_stencil_assemble_device(mfgpu_handle* h, const double* d_coef, const d
 int mfgpu_stencil_update_device(mfgpu_handle* h, const double* d_coef, const double* hxyz,
                                 const int* box_lo, const int* box_hi, double* d_val,
                                 int* modified_dofs, int capacity, int* n_modified);
+
+/* ---- Update-serving loop (no reference counterpart) ----
+ * A factored handle stays resident; each request multiplies the coefficients
+ * of one box of cells [box_lo, box_hi) by `factor` and solves the changed
+ * system for its right-hand sides.  Requests are independent of each other
+ * (each answer is that of the base matrix under its own change), refactor only
+ * the root paths of the leaves their box touches (the reference's Update,
+ * src/DE/mf2d.cpp:150-181) into private copies held in a device pool of
+ * pool_bytes, and run concurrently in `slots` slots, each a worker thread with
+ * its own stream.  A request is admitted when a slot is free and the pool has
+ * room for its private fronts; until then it waits, in arrival order.
+ * d_coef: the base coefficients on the device ((nx+2) x (ny+2) [x (nz+2)],
+ * C order, x slowest), copied by the server; hxyz: grid spacings (null = 1). */
+typedef struct mfgpu_request_info {
+  int status;               /* mfgpu_status of the request                       */
+  int fronts;               /* fronts refactored for it                          */
+  int iterations;           /* refinement iterations (mixed)                     */
+  int pad;
+  double queued_seconds;    /* submit -> start of its device work                */
+  double latency_seconds;   /* submit -> result written                          */
+  double residual;          /* relative residual reached (mixed)                 */
+  int64_t pool_bytes;       /* private memory it held                            */
+  int64_t reserved[4];
+} mfgpu_request_info;
+
+int mfgpu_server_create(mfgpu_handle* base, const double* d_coef, const double* hxyz, int slots,
+                        int64_t pool_bytes, mfgpu_server** out);
+/* Queue a request (host b, nrhs columns of leading dimension ld >= n); the
+ * answer is written to host x (same ld) before mfgpu_server_wait returns. */
+int mfgpu_server_submit(mfgpu_server* srv, const int* box_lo, const int* box_hi, double factor,
+                        const double* b, int nrhs, int64_t ld, double* x, int64_t* ticket);
+/* Block until the request is done; returns its status (each ticket once). */
+int mfgpu_server_wait(mfgpu_server* srv, int64_t ticket, mfgpu_request_info* info);
+const char* mfgpu_server_last_error(const mfgpu_server* srv);
+void mfgpu_server_destroy(mfgpu_server* srv);
 
 /* Batch of independent problems in one handle (no reference counterpart; the
  * reference factors one problem per MF2D/MF3D object).  Problem p has the

@@ -138,6 +138,9 @@ cudaError_t launch_stencil_rows(int dim, int nx, int ny, int nz, const double h[
                                 int* flag, cudaStream_t st);
 cudaError_t launch_collect_rows(int dim, int nx, int ny, const int lo[3], const int hi[3],
                                 const int* flag, int* out, int cap, int* count, cudaStream_t st);
+// Node coefficients of the cells [lo, hi) multiplied by factor (in place).
+cudaError_t launch_scale_box(int dim, int ny, int nz, const int lo[3], const int hi[3], double factor,
+                             double* a, cudaStream_t st);
 
 // Number of kernels this library has launched since it was loaded.
 long long launches_total();

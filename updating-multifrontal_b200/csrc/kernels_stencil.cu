@@ -107,7 +107,30 @@ __global__ void k_collect(const int* __restrict__ flag, int lo0, int lo1, int lo
   }
 }
 
+// Coefficients of the cells [lo, hi) multiplied by `factor` (node = cell + 1).
+__global__ void k_scale_box(double* __restrict__ a, int dim, int ny, int nz, int lo0, int lo1,
+                            int lo2, int bx, int by, int bz, double factor) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)bx * by * bz) return;
+  const int i = lo0 + (int)(t % bx) + 1, j = lo1 + (int)((t / bx) % by) + 1;
+  const int k = lo2 + (int)(t / ((int64_t)bx * by)) + 1;
+  const int64_t idx = dim == 2 ? (int64_t)i * (ny + 2) + j : ((int64_t)i * (ny + 2) + j) * (nz + 2) + k;
+  a[idx] = __dmul_rn(a[idx], factor);
+}
+
 }  // namespace
+
+cudaError_t launch_scale_box(int dim, int ny, int nz, const int lo[3], const int hi[3], double factor,
+                             double* a, cudaStream_t st) {
+  const int bx = hi[0] - lo[0], by = hi[1] - lo[1], bz = dim == 3 ? hi[2] - lo[2] : 1;
+  if (bx <= 0 || by <= 0 || bz <= 0) return cudaSuccess;
+  const int64_t cells = (int64_t)bx * by * bz;
+  k_scale_box<<<(unsigned)((cells + 255) / 256), 256, 0, st>>>(a, dim, ny, nz, lo[0], lo[1],
+                                                              dim == 3 ? lo[2] : 0, bx, by, bz,
+                                                              factor);
+  g_launches++;
+  return cudaGetLastError();
+}
 
 cudaError_t launch_stencil_rows(int dim, int nx, int ny, int nz, const double h[3], const double* a,
                                 const int* rp, double* val, const int lo[3], const int hi[3],

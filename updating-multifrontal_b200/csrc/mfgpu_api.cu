@@ -8,6 +8,11 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <chrono>
+#include <map>
+#include <deque>
+#include <condition_variable>
+#include <thread>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -214,7 +219,7 @@ struct Profiler {
 }  // namespace
 
 struct mfgpu_handle {
-  std::unique_ptr<Schedule> S;
+  std::shared_ptr<Schedule> S;   // shared with the serving loop's views
   mfgpu_options opt{};
   int device = 0;
   cudaStream_t own = nullptr, stream = nullptr;
@@ -280,28 +285,38 @@ struct mfgpu_handle {
   std::vector<int> lvMaxn;   // largest pivot count per level
   int solveCoopMinN = 1024;  // levels with a front this large use the cooperative sweeps
   bool stepped = false;      // MFGPU_STEPPED=1: per-step launches instead of the cooperative kernel
+  // A view (the serving loop's per-slot handle) shares the base handle's
+  // schedule, arenas, matrix pattern and tables and owns only its stream, its
+  // front table, values, error word, scratch and workspaces.
+  bool view = false;
 
   ~mfgpu_handle() {
     if (stream) cudaStreamSynchronize(stream);
     full.release();
     upd.release();
-    cudaFree(d_F);
-    cudaFree(d_Sep);
+    if (!view) {
+      cudaFree(d_F);
+      cudaFree(d_Sep);
+      cudaFree(d_rp);
+      cudaFree(d_ci);
+      cudaFree(d_dofs);
+      cudaFree(d_sp);
+      cudaFree(d_woff);
+      cudaFree(d_scale);
+      cudaFree(d_iscale);
+      cudaFree(d_segrow);
+      cudaFree(d_chunkrow);
+      cudaFree(d_segchunk);
+      cudaFree(d_all);
+    }
     cudaFree(d_val);
-    cudaFree(d_rp);
-    cudaFree(d_ci);
-    cudaFree(d_dofs);
     cudaFree(d_fr);
-    cudaFree(d_sp);
-    cudaFree(d_woff);
     cudaFree(d_err);
     cudaFree(d_slots);
     cudaFree(d_gbar);
     cudaFree(d_Wd);
     cudaFree(d_X);
     cudaFree(d_Td);
-    cudaFree(d_scale);
-    cudaFree(d_iscale);
     cudaFree(d_B);
     cudaFree(d_R);
     cudaFree(d_P);
@@ -311,12 +326,8 @@ struct mfgpu_handle {
     cudaFree(d_dotp);
     cudaFree(d_sc);
     cudaFree(d_active);
-    cudaFree(d_segrow);
-    cudaFree(d_chunkrow);
-    cudaFree(d_segchunk);
     cudaFree(d_flag);
     cudaFree(d_modbuf);
-    cudaFree(d_all);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (own) cudaStreamDestroy(own);
@@ -1554,5 +1565,441 @@ int mfgpu_symbolic_layout(const mfgpu_symbolic* s, int front_or_sep, int id, int
   }
   return MFGPU_OK;
 }
+
+}  // extern "C"
+
+// ===========================================================================
+// Update-serving loop.
+//
+// A base factorization stays resident.  Each request changes the coefficients
+// of one box of cells by a factor and brings right-hand sides; its answer is
+// x = A_r^{-1} b with A_r the base matrix under that change alone, so requests
+// are independent and their results do not depend on what else is in flight.
+// A request refactors only the root paths of the leaves its box touches
+// (src/DE/mf2d.cpp:150-181) into private copies of those fronts and
+// separators, carved out of a device pool; every other front is read from the
+// base factorization.  One worker thread per slot owns a view of the base
+// handle (its own stream, front table, matrix values and workspaces), so
+// admitted requests run concurrently on the device.  A request is admitted when
+// a slot is free and the pool holds its footprint (the bytes of its private
+// fronts and separators); requests wait in arrival order otherwise.
+// ===========================================================================
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  int64_t id = 0;
+  int lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+  double factor = 1.0;
+  std::vector<double> b;     // n x nrhs, column-major
+  int nrhs = 0;
+  double* x = nullptr;       // caller's output, n x nrhs, leading dimension ldx
+  int64_t ldx = 0;
+  Clock::time_point t_submit, t_start, t_done;
+  int status = MFGPU_OK;
+  std::string error;
+  mfgpu_stats stats{};
+  int64_t footprint = 0;     // pool elements
+  int nfronts = 0;
+  bool done = false;
+};
+
+// First-fit allocator over the pool (offsets and sizes in elements).
+struct PoolAlloc {
+  std::map<int64_t, int64_t> free_;   // offset -> size
+  explicit PoolAlloc(int64_t size) { free_[0] = size; }
+  int64_t take(int64_t size) {
+    for (auto it = free_.begin(); it != free_.end(); ++it)
+      if (it->second >= size) {
+        const int64_t off = it->first, rest = it->second - size;
+        free_.erase(it);
+        if (rest > 0) free_[off + size] = rest;
+        return off;
+      }
+    return -1;
+  }
+  void give(int64_t off, int64_t size) {
+    auto it = free_.emplace(off, size).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+};
+
+inline int64_t round32(int64_t v) { return (v + 31) / 32 * 32; }
+
+}  // namespace
+
+struct mfgpu_server {
+  mfgpu_handle* base = nullptr;
+  double h[3] = {1.0, 1.0, 1.0};
+  double* d_coef = nullptr;            // base coefficients
+  int64_t coef_elems = 0;
+  unsigned char* d_pool = nullptr;     // private fronts and separators
+  int64_t pool_elems = 0;
+  std::vector<std::unique_ptr<mfgpu_handle>> views;
+  std::vector<double*> slot_coef;
+  std::vector<std::thread> workers;
+  std::mutex mu;
+  std::condition_variable cv_queue, cv_pool, cv_done;
+  std::deque<std::shared_ptr<Request>> queue;
+  std::map<int64_t, std::shared_ptr<Request>> all;
+  std::unique_ptr<PoolAlloc> pool;
+  int64_t next_id = 1;
+  bool stop = false;
+  std::vector<FrontDev> base_table;
+  std::string err;
+
+  ~mfgpu_server() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stop = true;
+    }
+    cv_queue.notify_all();
+    cv_pool.notify_all();
+    for (auto& t : workers)
+      if (t.joinable()) t.join();
+    views.clear();
+    for (double* c : slot_coef) cudaFree(c);
+    cudaFree(d_coef);
+    cudaFree(d_pool);
+  }
+
+  // Private footprint of a request: the fronts refactored and the separators
+  // rebuilt for its box (the box grown by one cell: every row whose stencil
+  // reads a changed node).
+  void dirtyOf(const Request& r, std::vector<char>& dirty, std::vector<char>& dsep,
+               int64_t& elems) {
+    const Schedule& s = *base->S;
+    std::vector<int> mod;
+    int lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+    for (int a = 0; a < s.dim; a++) {
+      lo[a] = std::max(0, r.lo[a] - 1);
+      hi[a] = std::min(s.N[a], r.hi[a] + 1);
+    }
+    for (int k = lo[2]; k < hi[2]; k++)
+      for (int j = lo[1]; j < hi[1]; j++)
+        for (int i = lo[0]; i < hi[0]; i++)
+          mod.push_back(i + j * s.N[0] + k * s.N[0] * s.N[1]);
+    s.dirty_fronts(mod.data(), (int)mod.size(), dirty);
+    dsep.assign(s.seps.size(), 0);
+    elems = 0;
+    for (size_t f = 0; f < s.fronts.size(); f++)
+      if (dirty[f]) elems += round32((int64_t)s.fronts[f].ld * s.fronts[f].N);
+    for (size_t k = 0; k < s.seps.size(); k++)
+      if (dirty[s.seps[k].box[0]] || dirty[s.seps[k].box[1]]) {
+        dsep[k] = 1;
+        elems += round32((int64_t)s.seps[k].ld * s.seps[k].s);
+      }
+  }
+
+  void run(int slot) {
+    mfgpu_handle& V = *views[slot];
+    cudaSetDevice(V.device);
+    while (true) {
+      std::shared_ptr<Request> r;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_queue.wait(lk, [&] { return stop || !queue.empty(); });
+        if (stop) return;
+        r = queue.front();
+        queue.pop_front();
+      }
+      std::vector<char> dirty, dsep;
+      int64_t elems = 0;
+      dirtyOf(*r, dirty, dsep, elems);
+      int64_t region = -1;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        if (elems > pool_elems) {
+          r->status = MFGPU_ERR_OOM;
+          r->error = "request needs more private memory than the whole pool";
+        } else {
+          cv_pool.wait(lk, [&] { return stop || (region = pool->take(elems)) >= 0; });
+          if (stop) return;
+        }
+      }
+      if (region >= 0) {
+        r->t_start = Clock::now();
+        r->footprint = elems;
+        serve(V, slot, *r, dirty, dsep, region);
+        std::lock_guard<std::mutex> lk(mu);
+        pool->give(region, elems);
+      }
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        r->t_done = Clock::now();
+        r->done = true;
+      }
+      cv_pool.notify_all();
+      cv_done.notify_all();
+    }
+  }
+
+  void serve(mfgpu_handle& V, int slot, Request& r, const std::vector<char>& dirty,
+             const std::vector<char>& dsep, int64_t region) {
+    const Schedule& s = *V.S;
+    const int st = guarded(&V, [&]() {
+      // the request's coefficients and matrix values
+      ck(cudaMemcpyAsync(slot_coef[slot], d_coef, coef_elems * sizeof(double),
+                         cudaMemcpyDeviceToDevice, V.stream), "copy coefficients");
+      ck(mfgpu::launch_scale_box(s.dim, s.N[1], s.N[2], r.lo, r.hi, r.factor, slot_coef[slot],
+                                 V.stream), "launch coefficient change (k_scale_box)");
+      ck(cudaMemcpyAsync(V.d_val, base->d_val, V.nnz * sizeof(double), cudaMemcpyDeviceToDevice,
+                         V.stream), "copy values");
+      int nmod = 0;
+      const int rc = mfgpu_stencil_update_device(&V, slot_coef[slot], h, r.lo, r.hi, V.d_val,
+                                                 nullptr, 0, &nmod);
+      if (rc != MFGPU_OK) throw CudaError(V.err, rc);
+      // private layout: dirty fronts then dirty separators, from `region` on
+      const int64_t poolF = ((int64_t)(d_pool - (unsigned char*)V.d_F)) / (int64_t)V.esz + region;
+      const int64_t poolS = ((int64_t)(d_pool - (unsigned char*)V.d_Sep)) / (int64_t)V.esz + region;
+      std::vector<int64_t> fnew(s.fronts.size(), -1), snew(s.seps.size(), -1);
+      int64_t cur = 0;
+      for (size_t f = 0; f < s.fronts.size(); f++)
+        if (dirty[f]) {
+          fnew[f] = cur;
+          cur += round32((int64_t)s.fronts[f].ld * s.fronts[f].N);
+        }
+      for (size_t k = 0; k < s.seps.size(); k++)
+        if (dsep[k]) {
+          snew[k] = cur;
+          cur += round32((int64_t)s.seps[k].ld * s.seps[k].s);
+        }
+      // the view's front table: dirty fronts in the private region
+      std::vector<FrontDev> table = base_table;
+      int nd = 0;
+      for (size_t f = 0; f < s.fronts.size(); f++)
+        if (dirty[f]) {
+          table[f].off = poolF + fnew[f];
+          nd++;
+        }
+      ck(cudaMemcpyAsync(V.d_fr, table.data(), table.size() * sizeof(FrontDev),
+                         cudaMemcpyHostToDevice, V.stream), "upload front table");
+      // the update plan with task offsets moved to the private copies
+      V.buildPlan(V.upd, dirty);
+      auto ownerF = [&](int64_t off) {   // front whose storage holds element off
+        int lo = 0, hi = (int)s.fronts.size() - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (s.fronts[mid].off <= off) lo = mid;
+          else hi = mid - 1;
+        }
+        return lo;
+      };
+      auto ownerS = [&](int64_t off) {
+        int lo = 0, hi = (int)s.seps.size() - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (s.seps[mid].off <= off) lo = mid;
+          else hi = mid - 1;
+        }
+        return lo;
+      };
+      auto move = [&](int16_t arena, int64_t off) {
+        if (arena == mfgpu::AR_FRONT) {
+          const int f = ownerF(off);
+          return dirty[f] ? poolF + fnew[f] + (off - s.fronts[f].off) : off;
+        }
+        const int k = ownerS(off);
+        return dsep[k] ? poolS + snew[k] + (off - s.seps[k].off) : off;
+      };
+      for (Task& t : V.upd.tasks) {
+        t.dst_off = move(t.dst_arena, t.dst_off);
+        if (t.kind == mfgpu::TK_COPY || t.kind == mfgpu::TK_ADD)
+          t.src_off = move(t.src_arena, t.src_off);
+      }
+      V.upd.upload(V.stream);
+      // refactor the private root paths, then solve
+      V.factorWith(nullptr, true, V.upd, false);
+      V.checkDevError();
+      r.nfronts = nd;
+    });
+    if (st != MFGPU_OK) {
+      r.status = st;
+      r.error = V.err;
+      return;
+    }
+    V.factored = true;
+    std::vector<double> xs((size_t)V.n * r.nrhs);
+    const int rc = solveOrApply(&V, r.b.data(), xs.data(), r.nrhs, V.n, false, false);
+    r.status = rc;
+    if (rc != MFGPU_OK) {
+      r.error = V.err;
+      return;
+    }
+    for (int c = 0; c < r.nrhs; c++)
+      std::copy(xs.begin() + (int64_t)c * V.n, xs.begin() + (int64_t)(c + 1) * V.n,
+                r.x + (int64_t)c * r.ldx);
+    r.stats = V.stats;
+  }
+};
+
+namespace {
+
+std::unique_ptr<mfgpu_handle> makeView(mfgpu_handle& B) {
+  std::unique_ptr<mfgpu_handle> V(new mfgpu_handle());
+  mfgpu_handle& H = *V;
+  H.view = true;
+  H.S = B.S;
+  H.opt = B.opt;
+  H.device = B.device;
+  H.n = B.n;
+  H.nnz = B.nnz;
+  H.d_F = B.d_F;
+  H.d_Sep = B.d_Sep;
+  H.d_rp = B.d_rp;
+  H.d_ci = B.d_ci;
+  H.d_dofs = B.d_dofs;
+  H.d_sp = B.d_sp;
+  H.d_woff = B.d_woff;
+  H.d_all = B.d_all;
+  H.mixed = B.mixed;
+  H.esz = B.esz;
+  H.tcMinN = B.tcMinN;
+  H.tcSplit = B.tcSplit;
+  H.fusedMinFronts = B.fusedMinFronts;
+  H.d_scale = B.d_scale;
+  H.d_iscale = B.d_iscale;
+  H.nseg = B.nseg;
+  H.nchunks = B.nchunks;
+  H.d_segrow = B.d_segrow;
+  H.d_chunkrow = B.d_chunkrow;
+  H.d_segchunk = B.d_segchunk;
+  H.woffTotal = B.woffTotal;
+  H.lvMaxN = B.lvMaxN;
+  H.lvMaxn = B.lvMaxn;
+  H.solveCoopMinN = B.solveCoopMinN;
+  H.stepped = B.stepped;
+  ck(cudaStreamCreateWithFlags(&H.own, cudaStreamNonBlocking), "create stream");
+  H.stream = H.own;
+  ck(cudaEventCreate(&H.ev0), "event");
+  ck(cudaEventCreate(&H.ev1), "event");
+  H.d_fr = dalloc<FrontDev>(B.S->fronts.size(), "alloc view front table");
+  H.d_val = dalloc<double>(B.nnz, "alloc view values");
+  H.d_err = dalloc<DevError>(1, "alloc error word");
+  H.d_slots = dalloc<unsigned char>(mfgpu::coop_slot_elems() * H.esz, "alloc diagonal slots");
+  H.d_gbar = dalloc<unsigned>(1, "alloc grid barrier");
+  if (H.mixed) {
+    H.d_sc = dalloc<double>(80 * (size_t)H.nseg, "alloc refinement scalars");
+    H.d_active = dalloc<int>(16 * (size_t)H.nseg, "alloc refinement flags");
+  }
+  H.factored = true;
+  return V;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mfgpu_server_create(mfgpu_handle* base, const double* d_coef, const double* hxyz, int slots,
+                        int64_t pool_bytes, mfgpu_server** out) {
+  if (!out || !base || !d_coef || slots <= 0 || pool_bytes <= 0) return MFGPU_ERR_ARG;
+  *out = nullptr;
+  const Schedule& s = *base->S;
+  if (!base->factored) return fail(base, MFGPU_ERR_STATE, "the serving loop needs a factored handle");
+  if (s.forest() || s.width != 1)
+    return fail(base, MFGPU_ERR_ARG, "the serving loop takes one problem of width 1");
+  std::unique_ptr<mfgpu_server> S(new mfgpu_server());
+  S->base = base;
+  if (hxyz)
+    for (int a = 0; a < 3; a++) S->h[a] = hxyz[a];
+  const int st = guarded(base, [&]() {
+    ck(cudaStreamSynchronize(base->stream), "sync base");
+    S->coef_elems = (int64_t)(s.N[0] + 2) * (s.N[1] + 2) * (s.dim == 3 ? s.N[2] + 2 : 1);
+    S->d_coef = dalloc<double>(S->coef_elems, "alloc server coefficients");
+    ck(cudaMemcpy(S->d_coef, d_coef, S->coef_elems * sizeof(double), cudaMemcpyDeviceToDevice),
+       "copy coefficients");
+    S->pool_elems = pool_bytes / (int64_t)base->esz;
+    S->d_pool = dalloc<unsigned char>((size_t)S->pool_elems * base->esz, "alloc server pool");
+    S->pool.reset(new PoolAlloc(S->pool_elems));
+    S->base_table.resize(s.fronts.size());
+    for (size_t i = 0; i < s.fronts.size(); i++) {
+      const mfgpu::Front& f = s.fronts[i];
+      S->base_table[i] = FrontDev{f.off, f.dof_off, f.n, f.m, f.N, f.ld};
+    }
+    for (int k = 0; k < slots; k++) {
+      S->views.push_back(makeView(*base));
+      S->slot_coef.push_back(dalloc<double>(S->coef_elems, "alloc slot coefficients"));
+    }
+  });
+  if (st != MFGPU_OK) return st;
+  for (int k = 0; k < slots; k++) S->workers.emplace_back([srv = S.get(), k]() { srv->run(k); });
+  *out = S.release();
+  return MFGPU_OK;
+}
+
+int mfgpu_server_submit(mfgpu_server* srv, const int* box_lo, const int* box_hi, double factor,
+                        const double* b, int nrhs, int64_t ld, double* x, int64_t* ticket) {
+  if (!srv || !box_lo || !box_hi || !b || !x || !ticket || nrhs <= 0) return MFGPU_ERR_ARG;
+  const Schedule& s = *srv->base->S;
+  if (ld < s.ndof) return MFGPU_ERR_ARG;
+  auto r = std::make_shared<Request>();
+  for (int a = 0; a < 3; a++) {
+    r->lo[a] = a < s.dim ? box_lo[a] : 0;
+    r->hi[a] = a < s.dim ? box_hi[a] : 1;
+    if (a < s.dim && (r->lo[a] < 0 || r->hi[a] > s.N[a] || r->lo[a] >= r->hi[a]))
+      return MFGPU_ERR_ARG;
+  }
+  r->factor = factor;
+  r->nrhs = nrhs;
+  r->b.resize((size_t)s.ndof * nrhs);
+  for (int c = 0; c < nrhs; c++)
+    std::copy(b + (int64_t)c * ld, b + (int64_t)c * ld + s.ndof, r->b.begin() + (int64_t)c * s.ndof);
+  r->x = x;
+  r->ldx = ld;
+  r->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    r->id = srv->next_id++;
+    srv->all[r->id] = r;
+    srv->queue.push_back(r);
+  }
+  srv->cv_queue.notify_one();
+  *ticket = r->id;
+  return MFGPU_OK;
+}
+
+int mfgpu_server_wait(mfgpu_server* srv, int64_t ticket, mfgpu_request_info* info) {
+  if (!srv) return MFGPU_ERR_ARG;
+  std::shared_ptr<Request> r;
+  {
+    std::unique_lock<std::mutex> lk(srv->mu);
+    auto it = srv->all.find(ticket);
+    if (it == srv->all.end()) return MFGPU_ERR_ARG;
+    r = it->second;
+    srv->cv_done.wait(lk, [&] { return r->done; });
+    srv->all.erase(it);
+  }
+  if (info) {
+    std::memset(info, 0, sizeof(*info));
+    info->status = r->status;
+    const auto us = [](Clock::duration d) {
+      return std::chrono::duration<double>(d).count();
+    };
+    info->queued_seconds = us(r->t_start - r->t_submit);
+    info->latency_seconds = us(r->t_done - r->t_submit);
+    info->fronts = r->nfronts;
+    info->pool_bytes = r->footprint * (int64_t)srv->base->esz;
+    info->iterations = r->stats.iterations;
+    info->residual = r->stats.residual;
+  }
+  if (r->status != MFGPU_OK) srv->err = r->error;
+  return r->status;
+}
+
+const char* mfgpu_server_last_error(const mfgpu_server* srv) { return srv ? srv->err.c_str() : ""; }
+
+void mfgpu_server_destroy(mfgpu_server* srv) { delete srv; }
 
 }  // extern "C"

@@ -18,7 +18,7 @@ from . import _lib
 from ._lib import MFGPU_FP64, MFGPU_MIXED, TASK_DTYPE
 from .stencil import CSR, build_laplacian
 
-__all__ = ["MF2D", "MF3D", "MFBatch", "Symbolic", "CSR", "build_laplacian", "MFGPU_FP64",
+__all__ = ["MF2D", "MF3D", "MFBatch", "Server", "Symbolic", "CSR", "build_laplacian", "MFGPU_FP64",
            "MFGPU_MIXED", "MFError"]
 
 
@@ -261,6 +261,66 @@ class MFBatch(_MFBase):
         self._check(self._lib.mfgpu_update(self._h, _lib._ptr(B.val), B.nnz, _lib._ptr(mod),
                                            len(mod)))
         self.mats, self.A = mats, B
+
+
+class Server:
+    """Update-serving loop over a factored MF2D/MF3D (mfgpu_server_create).
+
+    submit(lo, hi, factor, b) queues a request (coefficients of the cell box
+    [lo, hi) times `factor`, right-hand sides b of shape (n,) or (n, k)) and
+    returns a ticket; wait(ticket) returns (x, info).  Requests are independent:
+    each answer is that of the base matrix under its own change.
+    """
+
+    def __init__(self, F, coef, slots=4, pool_gb=8.0, h=(1.0, 1.0, 1.0)):
+        import torch
+        self.F = F
+        self._lib = F._lib
+        self._coef = torch.from_numpy(np.ascontiguousarray(coef, np.float64)).cuda()
+        hh = np.ascontiguousarray(h, np.float64)
+        srv = C.c_void_p()
+        st = self._lib.mfgpu_server_create(F._h, C.c_void_p(self._coef.data_ptr()), _lib._ptr(hh),
+                                           int(slots), int(pool_gb * 2 ** 30), C.byref(srv))
+        if st != _lib.MFGPU_OK:
+            _raise(st, self._lib.mfgpu_last_error(F._h).decode())
+        self._srv = srv
+        self._pending = {}
+
+    def submit(self, lo, hi, factor, b):
+        b = np.asarray(b, np.float64)
+        one = b.ndim == 1
+        B = np.asfortranarray(b.reshape(-1, 1) if one else b)
+        X = np.zeros_like(B, order="F")
+        lo3 = np.ascontiguousarray(list(lo) + [0] * (3 - len(lo)), np.int32)
+        hi3 = np.ascontiguousarray(list(hi) + [1] * (3 - len(hi)), np.int32)
+        t = C.c_int64()
+        st = self._lib.mfgpu_server_submit(self._srv, _lib._ptr(lo3), _lib._ptr(hi3), float(factor),
+                                           B.ctypes.data_as(C.c_void_p), B.shape[1], B.shape[0],
+                                           X.ctypes.data_as(C.c_void_p), C.byref(t))
+        if st != _lib.MFGPU_OK:
+            _raise(st, "bad request")
+        self._pending[t.value] = (B, X, one)     # keep the buffers alive
+        return t.value
+
+    def wait(self, ticket):
+        info = _lib.RequestInfo()
+        st = self._lib.mfgpu_server_wait(self._srv, int(ticket), C.byref(info))
+        B, X, one = self._pending.pop(ticket)
+        if st != _lib.MFGPU_OK:
+            _raise(st, self._lib.mfgpu_server_last_error(self._srv).decode())
+        d = {f: getattr(info, f) for f, _ in _lib.RequestInfo._fields_ if f not in ("pad", "reserved")}
+        return (X[:, 0] if one else X), d
+
+    def close(self):
+        if getattr(self, "_srv", None):
+            self._lib.mfgpu_server_destroy(self._srv)
+            self._srv = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _block_diag(mats):

@@ -32,6 +32,8 @@ EXPORTED = [
     "mfgpu_profile_enable", "mfgpu_profile_reset", "mfgpu_profile_read", "mfgpu_kernel_launches",
     "mfgpu_symbolic_dirty", "mfgpu_batch_create", "mfgpu_batch_info",
     "mfgpu_symbolic_batch_create", "mfgpu_stencil_assemble_device", "mfgpu_stencil_update_device",
+    "mfgpu_server_create", "mfgpu_server_submit", "mfgpu_server_wait", "mfgpu_server_last_error",
+    "mfgpu_server_destroy",
 ]
 
 KERNEL_CLASSES = ["assemble", "potrf", "trsm", "syrk", "solve", "apply", "front", "coop", "tc"]
@@ -47,6 +49,12 @@ class Info(C.Structure):
                 ("ndof", C.c_int64), ("nnz", C.c_int64), ("leaf_box", C.c_int * 3),
                 ("max_front", C.c_int), ("factor_flops", C.c_double), ("front_bytes", C.c_int64),
                 ("sep_bytes", C.c_int64), ("device_bytes", C.c_int64)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("fronts", C.c_int), ("iterations", C.c_int), ("pad", C.c_int),
+                ("queued_seconds", C.c_double), ("latency_seconds", C.c_double),
+                ("residual", C.c_double), ("pool_bytes", C.c_int64), ("reserved", C.c_int64 * 4)]
 
 
 class Stats(C.Structure):
@@ -124,6 +132,18 @@ def load(path=None):
     lib.mfgpu_symbolic_create.restype = C.c_int
     lib.mfgpu_symbolic_batch_create.argtypes = [C.c_int] + [C.c_void_p] * 6 + [C.POINTER(P)]
     lib.mfgpu_symbolic_batch_create.restype = C.c_int
+    lib.mfgpu_server_create.argtypes = [P, C.c_void_p, C.c_void_p, C.c_int, C.c_int64,
+                                        C.POINTER(P)]
+    lib.mfgpu_server_create.restype = C.c_int
+    lib.mfgpu_server_submit.argtypes = [P, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_int,
+                                        C.c_int64, C.c_void_p, C.POINTER(C.c_int64)]
+    lib.mfgpu_server_submit.restype = C.c_int
+    lib.mfgpu_server_wait.argtypes = [P, C.c_int64, C.POINTER(RequestInfo)]
+    lib.mfgpu_server_wait.restype = C.c_int
+    lib.mfgpu_server_last_error.argtypes = [P]
+    lib.mfgpu_server_last_error.restype = C.c_char_p
+    lib.mfgpu_server_destroy.argtypes = [P]
+    lib.mfgpu_server_destroy.restype = None
     lib.mfgpu_stencil_assemble_device.argtypes = [P, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.mfgpu_stencil_assemble_device.restype = C.c_int
     lib.mfgpu_stencil_update_device.argtypes = [P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
