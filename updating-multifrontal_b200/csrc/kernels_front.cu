@@ -1234,15 +1234,16 @@ cudaError_t launch_level_coop(const int* flist, int nf, int maxn, const FrontDev
   if (me != cudaSuccess) return me;
   if (K1 < 0) K1 = maxn;
   const size_t sm = 2 * 64 * kPS * sizeof(T) + (size_t)(kMaxCoopFronts + 1) * sizeof(int);
-  static int grid = 0;   // co-resident CTAs of this instantiation on this device
-  if (grid == 0) {
+  // co-resident CTAs of this instantiation (thread-safe one-time set-up: the
+  // serving loop launches from several host threads)
+  static const int grid = [sm]() {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaFuncSetAttribute(k_level_coop<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_level_coop<T>, kCT, sm);
-    grid = sms * (per > 0 ? per : 1);
-  }
+    return sms * (per > 0 ? per : 1);
+  }();
   void* args[] = {(void*)&flist, (void*)&nf,    (void*)&fr,         (void*)&F,
                   (void*)&err,   (void*)&maxn,  (void*)&slots,      (void*)&phase_pref,
                   (void*)&K0,    (void*)&K1,    (void*)&phase0,     (void*)&trailing,
@@ -1258,7 +1259,13 @@ void launch_front_small(const int* flist, int nf, int maxN, const FrontDev* fr, 
                         cudaStream_t st) {
   if (nf <= 0) return;
   const size_t sm = (size_t)((maxN + 31) & ~31) * kPS * sizeof(T);
-  cudaFuncSetAttribute(k_front_small<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  // the largest dynamic size any launch asks for, set once (launches from
+  // several host threads must not race on the attribute)
+  static const bool attr = (cudaFuncSetAttribute(k_front_small<T>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 200 * 1024),
+                            true);
+  (void)attr;
   k_front_small<T><<<nf, 256, sm, st>>>(flist, fr, F, err);
   g_launches++;
 }
@@ -1284,8 +1291,11 @@ void launch_solve_fwd(const int* flist, int nf, int maxN, const FrontDev* fr, co
   smemFor(maxN, nrhs, sizeof(T), sm, use);
 #define MFGPU_FWD(NR)                                                                          \
   do {                                                                                         \
-    if (sm) cudaFuncSetAttribute(k_solve_fwd<T, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                 (int)sm);                                                     \
+    static const bool attr_ = (cudaFuncSetAttribute(k_solve_fwd<T, NR>,                     \
+                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                                    kSolveSmemBytes),                             \
+                               true);                                                             \
+    (void)attr_;                                                                                  \
     k_solve_fwd<T, NR><<<nf, ST, sm, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff, use);    \
   } while (0)
   if (nrhs == 1) MFGPU_FWD(1);
@@ -1306,8 +1316,11 @@ void launch_solve_bwd(const int* flist, int nf, int maxN, const FrontDev* fr, co
   smemFor(maxN, nrhs, sizeof(T), sm, use);
 #define MFGPU_BWD(NR)                                                                          \
   do {                                                                                         \
-    if (sm) cudaFuncSetAttribute(k_solve_bwd<T, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                 (int)sm);                                                     \
+    static const bool attr_ = (cudaFuncSetAttribute(k_solve_bwd<T, NR>,                     \
+                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                                    kSolveSmemBytes),                             \
+                               true);                                                             \
+    (void)attr_;                                                                                  \
     k_solve_bwd<T, NR><<<nf, ST, sm, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff, use);    \
   } while (0)
   if (nrhs == 1) MFGPU_BWD(1);
@@ -1326,8 +1339,11 @@ void launch_root_solve(int f, int N, const FrontDev* fr, const T* F, const int* 
   smemFor(N, nrhs, sizeof(T), sm, use);
 #define MFGPU_ROOT(NR)                                                                          \
   do {                                                                                          \
-    if (sm) cudaFuncSetAttribute(k_root_solve<T, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                 (int)sm);                                                      \
+    static const bool attr_ = (cudaFuncSetAttribute(k_root_solve<T, NR>,                     \
+                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                                    kSolveSmemBytes),                             \
+                               true);                                                             \
+    (void)attr_;                                                                                  \
     k_root_solve<T, NR><<<1, ST, sm, st>>>(f, fr, F, dofs, X, ldx, nrhs, W, woff, use);         \
   } while (0)
   if (nrhs == 1) MFGPU_ROOT(1);

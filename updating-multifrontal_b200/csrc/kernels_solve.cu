@@ -461,11 +461,8 @@ cudaError_t launchCoopSolve(bool fwd, const int* flist, int nf, int maxn, const 
                             const int64_t* woff, unsigned* gbar, DevError* err, cudaStream_t st) {
   cudaError_t me = cudaMemsetAsync(gbar, 0, sizeof(unsigned), st);
   if (me != cudaSuccess) return me;
-  static int gf = 0, gb = 0;
-  if (gf == 0) {
-    gf = coopGrid(k_solve_coop_fwd<T, NR>);
-    gb = coopGrid(k_solve_coop_bwd<T, NR>);
-  }
+  static const int gf = coopGrid(k_solve_coop_fwd<T, NR>);   // thread-safe one-time set-up
+  static const int gb = coopGrid(k_solve_coop_bwd<T, NR>);
   int maxnb = cdiv(maxn, SB);
   void* args[] = {(void*)&flist, (void*)&nf,   (void*)&fr,   (void*)&F,
                   (void*)&dofs,  (void*)&X,    (void*)&ldx,  (void*)&nrhs,

@@ -408,14 +408,14 @@ cudaError_t launch_trail_tc(const int* flist, int nf, int64_t ntiles, const Fron
                             int K, int split, DevError* err, cudaStream_t st) {
   if (nf <= 0 || ntiles <= 0) return cudaSuccess;
   if (nf > kMaxTcFronts || (split != 1 && split != 3)) return cudaErrorInvalidValue;
-  static int sms = 0;
-  if (sms == 0) {
-    int dev = 0;
+  static const int sms = []() {   // thread-safe one-time set-up
+    int dev = 0, n = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
     cudaFuncSetAttribute(k_trail_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
     cudaFuncSetAttribute(k_trail_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
-  }
+    return n;
+  }();
   const int grid = (int)std::min<int64_t>(ntiles, sms);
   if (split == 3)
     k_trail_tc<3><<<grid, TCT, kTcSmem, st>>>(flist, nf, fr, F, K, err);
