@@ -53,6 +53,10 @@ WORKLOADS = {
     # 256 independent 2D problems in one handle (sides 63..511, 1-8 RHS each)
     "batch256": dict(batch=True, count=256, sides=(63, 127, 255, 511), max_side=4, lo=0.1, hi=10.0,
                      max_nrhs=8, seed=SEED0 + 5),
+    # update serving on a resident 3D 95^3 factorization: Poisson arrivals, each
+    # request a coefficient box (side 3-15, factor log-U[0.1,10]) + 1-16 RHS
+    "serve95": dict(serve=True, dim=3, N=(95, 95, 95), max_side=4, lo=0.1, hi=10.0, side=(3, 15),
+                    nrhs=(1, 16), seed=SEED0 + 6),
     # a smaller 3D case of the same kind (profiling captures, quick checks)
     "3d-63": dict(dim=3, N=(63, 63, 63), max_side=4, lo=0.1, hi=100.0, nrhs=1, patch=5,
                   factor=10.0, seed=SEED0 + 4),
@@ -489,6 +493,122 @@ class BatchWork:
                           f"({t_tot:.2f} s), OPENBLAS_NUM_THREADS={threads}", "cpu": model}
 
 
+def run_serve(args, w):
+    """Update serving (the survey's configuration 5): a stream of requests with
+    Poisson arrivals against a resident factorization; each request changes
+    the coefficients of one box and brings right-hand sides.  Reports
+    throughput and p50/p99 latency (wall clock from submission to the result
+    on the host, queueing included) and the algorithmic TFLOP/s of the
+    completed requests (their root-path refactorizations and solves)."""
+    import threading
+    import torch
+    from mfgpu import MF2D, MF3D, MFGPU_FP64, MFGPU_MIXED, Server, Symbolic
+    if args.impl == "reference":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the reference has no serving loop; its Update + Solve per request is "
+                          "timed by the 3d workloads"}))
+        return 0
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    prec = MFGPU_MIXED if args.precision == "mixed" else MFGPU_FP64
+    N = w["N"]
+    seed = w["seed"] + 1000 * rank
+    a = stencil.loguniform_coefficients(N, w["lo"], w["hi"], seed)
+    A = stencil.build_laplacian(a)
+    F = (MF3D(A, N[0], N[1], N[2], 1, w["max_side"], device=local, precision=prec)
+         if w["dim"] == 3 else MF2D(A, N[0], N[1], 1, w["max_side"], device=local, precision=prec))
+    F.Factor()
+    rng = np.random.Generator(np.random.PCG64(seed + 1))
+    reqs = []
+    for _ in range(args.requests):
+        side = int(rng.integers(w["side"][0], w["side"][1] + 1))
+        lo = [int(rng.integers(0, n - side + 1)) for n in N]
+        factor = float(w["lo"] * (w["hi"] / w["lo"]) ** rng.random())
+        k = int(rng.integers(w["nrhs"][0], w["nrhs"][1] + 1))
+        b = rng.uniform(-1, 1, size=(A.n, k))
+        reqs.append((lo, [l + side for l in lo], factor, b))
+    gaps = rng.exponential(1.0 / args.rate, size=args.requests)
+    S = Symbolic(w["dim"], N, 1, w["max_side"])
+    fronts = [S.front(f) for f in range(S.n_fronts)]
+    solve_unit = sum(2.0 * (f["n"] ** 2 + 2.0 * f["n"] * f["m"]) for f in fronts)
+    free_gb = torch.cuda.mem_get_info()[0] / 2 ** 30
+    slot_gb = 2.5 * (1 if prec == MFGPU_MIXED else 2)     # views: values, workspaces, scratch
+    pool_gb = max(4.0, free_gb - 6.0 - args.slots * slot_gb)
+    srv = Server(F, a, slots=args.slots, pool_gb=pool_gb)
+    # one warm-up request outside the measurement
+    srv.wait(srv.submit(reqs[0][0], reqs[0][1], reqs[0][2], reqs[0][3][:, :1]))
+    results = [None] * len(reqs)
+    tickets = [None] * len(reqs)
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+
+    def producer():
+        t = t0
+        for i, (lo, hi, f, b) in enumerate(reqs):
+            t += gaps[i]
+            d = t - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets[i] = srv.submit(lo, hi, f, b)
+
+    th = threading.Thread(target=producer)
+    th.start()
+    for i in range(len(reqs)):
+        while tickets[i] is None:
+            time.sleep(0.0005)
+        results[i] = srv.wait(tickets[i])
+    th.join()
+    makespan = time.perf_counter() - t0
+    clk = clocks.stop()
+    lat = [r[1]["latency_seconds"] for r in results]
+    work = 0.0
+    for (lo, hi, f, b), (x, info) in zip(reqs, results):
+        dirty, fl = S.dirty([i + j * N[0] + k * N[0] * N[1]
+                             for k in range(max(0, lo[2] - 1), min(N[2], hi[2] + 1))
+                             for j in range(max(0, lo[1] - 1), min(N[1], hi[1] + 1))
+                             for i in range(max(0, lo[0] - 1), min(N[0], hi[0] + 1))])
+        work += fl + solve_unit * b.shape[1]
+    # correctness of what was timed: FP64 residual of one request's answer
+    lo, hi, f, b = reqs[-1]
+    Ar = stencil.build_laplacian(stencil.scale_box(a, lo, hi[0] - lo[0], f))
+    x = results[-1][0]
+    resid = max(float(np.linalg.norm(Ar.matvec(x[:, c]) - b[:, c]) / np.linalg.norm(b[:, c]))
+                for c in range(b.shape[1]))
+    srv.close()
+    line = {
+        "metric": "update-serving throughput (algorithmic TFLOP/s of completed requests) and "
+                  "latency p50/p99",
+        "value": work / makespan / 1e12, "unit": "TFLOP/s", "n_gpus": 1, "steps": len(reqs),
+        "warmup": 1, "ms_per_step": makespan / len(reqs) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32 factor + f64 refinement",
+        "data": "synthetic (seeded coefficients, boxes, factors and right-hand sides)",
+        "config": {"workload": f"{args.workload} (3D {N[0]}^3 7-point, a log-U[{w['lo']},{w['hi']}], "
+                               f"maxSideLength {w['max_side']}; {len(reqs)} requests, Poisson "
+                               f"arrivals at {args.rate}/s, box side {w['side'][0]}-{w['side'][1]}, "
+                               f"{w['nrhs'][0]}-{w['nrhs'][1]} RHS)",
+                   "slots": args.slots, "pool_gb": round(pool_gb, 1), "precision": args.precision,
+                   "timing": "wall clock, submission to result on the host"},
+        "requests_per_s": len(reqs) / makespan,
+        "latency_s": {"p50": statistics.median(lat), "p99": float(np.percentile(lat, 99)),
+                      "max": max(lat)},
+        "queued_s_p50": statistics.median(r[1]["queued_seconds"] for r in results),
+        "fronts_per_request_p50": statistics.median(r[1]["fronts"] for r in results),
+        "resid": resid, "clocks": clk,
+        "e2e": {"value": work / makespan / 1e12, "unit": "TFLOP/s",
+                "h2d_bytes_per_step": int(np.mean([b.nbytes for *_, b in reqs])),
+                "d2h_bytes_per_step": int(np.mean([b.nbytes for *_, b in reqs]))},
+    }
+    print(json.dumps(line))
+    if args.json_out:
+        with open(args.json_out, "w") as fo:
+            fo.write(json.dumps(line) + "\n")
+    F.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -499,8 +619,13 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--json-out", default=None)
+    ap.add_argument("--rate", type=float, default=4.0, help="serving: arrivals per second")
+    ap.add_argument("--requests", type=int, default=24, help="serving: requests in the stream")
+    ap.add_argument("--slots", type=int, default=4, help="serving: concurrent requests")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
+    if w.get("serve"):
+        return run_serve(args, w)
     if args.impl == "reference":
         return run_reference_arm(args, w)
 
