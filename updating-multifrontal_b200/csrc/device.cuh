@@ -101,6 +101,7 @@ void launch_front_small(const int* flist, int nf, int maxN, const FrontDev* fr, 
 bool coop_fits(int nf);
 size_t coop_slot_elems();
 std::vector<int> coop_phase_prefix(const std::vector<int>& n, const std::vector<int>& N, int maxn);
+// max_items (> 0): the largest work-item count of any phase, to size the grid;
 // K0/K1/phase0/trailing restrict the launch to the outer panels [K0, K1)
 // (K1 < 0: to the end) and optionally leave the last trailing update out.
 // gbar: one unsigned of device memory for the launch's grid barrier.
@@ -108,7 +109,7 @@ template <class T>
 cudaError_t launch_level_coop(const int* flist, int nf, int maxn, const FrontDev* fr, T* F,
                               DevError* err, T* slots, const int* phase_pref, unsigned* gbar,
                               cudaStream_t st, int K0 = 0, int K1 = -1, int phase0 = 0,
-                              int trailing = 1);
+                              int trailing = 1, int max_items = 0);
 int coop_outer();                   // outer panel width of the cooperative kernel
 int coop_phases(int K, int maxn);   // phases of outer panel K in the prefix table
 

@@ -1228,7 +1228,8 @@ int coop_phases(int K, int maxn) {
 template <class T>
 cudaError_t launch_level_coop(const int* flist, int nf, int maxn, const FrontDev* fr, T* F,
                               DevError* err, T* slots, const int* phase_pref, unsigned* gbar,
-                              cudaStream_t st, int K0, int K1, int phase0, int trailing) {
+                              cudaStream_t st, int K0, int K1, int phase0, int trailing,
+                              int max_items) {
   if (nf <= 0) return cudaSuccess;
   cudaError_t me = cudaMemsetAsync(gbar, 0, sizeof(unsigned), st);
   if (me != cudaSuccess) return me;
@@ -1248,7 +1249,11 @@ cudaError_t launch_level_coop(const int* flist, int nf, int maxn, const FrontDev
                   (void*)&err,   (void*)&maxn,  (void*)&slots,      (void*)&phase_pref,
                   (void*)&K0,    (void*)&K1,    (void*)&phase0,     (void*)&trailing,
                   (void*)&gbar};
-  cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_level_coop<T>, dim3(grid), dim3(kCT),
+  // levels with little parallel work: one CTA per work item, at least an
+  // eighth of the full grid (a grid barrier costs more the more CTAs arrive)
+  int g = grid;
+  if (max_items > 0) g = std::min(grid, std::max(max_items, std::max(1, grid / 8)));
+  cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_level_coop<T>, dim3(g), dim3(kCT),
                                               args, sm, st);
   g_launches++;
   return e;
@@ -1389,7 +1394,7 @@ void launch_sep_gather(const int* slist, int ns, const SepDev* sp, const int* do
                                 const int*, const double*, const int*, const double*, cudaStream_t); \
   template cudaError_t launch_level_coop<T>(const int*, int, int, const FrontDev*, T*, DevError*,  \
                                             T*, const int*, unsigned*, cudaStream_t, int, int, int, \
-                                            int);                                                   \
+                                            int, int);                                              \
   template void launch_front_small<T>(const int*, int, int, const FrontDev*, T*, DevError*,        \
                                       cudaStream_t);                                                \
   template void launch_solve_fwd<T>(const int*, int, int, const FrontDev*, const T*, const int*,   \

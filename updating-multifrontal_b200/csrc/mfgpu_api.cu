@@ -69,6 +69,7 @@ struct Plan {
     int maxN = 0, maxn = 0;
     Group ftask, sbase, sadd0, sadd1;
     int64_t cpref0 = 0;   // offset of the cooperative kernel's phase prefixes in cpref
+    int coopItems = 0;    // largest work-item count of any cooperative phase
   };
   std::vector<Level> lv;
   std::vector<Task> tasks;
@@ -381,6 +382,11 @@ struct mfgpu_handle {
         }
         std::vector<int> pp = mfgpu::coop_phase_prefix(nn, NN, L.maxn);
         P.cpref.insert(P.cpref.end(), pp.begin(), pp.end());
+        // the most work items any phase has: a level with little parallel work
+        // runs on fewer CTAs, so its grid barriers are cheaper
+        const size_t stride = fl.size() + 1;
+        for (size_t q = 0; q + stride <= pp.size(); q += stride)
+          L.coopItems = std::max(L.coopItems, pp[q + fl.size()]);
       }
     }
   }
@@ -442,7 +448,8 @@ struct mfgpu_handle {
           prof.flops[MFGPU_KC_COOP] += fl;
           prof.begin(MFGPU_KC_COOP, stream);
           ck(mfgpu::launch_level_coop<T>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, F, d_err,
-                                         (T*)d_slots, P.d_cpref + L.cpref0, d_gbar, stream),
+                                         (T*)d_slots, P.d_cpref + L.cpref0, d_gbar, stream, 0, -1,
+                                         0, 1, L.coopItems),
              "launch cooperative level factorization (k_level_coop)");
           prof.end(stream);
         }
@@ -489,7 +496,7 @@ struct mfgpu_handle {
       prof.begin(MFGPU_KC_COOP, stream);
       ck(mfgpu::launch_level_coop<float>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, (float*)d_F,
                                          d_err, (float*)d_slots, P.d_cpref + L.cpref0, d_gbar,
-                                         stream, K, K + outer, phase0, 0),
+                                         stream, K, K + outer, phase0, 0, L.coopItems),
          "launch cooperative panel factorization (k_level_coop)");
       prof.end(stream);
       phase0 += mfgpu::coop_phases(K, L.maxn);
