@@ -126,10 +126,19 @@ cudaError_t launch_trail_tc(const int* flist, int nf, int64_t ntiles, const Fron
 // solve_coop_max_fronts() fronts, nrhs <= 16): forward = gather, L11 solve
 // and boundary update; backward = gather, L21^T update and L11^T solve.
 int solve_coop_max_fronts();
+// The cooperative sweeps apply each 64 x 64 pivot block through its explicit
+// inverse (Dv, per front at dinv_off, written by launch_diag_inv after the
+// front is factored) and keep solved blocks in the second half of the front's
+// workspace, so a step needs no single-CTA substitution.
 template <class T>
 cudaError_t launch_solve_coop(bool forward, const int* flist, int nf, int maxn, const FrontDev* fr,
                               const T* F, const int* dofs, T* X, int64_t ldx, int nrhs, T* W,
-                              const int64_t* woff, unsigned* gbar, DevError* err, cudaStream_t st);
+                              const int64_t* woff, const T* Dv, const int64_t* dinv_off,
+                              unsigned* gbar, DevError* err, cudaStream_t st);
+constexpr int kDinvBlock = 64;   // diagonal-block size of the cooperative sweeps
+template <class T>
+void launch_diag_inv(const int* flist, int nf, int maxn, const FrontDev* fr, const T* F, T* Dv,
+                     const int64_t* dinv_off, cudaStream_t st);
 
 // Stencil assembly (width 1): recompute the CSR values of the rows of the
 // cells in [lo, hi) from the node coefficients; with `flag`, record which rows

@@ -414,7 +414,7 @@ __device__ __forceinline__ void row_trsm(double (&x)[kPanel], const double (*L)[
 // The panel of each step is staged in shared memory for the tensor-core update.
 // ---------------------------------------------------------------------------
 template <class T>
-__global__ void __launch_bounds__(256) k_front_small(const int* __restrict__ flist,
+__global__ void __launch_bounds__(256, 2) k_front_small(const int* __restrict__ flist,
                                                      const FrontDev* __restrict__ fr,
                                                      T* __restrict__ F, DevError* err) {
   extern __shared__ __align__(16) unsigned char smraw[];

@@ -8,18 +8,22 @@
 //
 //   forward  (src/DE/mf2d.cpp:976-1014, the per-box L11 solve and the
 //   boundary update b_bd -= L21 y):
-//     step j: every CTA takes 256 rows below block j and applies
-//             W(rows) -= L(rows, block j) y_j; the CTA holding the rows of
-//             block j+1 then solves that block (lookahead); grid barrier.
+//     step j: every CTA with work forms y_j = L_jj^{-1} w_j from the block's
+//             explicit inverse, takes 256 rows below block j and applies
+//             W(rows) -= L(rows, block j) y_j; grid barrier.
 //   backward (src/DE/mf2d.cpp:1016-1054, x_piv = L11^{-T}(y - L21^T x_bd)):
-//     first r = y - L21^T x_bd by column blocks, then for j = last .. 1
-//     every CTA takes one column block c < j and applies
-//     r_c -= L(block j, block c)^T x_j; the CTA holding block j-1 then solves
-//     it; grid barrier.
+//     first r = y - L21^T x_bd by column blocks; then for j = last .. 0 every
+//     CTA with work forms x_j = L_jj^{-T} r_j, takes one column block c < j and
+//     applies r_c -= L(block j, block c)^T x_j; grid barrier.
+// The inverses (k_diag_inv, after each factorization of the level) take the
+// sequential substitution out of every step: a step costs one block product,
+// one pass over a panel and one grid barrier.
 //
 // Each front's L is read once per sweep.  W is the front's right-hand-side
 // block (N x nrhs, ld N) in the same workspace the per-front kernels use, so
-// the separator gathers between levels are unchanged.
+// the separator gathers between levels are unchanged; the solved pivot blocks
+// go to the second half of that workspace (another N x nrhs), so no step reads
+// what another CTA of the same step writes.
 #include <cooperative_groups.h>
 
 #include <atomic>
@@ -38,7 +42,6 @@ namespace {
 constexpr int SB = 64;          // diagonal block of the substitution
 constexpr int SCT = 256;        // threads per CTA
 constexpr int kMaxSolveCoopFronts = SCT;
-constexpr int SP = 32;          // sub-block solved by one warp
 
 __host__ __device__ __forceinline__ int cdiv(int a, int b) { return (a + b - 1) / b; }
 
@@ -80,110 +83,43 @@ __device__ __forceinline__ int find_front(const int* pre, int nf, int item) {
   return lo;
 }
 
-// In place: W(k:k+kb, :) <- L(k:k+kb, k:k+kb)^{-1} W(k:k+kb, :), kb <= SB.
-// Warp 0 substitutes 32-row sub-blocks; the whole CTA updates the rows of the
-// second sub-block in between.  Every thread must call.
-template <class T, int NR>
-__device__ void diag_lower_solve(const T* __restrict__ A, int64_t ld, T* W, int N, int k, int kb,
-                                 int nrhs, T (*Ls)[SP + 1], T (*xs)[NR + 1]) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int s = 0; s < kb; s += SP) {
-    const int sb = min(SP, kb - s), k0 = k + s;
-    __syncthreads();
-    for (int idx = tid; idx < sb * sb; idx += SCT) {
-      const int i = idx % sb, j = idx / sb;
-      if (i >= j) Ls[i][j] = A[(k0 + i) + (int64_t)(k0 + j) * ld];
-    }
-    for (int idx = tid; idx < sb * nrhs; idx += SCT) {
-      const int i = idx % sb, c = idx / sb;
-      xs[i][c] = W[k0 + i + (int64_t)c * N];
-    }
-    __syncthreads();
-    if (warp == 0) {
-      for (int j = 0; j < sb; j++) {
-        if (lane == j) {
-          const T djj = Ls[j][j];
-#pragma unroll
-          for (int c = 0; c < NR; c++)
-            if (c < nrhs) xs[j][c] = xs[j][c] / djj;
-        }
-        __syncwarp();
-        if (lane > j && lane < sb) {
-          const T l = Ls[lane][j];
-#pragma unroll
-          for (int c = 0; c < NR; c++)
-            if (c < nrhs) xs[lane][c] -= l * xs[j][c];
-        }
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-    for (int idx = tid; idx < sb * nrhs; idx += SCT) {
-      const int i = idx % sb, c = idx / sb;
-      W[k0 + i + (int64_t)c * N] = xs[i][c];
-    }
-    // rows of the remaining sub-block: W(r) -= L(r, k0:k0+sb) x
-    const int rend = k + kb;
-    for (int idx = tid; idx < (rend - k0 - sb) * nrhs; idx += SCT) {
-      const int r = k0 + sb + idx % (rend - k0 - sb), c = idx / (rend - k0 - sb);
-      T acc = T(0);
-      for (int t = 0; t < sb; t++) acc = fma(A[r + (int64_t)(k0 + t) * ld], xs[t][c], acc);
-      W[r + (int64_t)c * N] -= acc;
+// Diagonal-block inverses of the cooperative levels' pivot blocks: block b of
+// front f (rows and columns [64 b, 64 b + kb)) gets Dinv = L_bb^{-1} (lower,
+// column-major 64 x 64, zero outside kb x kb) at Dv + dinv_off[f] + b * 8192
+// and its transpose right after it.  Column t of the inverse is computed by
+// thread t with forward substitution on the block staged in shared memory.
+template <class T>
+__global__ void __launch_bounds__(SB) k_diag_inv(const int* __restrict__ flist,
+                                                 const FrontDev* __restrict__ fr,
+                                                 const T* __restrict__ F, T* __restrict__ Dv,
+                                                 const int64_t* __restrict__ dinv_off) {
+  extern __shared__ __align__(16) unsigned char dsm[];   // Ls and Iv, 2 x 64 x 65
+  T(*Ls)[SB + 1] = reinterpret_cast<T(*)[SB + 1]>(dsm);
+  T(*Iv)[SB + 1] = Ls + SB;
+  const int f = flist[blockIdx.y];
+  const FrontDev d = fr[f];
+  const int b = blockIdx.x, k = b * SB;
+  if (k >= d.n || dinv_off[f] < 0) return;
+  const int kb = min(SB, d.n - k), t = threadIdx.x;
+  const T* A = F + d.off;
+  for (int c = 0; c < kb; c++)
+    if (t < kb) Ls[t][c] = t >= c ? A[(k + t) + (int64_t)(k + c) * d.ld] : T(0);
+  __syncthreads();
+  if (t < kb) {
+    for (int i = 0; i < t; i++) Iv[i][t] = T(0);
+    for (int i = t; i < kb; i++) {
+      T acc = i == t ? T(1) : T(0);
+      for (int q = t; q < i; q++) acc = fma(-Ls[i][q], Iv[q][t], acc);
+      Iv[i][t] = acc / Ls[i][i];
     }
   }
   __syncthreads();
-}
-
-// In place: W(k:k+kb, :) <- L(k:k+kb, k:k+kb)^{-T} W(k:k+kb, :), kb <= SB.
-template <class T, int NR>
-__device__ void diag_upper_solve(const T* __restrict__ A, int64_t ld, T* W, int N, int k, int kb,
-                                 int nrhs, T (*Ls)[SP + 1], T (*xs)[NR + 1]) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nsub = cdiv(kb, SP);
-  for (int q = nsub - 1; q >= 0; q--) {
-    const int s = q * SP, sb = min(SP, kb - s), k0 = k + s;
-    __syncthreads();
-    for (int idx = tid; idx < sb * sb; idx += SCT) {
-      const int i = idx % sb, j = idx / sb;
-      if (i >= j) Ls[i][j] = A[(k0 + i) + (int64_t)(k0 + j) * ld];
-    }
-    for (int idx = tid; idx < sb * nrhs; idx += SCT) {
-      const int i = idx % sb, c = idx / sb;
-      xs[i][c] = W[k0 + i + (int64_t)c * N];
-    }
-    __syncthreads();
-    if (warp == 0) {
-      for (int j = sb - 1; j >= 0; j--) {
-        if (lane == j) {
-          const T djj = Ls[j][j];
-#pragma unroll
-          for (int c = 0; c < NR; c++)
-            if (c < nrhs) xs[j][c] = xs[j][c] / djj;
-        }
-        __syncwarp();
-        if (lane < j) {
-          const T l = Ls[j][lane];
-#pragma unroll
-          for (int c = 0; c < NR; c++)
-            if (c < nrhs) xs[lane][c] -= l * xs[j][c];
-        }
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-    for (int idx = tid; idx < sb * nrhs; idx += SCT) {
-      const int i = idx % sb, c = idx / sb;
-      W[k0 + i + (int64_t)c * N] = xs[i][c];
-    }
-    // columns of the earlier sub-block: W(col) -= L(k0:k0+sb, col)^T x
-    for (int idx = tid; idx < s * nrhs; idx += SCT) {
-      const int col = k + idx % s, c = idx / s;
-      T acc = T(0);
-      for (int t = 0; t < sb; t++) acc = fma(A[(k0 + t) + (int64_t)col * ld], xs[t][c], acc);
-      W[col + (int64_t)c * N] -= acc;
-    }
+  T* D = Dv + dinv_off[f] + (int64_t)b * 2 * SB * SB;
+  for (int c = 0; c < SB; c++) {
+    const int r = t;
+    D[r + c * SB] = (r < kb && c < kb) ? Iv[r][c] : T(0);                 // Dinv
+    D[SB * SB + r + c * SB] = (r < kb && c < kb) ? Iv[c][r] : T(0);       // Dinv^T
   }
-  __syncthreads();
 }
 
 template <class T, int NR>
@@ -193,13 +129,14 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_fwd(const int* __restrict__ 
                                                         const int* __restrict__ dofs, T* X,
                                                         int64_t ldx, int nrhs, T* Wb,
                                                         const int64_t* __restrict__ woff,
-                                                        int maxnb, unsigned* gbar, DevError* err) {
+                                                        int maxnb, const T* __restrict__ Dv,
+                                                        const int64_t* __restrict__ dinv_off,
+                                                        unsigned* gbar, DevError* err) {
   unsigned gtarget = 0;
   __shared__ int pre[kMaxSolveCoopFronts + 1];
   __shared__ int wt[SCT / 32];
+  __shared__ T ws[SB][NR + 1];
   __shared__ T ys[SB][NR + 1];
-  __shared__ T Ls[SP][SP + 1];
-  __shared__ T xs[SP][NR + 1];
   const int tid = threadIdx.x;
   const int64_t gstride = (int64_t)gridDim.x * SCT;
   // gather: pivot rows from X, boundary rows zero
@@ -214,23 +151,12 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_fwd(const int* __restrict__ 
     }
   }
   grid_barrier(gbar, gtarget, err);
-  for (int i = blockIdx.x; i < nf; i += gridDim.x) {
-    const int f = flist[i];
-    const FrontDev d = fr[f];
-    if (d.n > 0)
-      diag_lower_solve<T, NR>(F + d.off, d.ld, Wb + woff[f] * nrhs, d.N, 0, min(SB, d.n), nrhs, Ls,
-                              xs);
-  }
-  grid_barrier(gbar, gtarget, err);
   for (int j = 0; j < maxnb; j++) {
     int cnt = 0;
     if (tid < nf) {
       const FrontDev d = fr[flist[tid]];
       const int k = j * SB;
-      if (k < d.n) {
-        const int r0 = k + min(SB, d.n - k);
-        if (d.N > r0) cnt = cdiv(d.N - r0, SCT);
-      }
+      if (k < d.n) cnt = max(1, cdiv(d.N - k - min(SB, d.n - k), SCT));
     }
     scan_counts(cnt, nf, pre, wt);
     for (int item = blockIdx.x; item < pre[nf]; item += gridDim.x) {
@@ -238,16 +164,32 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_fwd(const int* __restrict__ 
       const int f = flist[i];
       const FrontDev d = fr[f];
       const T* A = F + d.off;
-      T* W = Wb + woff[f] * nrhs;
+      T* W = Wb + woff[f] * nrhs;          // right-hand sides being reduced
+      T* Y = W + (int64_t)d.N * nrhs;      // solved pivot blocks
       const int k = j * SB, kb = min(SB, d.n - k);
       const int local = item - pre[i];
       const int r0 = k + kb + local * SCT;
+      // y_j = Dinv_j w_j (w_j is final: every block above it was applied)
       __syncthreads();
       for (int idx = tid; idx < SB * nrhs; idx += SCT) {
         const int t = idx % SB, c = idx / SB;
-        ys[t][c] = t < kb ? W[k + t + (int64_t)c * d.N] : T(0);
+        ws[t][c] = t < kb ? W[k + t + (int64_t)c * d.N] : T(0);
       }
       __syncthreads();
+      const T* Dj = Dv + dinv_off[f] + (int64_t)j * 2 * SB * SB;
+      for (int idx = tid; idx < SB * nrhs; idx += SCT) {
+        const int t = idx % SB, c = idx / SB;
+        T acc = T(0);
+        for (int q = 0; q <= t && q < kb; q++) acc = fma(Dj[t + q * SB], ws[q][c], acc);
+        ys[t][c] = t < kb ? acc : T(0);
+      }
+      __syncthreads();
+      if (local == 0)
+        for (int idx = tid; idx < kb * nrhs; idx += SCT) {
+          const int t = idx % kb, c = idx / kb;
+          Y[k + t + (int64_t)c * d.N] = ys[t][c];
+        }
+      // rows below block j: W(r) -= L(r, block j) y_j
       const int r = r0 + tid;
       if (r < d.N) {
         T acc[NR];
@@ -276,11 +218,6 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_fwd(const int* __restrict__ 
         for (int c = 0; c < NR; c++)
           if (c < nrhs) W[r + (int64_t)c * d.N] -= acc[c];
       }
-      // lookahead: the CTA holding block j+1's rows solves it now
-      if (local == 0 && k + kb < d.n) {
-        __syncthreads();
-        diag_lower_solve<T, NR>(A, d.ld, W, d.N, k + kb, min(SB, d.n - k - kb), nrhs, Ls, xs);
-      }
     }
     grid_barrier(gbar, gtarget, err);
   }
@@ -288,11 +225,11 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_fwd(const int* __restrict__ 
   for (int i = 0; i < nf; i++) {
     const int f = flist[i];
     const FrontDev d = fr[f];
-    const T* W = Wb + woff[f] * nrhs;
+    const T* Y = Wb + woff[f] * nrhs + (int64_t)d.N * nrhs;
     const int* dl = dofs + d.dof_off;
     for (int64_t idx = (int64_t)blockIdx.x * SCT + tid; idx < (int64_t)d.n * nrhs; idx += gstride) {
       const int r = (int)(idx % d.n), c = (int)(idx / d.n);
-      X[dl[r] + (int64_t)c * ldx] = W[r + (int64_t)c * d.N];
+      X[dl[r] + (int64_t)c * ldx] = Y[r + (int64_t)c * d.N];
     }
   }
 }
@@ -304,13 +241,14 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_bwd(const int* __restrict__ 
                                                         const int* __restrict__ dofs, T* X,
                                                         int64_t ldx, int nrhs, T* Wb,
                                                         const int64_t* __restrict__ woff,
-                                                        int maxnb, unsigned* gbar, DevError* err) {
+                                                        int maxnb, const T* __restrict__ Dv,
+                                                        const int64_t* __restrict__ dinv_off,
+                                                        unsigned* gbar, DevError* err) {
   unsigned gtarget = 0;
   __shared__ int pre[kMaxSolveCoopFronts + 1];
   __shared__ int wt[SCT / 32];
+  __shared__ T ws[SB][NR + 1];
   __shared__ T xj[SB][NR + 1];
-  __shared__ T Ls[SP][SP + 1];
-  __shared__ T xs[SP][NR + 1];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t gstride = (int64_t)gridDim.x * SCT;
   for (int i = 0; i < nf; i++) {
@@ -324,11 +262,13 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_bwd(const int* __restrict__ 
     }
   }
   grid_barrier(gbar, gtarget, err);
-  // r = y - L21^T x_bd, one column block per item; the CTA with the last
-  // block then solves it
+  // r = y - L21^T x_bd, one column block per item
   {
     int cnt = 0;
-    if (tid < nf) cnt = cdiv(fr[flist[tid]].n, SB);
+    if (tid < nf) {
+      const FrontDev d = fr[flist[tid]];
+      cnt = d.m > 0 ? cdiv(d.n, SB) : 0;
+    }
     scan_counts(cnt, nf, pre, wt);
     for (int item = blockIdx.x; item < pre[nf]; item += gridDim.x) {
       const int i = find_front(pre, nf, item);
@@ -337,52 +277,47 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_bwd(const int* __restrict__ 
       const T* A = F + d.off;
       T* W = Wb + woff[f] * nrhs;
       const int cb = item - pre[i], k = cb * SB, kb = min(SB, d.n - k);
-      if (d.m > 0) {
-        for (int jj = warp; jj < kb; jj += SCT / 32) {
-          const T* Lc = A + (int64_t)(k + jj) * d.ld;
-          T acc[NR];
+      for (int jj = warp; jj < kb; jj += SCT / 32) {
+        const T* Lc = A + (int64_t)(k + jj) * d.ld;
+        T acc[NR];
 #pragma unroll
-          for (int c = 0; c < NR; c++) acc[c] = T(0);
-          int r = d.n + lane;
-          for (; r + 96 < d.N; r += 128) {
-            const T l0 = Lc[r], l1 = Lc[r + 32], l2 = Lc[r + 64], l3 = Lc[r + 96];
+        for (int c = 0; c < NR; c++) acc[c] = T(0);
+        int r = d.n + lane;
+        for (; r + 96 < d.N; r += 128) {
+          const T l0 = Lc[r], l1 = Lc[r + 32], l2 = Lc[r + 64], l3 = Lc[r + 96];
 #pragma unroll
-            for (int c = 0; c < NR; c++)
-              if (c < nrhs) {
-                const T* w = W + (int64_t)c * d.N + r;
-                acc[c] = fma(l0, w[0], acc[c]);
-                acc[c] = fma(l1, w[32], acc[c]);
-                acc[c] = fma(l2, w[64], acc[c]);
-                acc[c] = fma(l3, w[96], acc[c]);
-              }
-          }
-          for (; r < d.N; r += 32) {
-            const T l = Lc[r];
-#pragma unroll
-            for (int c = 0; c < NR; c++)
-              if (c < nrhs) acc[c] = fma(l, W[r + (int64_t)c * d.N], acc[c]);
-          }
-#pragma unroll
-          for (int c = 0; c < NR; c++) {
-            T v = acc[c];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-            if (lane == 0 && c < nrhs) W[k + jj + (int64_t)c * d.N] -= v;
-          }
+          for (int c = 0; c < NR; c++)
+            if (c < nrhs) {
+              const T* w = W + (int64_t)c * d.N + r;
+              acc[c] = fma(l0, w[0], acc[c]);
+              acc[c] = fma(l1, w[32], acc[c]);
+              acc[c] = fma(l2, w[64], acc[c]);
+              acc[c] = fma(l3, w[96], acc[c]);
+            }
         }
-      }
-      if (k + kb == d.n) {
-        __syncthreads();
-        diag_upper_solve<T, NR>(A, d.ld, W, d.N, k, kb, nrhs, Ls, xs);
+        for (; r < d.N; r += 32) {
+          const T l = Lc[r];
+#pragma unroll
+          for (int c = 0; c < NR; c++)
+            if (c < nrhs) acc[c] = fma(l, W[r + (int64_t)c * d.N], acc[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < NR; c++) {
+          T v = acc[c];
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+          if (lane == 0 && c < nrhs) W[k + jj + (int64_t)c * d.N] -= v;
+        }
       }
     }
     grid_barrier(gbar, gtarget, err);
   }
-  // step t: front i works on its block j = nb_i - 1 - t
-  for (int t = 0; t < maxnb - 1; t++) {
+  // step t: front i finishes its block j = nb_i - 1 - t: x_j = Dinv_j^T r_j
+  // (r_j is final), written once, and applied to every earlier column block
+  for (int t = 0; t < maxnb; t++) {
     int cnt = 0;
     if (tid < nf) {
       const int j = cdiv(fr[flist[tid]].n, SB) - 1 - t;
-      cnt = j >= 1 ? j : 0;
+      cnt = j >= 1 ? j : (j == 0 ? 1 : 0);
     }
     scan_counts(cnt, nf, pre, wt);
     for (int item = blockIdx.x; item < pre[nf]; item += gridDim.x) {
@@ -391,16 +326,31 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_bwd(const int* __restrict__ 
       const FrontDev d = fr[f];
       const T* A = F + d.off;
       T* W = Wb + woff[f] * nrhs;
+      T* Y = W + (int64_t)d.N * nrhs;
       const int j = cdiv(d.n, SB) - 1 - t;
       const int kj = j * SB, kbj = min(SB, d.n - kj);
-      const int cb = item - pre[i], k = cb * SB;   // column block cb < j (full width)
+      const int cb = item - pre[i], k = cb * SB;
       __syncthreads();
       for (int idx = tid; idx < SB * nrhs; idx += SCT) {
         const int r = idx % SB, c = idx / SB;
-        xj[r][c] = r < kbj ? W[kj + r + (int64_t)c * d.N] : T(0);
+        ws[r][c] = r < kbj ? W[kj + r + (int64_t)c * d.N] : T(0);
       }
       __syncthreads();
-      // thread (cl, q): column k + cl of the block, rows kj + 16 q .. +16; the
+      const T* DjT = Dv + dinv_off[f] + (int64_t)j * 2 * SB * SB + SB * SB;
+      for (int idx = tid; idx < SB * nrhs; idx += SCT) {
+        const int r = idx % SB, c = idx / SB;
+        T acc = T(0);
+        for (int q = r; q < kbj; q++) acc = fma(DjT[r + q * SB], ws[q][c], acc);
+        xj[r][c] = r < kbj ? acc : T(0);
+      }
+      __syncthreads();
+      if (cb == 0)
+        for (int idx = tid; idx < kbj * nrhs; idx += SCT) {
+          const int r = idx % kbj, c = idx / kbj;
+          Y[kj + r + (int64_t)c * d.N] = xj[r][c];
+        }
+      if (j == 0) continue;
+      // thread (cl, q): column k + cl of block cb, rows kj + 16 q .. +16; the
       // four row quarters of a column sit in adjacent lanes
       const int cl = tid >> 2, q = tid & 3, col = k + cl;
       T acc[NR];
@@ -425,21 +375,17 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_bwd(const int* __restrict__ 
 #pragma unroll
         for (int c = 0; c < NR; c++)
           if (c < nrhs) W[col + (int64_t)c * d.N] -= acc[c];
-      if (cb == j - 1) {
-        __syncthreads();
-        diag_upper_solve<T, NR>(A, d.ld, W, d.N, k, SB, nrhs, Ls, xs);
-      }
     }
     grid_barrier(gbar, gtarget, err);
   }
   for (int i = 0; i < nf; i++) {
     const int f = flist[i];
     const FrontDev d = fr[f];
-    const T* W = Wb + woff[f] * nrhs;
+    const T* Y = Wb + woff[f] * nrhs + (int64_t)d.N * nrhs;
     const int* dl = dofs + d.dof_off;
     for (int64_t idx = (int64_t)blockIdx.x * SCT + tid; idx < (int64_t)d.n * nrhs; idx += gstride) {
       const int r = (int)(idx % d.n), c = (int)(idx / d.n);
-      X[dl[r] + (int64_t)c * ldx] = W[r + (int64_t)c * d.N];
+      X[dl[r] + (int64_t)c * ldx] = Y[r + (int64_t)c * d.N];
     }
   }
 }
@@ -458,7 +404,8 @@ int coopGrid(K kern) {
 template <class T, int NR>
 cudaError_t launchCoopSolve(bool fwd, const int* flist, int nf, int maxn, const FrontDev* fr,
                             const T* F, const int* dofs, T* X, int64_t ldx, int nrhs, T* W,
-                            const int64_t* woff, unsigned* gbar, DevError* err, cudaStream_t st) {
+                            const int64_t* woff, const T* Dv, const int64_t* dinv_off,
+                            unsigned* gbar, DevError* err, cudaStream_t st) {
   cudaError_t me = cudaMemsetAsync(gbar, 0, sizeof(unsigned), st);
   if (me != cudaSuccess) return me;
   static const int gf = coopGrid(k_solve_coop_fwd<T, NR>);   // thread-safe one-time set-up
@@ -466,7 +413,8 @@ cudaError_t launchCoopSolve(bool fwd, const int* flist, int nf, int maxn, const 
   int maxnb = cdiv(maxn, SB);
   void* args[] = {(void*)&flist, (void*)&nf,   (void*)&fr,   (void*)&F,
                   (void*)&dofs,  (void*)&X,    (void*)&ldx,  (void*)&nrhs,
-                  (void*)&W,     (void*)&woff, (void*)&maxnb, (void*)&gbar, (void*)&err};
+                  (void*)&W,     (void*)&woff, (void*)&maxnb, (void*)&Dv,
+                  (void*)&dinv_off, (void*)&gbar, (void*)&err};
   g_launches++;
   if (fwd)
     return cudaLaunchCooperativeKernel((const void*)k_solve_coop_fwd<T, NR>, dim3(gf), dim3(SCT),
@@ -482,24 +430,43 @@ int solve_coop_max_fronts() { return kMaxSolveCoopFronts; }
 template <class T>
 cudaError_t launch_solve_coop(bool forward, const int* flist, int nf, int maxn, const FrontDev* fr,
                               const T* F, const int* dofs, T* X, int64_t ldx, int nrhs, T* W,
-                              const int64_t* woff, unsigned* gbar, DevError* err, cudaStream_t st) {
+                              const int64_t* woff, const T* Dv, const int64_t* dinv_off,
+                              unsigned* gbar, DevError* err, cudaStream_t st) {
   if (nf <= 0) return cudaSuccess;
   if (nf > kMaxSolveCoopFronts || nrhs > 16) return cudaErrorInvalidValue;
   if (nrhs == 1)
-    return launchCoopSolve<T, 1>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, gbar, err, st);
+    return launchCoopSolve<T, 1>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, Dv, dinv_off, gbar, err, st);
   if (nrhs <= 4)
-    return launchCoopSolve<T, 4>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, gbar, err, st);
+    return launchCoopSolve<T, 4>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, Dv, dinv_off, gbar, err, st);
   if (nrhs <= 8)
-    return launchCoopSolve<T, 8>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, gbar, err, st);
-  return launchCoopSolve<T, 16>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, gbar, err, st);
+    return launchCoopSolve<T, 8>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, Dv, dinv_off, gbar, err, st);
+  return launchCoopSolve<T, 16>(forward, flist, nf, maxn, fr, F, dofs, X, ldx, nrhs, W, woff, Dv, dinv_off, gbar, err, st);
+}
+
+template <class T>
+void launch_diag_inv(const int* flist, int nf, int maxn, const FrontDev* fr, const T* F, T* Dv,
+                     const int64_t* dinv_off, cudaStream_t st) {
+  if (nf <= 0 || maxn <= 0) return;
+  const int sm = 2 * SB * (SB + 1) * (int)sizeof(T);
+  static const bool attr = (cudaFuncSetAttribute(k_diag_inv<T>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, sm),
+                            true);
+  (void)attr;
+  k_diag_inv<T><<<dim3(cdiv(maxn, SB), nf), SB, sm, st>>>(flist, fr, F, Dv, dinv_off);
+  g_launches++;
 }
 
 template cudaError_t launch_solve_coop<double>(bool, const int*, int, int, const FrontDev*,
                                                const double*, const int*, double*, int64_t, int,
-                                               double*, const int64_t*, unsigned*, DevError*,
-                                               cudaStream_t);
+                                               double*, const int64_t*, const double*,
+                                               const int64_t*, unsigned*, DevError*, cudaStream_t);
 template cudaError_t launch_solve_coop<float>(bool, const int*, int, int, const FrontDev*,
                                               const float*, const int*, float*, int64_t, int, float*,
-                                              const int64_t*, unsigned*, DevError*, cudaStream_t);
+                                              const int64_t*, const float*, const int64_t*,
+                                              unsigned*, DevError*, cudaStream_t);
+template void launch_diag_inv<double>(const int*, int, int, const FrontDev*, const double*, double*,
+                                      const int64_t*, cudaStream_t);
+template void launch_diag_inv<float>(const int*, int, int, const FrontDev*, const float*, float*,
+                                     const int64_t*, cudaStream_t);
 
 }  // namespace mfgpu

@@ -243,6 +243,9 @@ struct mfgpu_handle {
   DevError* d_err = nullptr;
   void* d_slots = nullptr;     // diagonal-block hand-off slots of the cooperative kernel
   unsigned* d_gbar = nullptr;  // grid-barrier arrival counter of the cooperative kernels
+  void* d_Dinv = nullptr;      // inverses of the cooperative-sweep levels' 64 x 64 pivot blocks
+  int64_t* d_dinv_off = nullptr;   // per front: element offset in d_Dinv, -1 outside those levels
+  int64_t dinvElems = 0;
   // solve workspaces (d_Wd / d_Td hold elements of the factor's precision)
   double* d_Wd = nullptr;
   size_t capW = 0;
@@ -309,7 +312,9 @@ struct mfgpu_handle {
       cudaFree(d_chunkrow);
       cudaFree(d_segchunk);
       cudaFree(d_all);
+      cudaFree(d_dinv_off);
     }
+    cudaFree(d_Dinv);
     cudaFree(d_val);
     cudaFree(d_fr);
     cudaFree(d_err);
@@ -457,6 +462,11 @@ struct mfgpu_handle {
         if (sizeof(T) != sizeof(double))
           throw CudaError("no single-precision path for this level", MFGPU_ERR_ARG);
         runStepped(P, L);
+      }
+      if (L.nf > 0 && coopSweep(ell)) {   // block inverses for the cooperative sweeps
+        mfgpu::launch_diag_inv<T>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, F, (T*)d_Dinv,
+                                  d_dinv_off, stream);
+        ck(cudaGetLastError(), "launch diagonal-block inverses (k_diag_inv)");
       }
       runGroup<T>(P, L.sadd0, groupBytes(P, L.sadd0));
       runGroup<T>(P, L.sadd1, groupBytes(P, L.sadd1));
@@ -642,7 +652,7 @@ struct mfgpu_handle {
     const int nf = s.lv[ell].nbox;
     if (coopSweep(ell)) {
       ck(mfgpu::launch_solve_coop<T>(forward, fl, nf, lvMaxn[ell], d_fr, F, d_dofs, X, ldx, nrhs, W,
-                                     d_woff, d_gbar, d_err, stream),
+                                     d_woff, (const T*)d_Dinv, d_dinv_off, d_gbar, d_err, stream),
          forward ? "launch cooperative forward sweep (k_solve_coop_fwd)"
                  : "launch cooperative backward sweep (k_solve_coop_bwd)");
     } else if (forward) {
@@ -1055,6 +1065,21 @@ int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const
     for (const mfgpu::Front& f : s.fronts) {
       H.lvMaxN[f.level] = std::max(H.lvMaxN[f.level], f.N);
       H.lvMaxn[f.level] = std::max(H.lvMaxn[f.level], f.n);
+    }
+    {
+      std::vector<int64_t> doff(s.fronts.size(), -1);
+      int64_t cur = 0;
+      const int B = mfgpu::kDinvBlock;
+      for (size_t i = 0; i < s.fronts.size(); i++)
+        if (H.coopSweep(s.fronts[i].level)) {
+          doff[i] = cur;
+          cur += (int64_t)((s.fronts[i].n + B - 1) / B) * 2 * B * B;
+        }
+      H.dinvElems = cur;
+      H.d_Dinv = dalloc<unsigned char>(std::max<int64_t>(cur, 1) * H.esz, "alloc block inverses");
+      H.d_dinv_off = dalloc<int64_t>(doff.size(), "alloc block inverse offsets");
+      ck(cudaMemcpy(H.d_dinv_off, doff.data(), doff.size() * sizeof(int64_t),
+                    cudaMemcpyHostToDevice), "upload block inverse offsets");
     }
     std::vector<SepDev> sp(s.seps.size());
     for (size_t i = 0; i < s.seps.size(); i++) {
@@ -1827,6 +1852,10 @@ struct mfgpu_server {
           t.src_off = move(t.src_arena, t.src_off);
       }
       V.upd.upload(V.stream);
+      // block inverses: the base's, then the dirty fronts' own
+      if (V.dinvElems > 0)
+        ck(cudaMemcpyAsync(V.d_Dinv, base->d_Dinv, V.dinvElems * V.esz, cudaMemcpyDeviceToDevice,
+                           V.stream), "copy block inverses");
       // refactor the private root paths, then solve
       V.factorWith(nullptr, true, V.upd, false);
       V.checkDevError();
@@ -1897,6 +1926,9 @@ std::unique_ptr<mfgpu_handle> makeView(mfgpu_handle& B) {
   H.d_err = dalloc<DevError>(1, "alloc error word");
   H.d_slots = dalloc<unsigned char>(mfgpu::coop_slot_elems() * H.esz, "alloc diagonal slots");
   H.d_gbar = dalloc<unsigned>(1, "alloc grid barrier");
+  H.dinvElems = B.dinvElems;
+  H.d_dinv_off = B.d_dinv_off;
+  H.d_Dinv = dalloc<unsigned char>(std::max<int64_t>(B.dinvElems, 1) * H.esz, "alloc block inverses");
   if (H.mixed) {
     H.d_sc = dalloc<double>(80 * (size_t)H.nseg, "alloc refinement scalars");
     H.d_active = dalloc<int>(16 * (size_t)H.nseg, "alloc refinement flags");
