@@ -137,6 +137,8 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_fwd(const int* __restrict__ 
   __shared__ int wt[SCT / 32];
   __shared__ T ws[SB][NR + 1];
   __shared__ T ys[SB][NR + 1];
+  extern __shared__ __align__(16) unsigned char dsm[];
+  T* Ds = reinterpret_cast<T*>(dsm);   // the step's block inverse, SB x SB
   const int tid = threadIdx.x;
   const int64_t gstride = (int64_t)gridDim.x * SCT;
   // gather: pivot rows from X, boundary rows zero
@@ -177,10 +179,12 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_fwd(const int* __restrict__ 
       }
       __syncthreads();
       const T* Dj = Dv + dinv_off[f] + (int64_t)j * 2 * SB * SB;
+      for (int idx = tid; idx < SB * SB; idx += SCT) Ds[idx] = Dj[idx];   // one coalesced pass
+      __syncthreads();
       for (int idx = tid; idx < SB * nrhs; idx += SCT) {
         const int t = idx % SB, c = idx / SB;
         T acc = T(0);
-        for (int q = 0; q <= t && q < kb; q++) acc = fma(Dj[t + q * SB], ws[q][c], acc);
+        for (int q = 0; q <= t && q < kb; q++) acc = fma(Ds[t + q * SB], ws[q][c], acc);
         ys[t][c] = t < kb ? acc : T(0);
       }
       __syncthreads();
@@ -249,6 +253,8 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_bwd(const int* __restrict__ 
   __shared__ int wt[SCT / 32];
   __shared__ T ws[SB][NR + 1];
   __shared__ T xj[SB][NR + 1];
+  extern __shared__ __align__(16) unsigned char dsm[];
+  T* Ds = reinterpret_cast<T*>(dsm);   // the step's block inverse (transposed), SB x SB
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t gstride = (int64_t)gridDim.x * SCT;
   for (int i = 0; i < nf; i++) {
@@ -337,10 +343,12 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_bwd(const int* __restrict__ 
       }
       __syncthreads();
       const T* DjT = Dv + dinv_off[f] + (int64_t)j * 2 * SB * SB + SB * SB;
+      for (int idx = tid; idx < SB * SB; idx += SCT) Ds[idx] = DjT[idx];  // one coalesced pass
+      __syncthreads();
       for (int idx = tid; idx < SB * nrhs; idx += SCT) {
         const int r = idx % SB, c = idx / SB;
         T acc = T(0);
-        for (int q = r; q < kbj; q++) acc = fma(DjT[r + q * SB], ws[q][c], acc);
+        for (int q = r; q < kbj; q++) acc = fma(Ds[r + q * SB], ws[q][c], acc);
         xj[r][c] = r < kbj ? acc : T(0);
       }
       __syncthreads();
@@ -393,11 +401,12 @@ __global__ void __launch_bounds__(SCT) k_solve_coop_bwd(const int* __restrict__ 
 // One CTA per SM: a step's work (at most a few hundred row or column blocks)
 // needs no more, and a smaller grid makes each grid barrier cheaper.
 template <class K>
-int coopGrid(K kern) {
+int coopGrid(K kern, int dyn) {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, SCT, 0);
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, SCT, dyn);
   return per > 0 ? sms : 1;
 }
 
@@ -408,8 +417,9 @@ cudaError_t launchCoopSolve(bool fwd, const int* flist, int nf, int maxn, const 
                             unsigned* gbar, DevError* err, cudaStream_t st) {
   cudaError_t me = cudaMemsetAsync(gbar, 0, sizeof(unsigned), st);
   if (me != cudaSuccess) return me;
-  static const int gf = coopGrid(k_solve_coop_fwd<T, NR>);   // thread-safe one-time set-up
-  static const int gb = coopGrid(k_solve_coop_bwd<T, NR>);
+  const int dyn = SB * SB * (int)sizeof(T);
+  static const int gf = coopGrid(k_solve_coop_fwd<T, NR>, dyn);   // thread-safe one-time set-up
+  static const int gb = coopGrid(k_solve_coop_bwd<T, NR>, dyn);
   int maxnb = cdiv(maxn, SB);
   void* args[] = {(void*)&flist, (void*)&nf,   (void*)&fr,   (void*)&F,
                   (void*)&dofs,  (void*)&X,    (void*)&ldx,  (void*)&nrhs,
@@ -418,9 +428,9 @@ cudaError_t launchCoopSolve(bool fwd, const int* flist, int nf, int maxn, const 
   g_launches++;
   if (fwd)
     return cudaLaunchCooperativeKernel((const void*)k_solve_coop_fwd<T, NR>, dim3(gf), dim3(SCT),
-                                       args, 0, st);
+                                       args, dyn, st);
   return cudaLaunchCooperativeKernel((const void*)k_solve_coop_bwd<T, NR>, dim3(gb), dim3(SCT), args,
-                                     0, st);
+                                     dyn, st);
 }
 
 }  // namespace
