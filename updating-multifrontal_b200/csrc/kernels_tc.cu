@@ -157,40 +157,6 @@ __device__ __forceinline__ void tri_ij(int t, int& I, int& J) {
   J = t - I * (I + 1) / 2;
 }
 
-// Rows [r0, r0+128) x columns [kc, kc+32) of the front (zero outside rows < N
-// and columns < kend) into the hi / lo operand images.  Thread t owns row t.
-template <int SPLIT>
-__device__ __forceinline__ void load_split(const float* __restrict__ A, int64_t ld, int N, int r0,
-                                           int kc, int kend, unsigned char* hi, unsigned char* lo,
-                                           int t) {
-  const int row = r0 + t;
-  const int sw = t & 7;
-#pragma unroll
-  for (int h = 0; h < TK; h += 16) {   // two halves of 16 columns: fewer live registers
-    float x[16];
-#pragma unroll
-    for (int j = 0; j < 16; j++)
-      x[j] = (row < N && kc + h + j < kend) ? __ldg(A + row + (int64_t)(kc + h + j) * ld) : 0.0f;
-#pragma unroll
-    for (int g4 = 0; g4 < 4; g4++) {
-      const int g = h / 4 + g4;
-      float4 hv, lv;
-      float* hp = &hv.x;
-      float* lp = &lv.x;
-#pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const float v = x[4 * g4 + e];
-        const float vh = tf32_round(v);
-        hp[e] = vh;
-        if (SPLIT == 3) lp[e] = tf32_round(v - vh);
-      }
-      const int off = t * 128 + ((g ^ sw) << 4);
-      *reinterpret_cast<float4*>(hi + off) = hv;
-      if (SPLIT == 3) *reinterpret_cast<float4*>(lo + off) = lv;
-    }
-  }
-}
-
 // Tile t of the launch: front slot lo, block row I >= block column J.
 struct TileInfo {
   float* A;
@@ -228,6 +194,108 @@ __device__ __forceinline__ void c_load(const float* p, int64_t ld, int row, int 
 #pragma unroll
   for (int j = 0; j < 16; j++)
     c[j] = (cb + j < N && row >= cb + j) ? p[(int64_t)j * ld] : 0.0f;
+}
+
+// One part of a loader's work: 16 panel columns of one row for one operand
+// image of one chunk.
+struct LPart {
+  const float* row_ptr;   // the front's element (row, 0)
+  int64_t ld;
+  int kc, kend;           // first column of the part, end of the panel
+  bool row_ok;            // row < N
+  int img, h;             // 0 = tile rows (A), 1 = tile columns (B); half of the chunk
+  bool first, last;       // first / last part of its chunk
+  uint32_t use;           // how many times the loader's stage was filled before
+  __device__ __forceinline__ void load(float (&x)[16]) const {
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      const int col = kc + j;
+      x[j] = (row_ok && col < kend) ? __ldg(row_ptr + (int64_t)col * ld) : 0.0f;
+    }
+  }
+};
+
+// The parts of loader group q, in order: the chunks g = q, q + NLOAD, ... of
+// the CTA's tiles, each 2 or 4 parts.
+struct LoaderIter {
+  const int* pre;
+  int nf;
+  const int* flist;
+  const FrontDev* fr;
+  float* F;
+  int K, total, q, t;
+  int tile;
+  bool have_ti = false;
+  TileInfo ti;
+  int c = 0, p = 0;
+  uint32_t g = 0;
+  __device__ LoaderIter(const int* pre_, int nf_, const int* flist_, const FrontDev* fr_, float* F_,
+                        int K_, int total_, int q_, int t_)
+      : pre(pre_), nf(nf_), flist(flist_), fr(fr_), F(F_), K(K_), total(total_), q(q_), t(t_),
+        tile(blockIdx.x) {}
+  __device__ bool next(LPart& o) {
+    while (true) {
+      if (tile >= total) return false;
+      if (!have_ti) {
+        ti = tile_info(pre, nf, flist, fr, F, K, tile);
+        have_ti = true;
+        c = 0;
+        p = 0;
+      }
+      if (c >= ti.nch) {
+        tile += gridDim.x;
+        have_ti = false;
+        continue;
+      }
+      const int nparts = ti.diag ? 2 : 4;
+      if ((int)(g % NLOAD) != q || p >= nparts) {
+        c++;
+        g++;
+        p = 0;
+        continue;
+      }
+      o.img = p >> 1;
+      o.h = p & 1;
+      const int row = (o.img ? ti.c0 : ti.r0) + t;
+      o.row_ok = row < ti.N;
+      o.row_ptr = ti.A + row;
+      o.ld = ti.ld;
+      o.kc = K + c * TK + o.h * 16;
+      o.kend = ti.k1;
+      o.first = p == 0;
+      o.last = p == nparts - 1;
+      o.use = g / NSTAGE;
+      p++;
+      return true;
+    }
+  }
+};
+
+// Split 16 values of row t into the hi / lo images of operand `img`, columns
+// 16 h .. 16 h + 15 of the chunk.
+template <int SPLIT>
+__device__ __forceinline__ void store_part(const float (&x)[16], unsigned char* st, int img, int h,
+                                           int t) {
+  unsigned char* hi = st + img * 2 * IMG;
+  unsigned char* lo = hi + IMG;
+  const int sw = t & 7;
+#pragma unroll
+  for (int g4 = 0; g4 < 4; g4++) {
+    const int gch = h * 4 + g4;
+    float4 hv, lv;
+    float* hp = &hv.x;
+    float* lp = &lv.x;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const float v = x[4 * g4 + e];
+      const float vh = tf32_round(v);
+      hp[e] = vh;
+      if (SPLIT == 3) lp[e] = tf32_round(v - vh);
+    }
+    const int off = t * 128 + ((gch ^ sw) << 4);
+    *reinterpret_cast<float4*>(hi + off) = hv;
+    if (SPLIT == 3) *reinterpret_cast<float4*>(lo + off) = lv;
+  }
 }
 
 template <int SPLIT>
@@ -283,19 +351,26 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
   const int total = pre[nf];
 
   if (warp < MMA_WARP) {
-    // ---- loaders: group q fills stage q with chunks g = q, q + 3, ... ----
+    // ---- loaders: group q fills stage q with chunks g = q, q + 3, ...; each
+    // chunk is 2 (diagonal tile) or 4 parts of 16 columns; the next part's
+    // global loads are issued before the current part is converted and before
+    // its stage is known to be free, so a thread always has loads in flight ----
     const int q = warp >> 2, t = tid & 127;
     unsigned char* st = sm + q * STAGE_BYTES;
-    uint32_t g = 0;
-    for (int tile = blockIdx.x; tile < total && !abort_flag; tile += gridDim.x) {
-      const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, tile);
-      for (int c = 0; c < ti.nch; c++, g++) {
-        if ((int)(g % NLOAD) != q) continue;
-        const uint32_t use = g / NSTAGE;
-        if (use >= 1 && !mbar_wait(&empty[q], (use - 1) & 1, &abort_flag)) break;
-        const int kc = K + c * TK;
-        load_split<SPLIT>(ti.A, ti.ld, ti.N, ti.r0, kc, ti.k1, st, st + IMG, t);
-        if (!ti.diag) load_split<SPLIT>(ti.A, ti.ld, ti.N, ti.c0, kc, ti.k1, st + 2 * IMG, st + 3 * IMG, t);
+    LoaderIter it(pre, nf, flist, fr, F, K, total, q, t);
+    float cur[16], nxt[16];
+    LPart pc, pn;
+    bool have = it.next(pn);
+    if (have) pn.load(nxt);
+    while (have && !abort_flag) {
+      pc = pn;
+#pragma unroll
+      for (int j = 0; j < 16; j++) cur[j] = nxt[j];
+      have = it.next(pn);
+      if (have) pn.load(nxt);
+      if (pc.first && pc.use >= 1 && !mbar_wait(&empty[q], (pc.use - 1) & 1, &abort_flag)) break;
+      store_part<SPLIT>(cur, st, pc.img, pc.h, t);
+      if (pc.last) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_arrive(&full[q]);
       }
