@@ -578,7 +578,7 @@ __global__ void __launch_bounds__(128) k_syrk(const int* __restrict__ flist,
 // Phases are separated by grid-wide barriers; work items (row blocks, 64 x 64
 // tiles) of all fronts of the level are spread over all CTAs.
 // ---------------------------------------------------------------------------
-constexpr int kOuter = 256;
+constexpr int kOuter = 512;
 constexpr int kCT = 128;           // threads per CTA of the cooperative kernel
 constexpr int kMaxCoopFronts = 8192;
 

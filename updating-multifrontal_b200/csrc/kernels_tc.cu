@@ -1,7 +1,7 @@
 // Tensor-core trailing update of the mixed-precision factorization (sm_100a).
 //
-// After an outer panel of 256 pivot columns [K, k1) of a front has been
-// factored (k1 = min(K + 256, n)), the rest of the front is updated by
+// After an outer panel of 512 pivot columns [K, k1) of a front has been
+// factored (k1 = min(K + 512, n)), the rest of the front is updated by
 //     C(k1:N, k1:N) -= P P^T,   P = L(k1:N, K:k1)
 // (lower triangle only), the right-looking Cholesky step that the reference's
 // dense LU performs inside Factor() (src/DE/mf2d.cpp:792-901, via
@@ -54,7 +54,7 @@ constexpr int IMG = TM * TK * 4;           // one operand image, 16 KB
 constexpr int STAGE_BYTES = 4 * IMG;       // a_hi, a_lo, b_hi, b_lo
 constexpr int kTcSmem = NSTAGE * STAGE_BYTES + 1024;   // + alignment slack
 constexpr int kMaxTcFronts = 1024;
-constexpr int kTcOuter = 256;              // outer panel width (the cooperative kernel's)
+constexpr int kTcOuter = 512;              // outer panel width (the cooperative kernel's)
 constexpr uint32_t kSpinLimit = 1u << 24;
 
 // Instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = 128.
