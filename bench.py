@@ -295,7 +295,8 @@ def update_flops(w, mod):
     return S.dirty(mod)[1]
 
 
-METRIC = "factor+update+solve TFLOP/s (Cholesky-form algorithmic flops), FP64 on 1 B200"
+METRIC = ("factor+update+solve TFLOP/s (Cholesky-form algorithmic flops) on 1 B200; "
+          "mixed vs FP64 in precision_comparison")
 
 
 def config_of(w, args):
@@ -618,6 +619,8 @@ def main():
     ap.add_argument("--workload", default="2d-1023", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip timing the other precision for the mixed-vs-FP64 comparison")
     ap.add_argument("--json-out", default=None)
     ap.add_argument("--rate", type=float, default=4.0, help="serving: arrivals per second")
     ap.add_argument("--requests", type=int, default=24, help="serving: requests in the stream")
@@ -749,6 +752,50 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = work.cpu_baseline(os.cpu_count() or 1)
 
+    # the metric compares mixed precision with FP64: time the other precision
+    # on the same workload (after releasing this handle's memory)
+    comparison = None
+    if not args.no_compare and world == 1:
+        work.F.close()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        other = MFGPU_FP64 if prec == MFGPU_MIXED else MFGPU_MIXED
+        w2 = (BatchWork if w.get("batch") else SingleWork)(w, rank, local, other)
+        st2 = torch.cuda.Stream()
+        w2.F.set_stream(st2.cuda_stream)
+        w2.to_device(torch)
+        for _ in range(max(3, args.warmup)):
+            w2.step()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(st2):
+            c0 = torch.cuda.Event(enable_timing=True)
+            c1 = torch.cuda.Event(enable_timing=True)
+            ms2 = []
+            c0.record(st2)
+            for _ in range(args.steps):
+                a0 = torch.cuda.Event(enable_timing=True)
+                a1 = torch.cuda.Event(enable_timing=True)
+                a0.record(st2)
+                w2.step()
+                a1.record(st2)
+                ms2.append((a0, a1))
+            c1.record(st2)
+        st2.synchronize()
+        steps2 = [a.elapsed_time(b) for a, b in ms2]
+        this = {"ms_per_step": ms_max / args.steps, "step_ms_p50": statistics.median(step_ms),
+                "step_ms_p99": float(np.percentile(step_ms, 99)), "resid": resid,
+                "value": value}
+        that = {"ms_per_step": c0.elapsed_time(c1) / args.steps,
+                "step_ms_p50": statistics.median(steps2),
+                "step_ms_p99": float(np.percentile(steps2, 99)), "resid": w2.resid(),
+                "value": step_fl * args.steps / (c0.elapsed_time(c1) * 1e-3) / 1e12}
+        mixed_, fp64_ = (this, that) if prec == MFGPU_MIXED else (that, this)
+        comparison = {"fp64": fp64_, "mixed": mixed_,
+                      "mixed_speedup": fp64_["ms_per_step"] / mixed_["ms_per_step"],
+                      "note": "same workload and step; device time (CUDA events); residuals "
+                              "of the updated system in FP64"}
+        w2.F.close()
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
@@ -769,6 +816,7 @@ def main():
             "gpu_launches": launches,
             "roofline": roof,
             "cpu_baseline": cpu,
+            "precision_comparison": comparison,
         }
         s = json.dumps(line)
         print(s)
