@@ -754,6 +754,9 @@ def main():
 
     # the metric compares mixed precision with FP64: time the other precision
     # on the same workload (after releasing this handle's memory)
+    config = work.config(args)
+    flops_bd = work.flops_breakdown()
+    iters = F.stats()["iterations"] if args.precision == "mixed" else 0
     comparison = None
     if not args.no_compare and world == 1:
         work.F.close()
@@ -803,12 +806,12 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32 factor + f64 refinement",
             "data": "synthetic (seeded coefficients and right-hand sides)",
-            "config": work.config(args),
+            "config": config,
             "step_ms_p50": statistics.median(step_ms),
             "step_ms_p99": float(np.percentile(step_ms, 99)),
             "resid": resid,
-            "refine_iterations": F.stats()["iterations"] if args.precision == "mixed" else 0,
-            "flops_per_step": work.flops_breakdown(),
+            "refine_iterations": iters,
+            "flops_per_step": flops_bd,
             "kernel_classes": {k: {"launches": v["launches"], "ms": v["ms"]} for k, v in prof.items()},
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
