@@ -116,11 +116,19 @@ int coop_phases(int K, int maxn);   // phases of outer panel K in the prefix tab
 // Tensor-core (tcgen05, TF32) trailing update of the mixed path after outer
 // panel K of every front in flist: C(k1:N, k1:N) -= P P^T with P the panel's
 // columns, split = 1 (TF32) or 3 (hi/lo three-term TF32, about FP32 accuracy).
+// launch_tc_pack first writes P, split into TF32 hi / lo tensor-core images,
+// into `pack` (tc_pack_bytes(nf, cap) bytes, cap = tc_pack_cap(n, N, K));
+// launch_trail_tc then reads P only from there.
 int tc_outer();
 int tc_max_fronts();
 int64_t tc_tiles(const std::vector<int>& n, const std::vector<int>& N, int K);
+int tc_pack_cap(const std::vector<int>& n, const std::vector<int>& N, int K);
+size_t tc_pack_bytes(int nf, int cap);
+cudaError_t launch_tc_pack(const int* flist, int nf, int cap, const FrontDev* fr, const float* F,
+                           int K, int split, void* pack, cudaStream_t st);
 cudaError_t launch_trail_tc(const int* flist, int nf, int64_t ntiles, const FrontDev* fr, float* F,
-                            int K, int split, DevError* err, cudaStream_t st);
+                            int K, int split, int cap, const void* pack, DevError* err,
+                            cudaStream_t st);
 
 // Cooperative sweeps over all fronts of one level (at most
 // solve_coop_max_fronts() fronts, nrhs <= 16): forward = gather, L11 solve

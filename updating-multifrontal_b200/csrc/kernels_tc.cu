@@ -8,28 +8,36 @@
 // LinAlg::Dense::LU).  For the large fronts of the top tree levels this is
 // nearly all of the work.
 //
-// Each CTA is a persistent, warp-specialised pipeline over 128 x 128 tiles of
-// C (lower triangle only):
-//   * three loader warpgroups take the 32-column panel chunks in turn: each
-//     reads 128 rows x 32 columns of the panel for the tile's rows (and, off
-//     the diagonal, for its columns), splits them into TF32 "hi" and "lo"
-//     parts (x = hi + lo, both exactly representable after rounding) and
-//     writes them to its own shared-memory stage in the K-major 128-byte
-//     swizzled layout the tensor core reads;
-//   * one MMA warp issues tcgen05.mma (kind::tf32, M = N = 128, K = 8) from an
-//     elected lane into one of two tensor-memory accumulators:
-//         SPLIT = 3:  acc += hi_a hi_b^T + hi_a lo_b^T + lo_a hi_b^T
-//         SPLIT = 1:  acc += hi_a hi_b^T
-//     and hands stages back to the loaders with tcgen05.commit;
-//   * four epilogue warps read the other accumulator with tcgen05.ld and
-//     subtract it from C in place, with the next columns' loads of C in
-//     flight while the current ones are stored.
+// Two kernels per outer panel:
+//   * k_tc_pack writes the panel once, split into TF32 "hi" and "lo" parts
+//     (x = hi + lo, both exactly representable), as 16 KB images of 128 rows x
+//     32 columns in the K-major 128-byte-swizzled layout the tensor core
+//     reads: one CTA per (128-row block, 32-column chunk) reads its block
+//     coalesced from the column-major front, splits it in shared memory and
+//     writes the hi / lo image pair out contiguously;
+//   * k_trail_tc, a persistent warp-specialised pipeline over 128 x 128 tiles
+//     of C (lower triangle only):
+//       - one producer thread brings the image pairs of each chunk (the
+//         tile's row block and, off the diagonal, its column block) into a
+//         ring of three shared-memory stages with bulk asynchronous copies
+//         (cp.async.bulk, completion counted in bytes on an mbarrier);
+//       - one MMA warp issues tcgen05.mma (kind::tf32, M = N = 128, K = 8)
+//         from an elected lane into one of two tensor-memory accumulators:
+//             SPLIT = 3:  acc += hi_a hi_b^T + hi_a lo_b^T + lo_a hi_b^T
+//             SPLIT = 1:  acc += hi_a hi_b^T
+//         and hands stages back to the producer with tcgen05.commit;
+//       - eight epilogue warps (two per accumulator lane quarter, 64 columns
+//         each) load their C values for a tile before its accumulator is
+//         ready, then read the accumulator with tcgen05.ld and subtract it
+//         from C in place.
+// MN-major TF32 operands would let the tensor core read the column-major
+// front directly, but they read back as zeros on sm_100a, hence the pack.
 // The three-term form keeps products to about 2^-21 relative error, close to
 // FP32.
 //
 // Every mbarrier wait is bounded; on expiry (or once another warp gave up) the
 // kernel records error code 2 in the error word, skips the remaining work,
-// releases its tensor memory and returns.
+// waits for its own copies in flight, releases its tensor memory and returns.
 #include <atomic>
 #include <cstdint>
 
@@ -43,23 +51,45 @@ namespace {
 
 constexpr int TM = 128;                    // C tile rows = accumulator lanes
 constexpr int TN = 128;                    // C tile columns = accumulator columns
-constexpr int TK = 32;                     // panel columns per stage (128-byte rows)
-constexpr int NLOAD = 3;                   // loader warpgroups = shared-memory stages
-constexpr int NSTAGE = NLOAD;
+constexpr int TK = 32;                     // panel columns per chunk
+constexpr int NSTAGE = 3;                  // shared-memory stages
 constexpr int NACC = 2;                    // tensor-memory accumulators
-constexpr int MMA_WARP = NLOAD * 4;        // warp 12 issues the MMAs
-constexpr int EPI_WARP0 = MMA_WARP + 1;    // warps 13..16 run the epilogue
-constexpr int TCT = (EPI_WARP0 + 4) * 32;  // 544 threads
-constexpr int IMG = TM * TK * 4;           // one operand image, 16 KB
+constexpr int MMA_WARP = 1;                // warp 0 produces, warp 1 issues the MMAs
+constexpr int EPI_WARP0 = 2;               // warps 2..9 run the epilogue
+constexpr int NEPI = 8;
+constexpr int TCT = (EPI_WARP0 + NEPI) * 32;   // 320 threads
+constexpr int IMG = TM * TK * 4;           // one image of 128 rows x 32 columns, 16 KB
 constexpr int STAGE_BYTES = 4 * IMG;       // a_hi, a_lo, b_hi, b_lo
 constexpr int kTcSmem = NSTAGE * STAGE_BYTES + 1024;   // + alignment slack
 constexpr int kMaxTcFronts = 1024;
 constexpr int kTcOuter = 512;              // outer panel width (the cooperative kernel's)
 constexpr uint32_t kSpinLimit = 1u << 24;
 
+// Image layout (K-major, 128-byte swizzle): element (m, k) of a 128 x 32
+// image sits in 128-byte row m, 16-byte chunk (k / 4) ^ (m % 8), word k % 4;
+// 8-row groups are 1024 bytes apart.
+__host__ __device__ constexpr int img_off(int m, int k) {
+  return m * 128 + ((((k >> 2) ^ (m & 7))) << 4) + (k & 3) * 4;
+}
+
 // Instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = 128.
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TN >> 3) << 17) |
                             ((uint32_t)(TM >> 4) << 24);
+
+// Panel geometry of a front for outer panel K: k1, 128-row blocks below k1,
+// 32-column chunks in [K, k1); nb = 0 when the front has no trailing update.
+struct PanelGeo {
+  int k1, nb, nch;
+};
+__host__ __device__ inline PanelGeo panel_geo(int n, int N, int K) {
+  PanelGeo g{0, 0, 0};
+  if (K >= n) return g;
+  g.k1 = n < K + kTcOuter ? n : K + kTcOuter;
+  if (N <= g.k1) return g;
+  g.nb = (N - g.k1 + TM - 1) / TM;
+  g.nch = (g.k1 - K + TK - 1) / TK;
+  return g;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -70,6 +100,27 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
          ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// Bulk asynchronous copy global -> this CTA's shared memory; completion is
+// counted in bytes on the mbarrier (addresses 16-byte aligned, size a
+// multiple of 16).
+__device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          dst),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Arrive on the mbarrier and add `bytes` to the transaction count its
+// current phase waits for.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
+                   smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
@@ -157,11 +208,11 @@ __device__ __forceinline__ void tri_ij(int t, int& I, int& J) {
   J = t - I * (I + 1) / 2;
 }
 
-// Tile t of the launch: front slot lo, block row I >= block column J.
+// Tile t of the launch: front slot i, block row I >= block column J.
 struct TileInfo {
   float* A;
   int64_t ld;
-  int N, k1, r0, c0, nch;
+  int N, k1, r0, c0, nch, slot, I, J;
   bool diag;
 };
 
@@ -174,134 +225,75 @@ __device__ __forceinline__ TileInfo tile_info(const int* pre, int nf, const int*
     else hi = mid - 1;
   }
   const FrontDev d = fr[flist[lo]];
+  const PanelGeo g = panel_geo(d.n, d.N, K);
   TileInfo t;
   t.A = F + d.off;
   t.ld = d.ld;
   t.N = d.N;
-  t.k1 = min(K + kTcOuter, d.n);
-  int I, J;
-  tri_ij(tile - pre[lo], I, J);
-  t.r0 = t.k1 + I * TM;
-  t.c0 = t.k1 + J * TN;
-  t.diag = (I == J);
-  t.nch = (t.k1 - K + TK - 1) / TK;
+  t.k1 = g.k1;
+  t.nch = g.nch;
+  t.slot = lo;
+  tri_ij(tile - pre[lo], t.I, t.J);
+  t.r0 = t.k1 + t.I * TM;
+  t.c0 = t.k1 + t.J * TN;
+  t.diag = (t.I == t.J);
   return t;
 }
 
-// 16 values of C for one row: columns cb .. cb+15 inside the lower triangle.
-__device__ __forceinline__ void c_load(const float* p, int64_t ld, int row, int cb, int N,
-                                       float (&c)[16]) {
-#pragma unroll
-  for (int j = 0; j < 16; j++)
-    c[j] = (cb + j < N && row >= cb + j) ? p[(int64_t)j * ld] : 0.0f;
-}
-
-// One part of a loader's work: 16 panel columns of one row for one operand
-// image of one chunk.
-struct LPart {
-  const float* row_ptr;   // the front's element (row, 0)
-  int64_t ld;
-  int kc, kend;           // first column of the part, end of the panel
-  bool row_ok;            // row < N
-  int img, h;             // 0 = tile rows (A), 1 = tile columns (B); half of the chunk
-  bool first, last;       // first / last part of its chunk
-  uint32_t use;           // how many times the loader's stage was filled before
-  __device__ __forceinline__ void load(float (&x)[16]) const {
-#pragma unroll
-    for (int j = 0; j < 16; j++) {
-      const int col = kc + j;
-      x[j] = (row_ok && col < kend) ? __ldg(row_ptr + (int64_t)col * ld) : 0.0f;
-    }
-  }
-};
-
-// The parts of loader group q, in order: the chunks g = q, q + NLOAD, ... of
-// the CTA's tiles, each 2 or 4 parts.
-struct LoaderIter {
-  const int* pre;
-  int nf;
-  const int* flist;
-  const FrontDev* fr;
-  float* F;
-  int K, total, q, t;
-  int tile;
-  bool have_ti = false;
-  TileInfo ti;
-  int c = 0, p = 0;
-  uint32_t g = 0;
-  __device__ LoaderIter(const int* pre_, int nf_, const int* flist_, const FrontDev* fr_, float* F_,
-                        int K_, int total_, int q_, int t_)
-      : pre(pre_), nf(nf_), flist(flist_), fr(fr_), F(F_), K(K_), total(total_), q(q_), t(t_),
-        tile(blockIdx.x) {}
-  __device__ bool next(LPart& o) {
-    while (true) {
-      if (tile >= total) return false;
-      if (!have_ti) {
-        ti = tile_info(pre, nf, flist, fr, F, K, tile);
-        have_ti = true;
-        c = 0;
-        p = 0;
-      }
-      if (c >= ti.nch) {
-        tile += gridDim.x;
-        have_ti = false;
-        continue;
-      }
-      const int nparts = ti.diag ? 2 : 4;
-      if ((int)(g % NLOAD) != q || p >= nparts) {
-        c++;
-        g++;
-        p = 0;
-        continue;
-      }
-      o.img = p >> 1;
-      o.h = p & 1;
-      const int row = (o.img ? ti.c0 : ti.r0) + t;
-      o.row_ok = row < ti.N;
-      o.row_ptr = ti.A + row;
-      o.ld = ti.ld;
-      o.kc = K + c * TK + o.h * 16;
-      o.kend = ti.k1;
-      o.first = p == 0;
-      o.last = p == nparts - 1;
-      o.use = g / NSTAGE;
-      p++;
-      return true;
-    }
-  }
-};
-
-// Split 16 values of row t into the hi / lo images of operand `img`, columns
-// 16 h .. 16 h + 15 of the chunk.
+// Pack: CTA (x, i) = image pair x = b * nch + c of front slot i, rows
+// k1 + 128 b + t (thread t), columns K + 32 c .. +31; zeros outside the front
+// and beyond k1.  Pair (i, x) starts at byte (i * cap + x) * 2 * IMG of pack:
+// hi image, then lo image (SPLIT = 3 only).
 template <int SPLIT>
-__device__ __forceinline__ void store_part(const float (&x)[16], unsigned char* st, int img, int h,
-                                           int t) {
-  unsigned char* hi = st + img * 2 * IMG;
-  unsigned char* lo = hi + IMG;
-  const int sw = t & 7;
+__global__ void __launch_bounds__(128) k_tc_pack(const int* __restrict__ flist,
+                                                 const FrontDev* __restrict__ fr,
+                                                 const float* __restrict__ F, int K, int cap,
+                                                 unsigned char* __restrict__ pack) {
+  __shared__ __align__(1024) unsigned char img[SPLIT == 3 ? 2 * IMG : IMG];
+  const FrontDev d = fr[flist[blockIdx.y]];
+  const PanelGeo g = panel_geo(d.n, d.N, K);
+  const int x = blockIdx.x;
+  if (x >= g.nb * g.nch) return;
+  const int b = x / g.nch, c = x - b * g.nch, t = threadIdx.x;
+  const int row = g.k1 + b * TM + t, kc = K + c * TK;
+  const bool row_ok = row < d.N;
+  const float* src = F + d.off + (row_ok ? row : 0) + (int64_t)kc * d.ld;
+  const int kend = g.k1 - kc;   // columns of this chunk inside the panel
 #pragma unroll
-  for (int g4 = 0; g4 < 4; g4++) {
-    const int gch = h * 4 + g4;
-    float4 hv, lv;
-    float* hp = &hv.x;
-    float* lp = &lv.x;
+  for (int q = 0; q < TK / 4; q++) {
+    float v[4];
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const float v = x[4 * g4 + e];
-      const float vh = tf32_round(v);
-      hp[e] = vh;
-      if (SPLIT == 3) lp[e] = tf32_round(v - vh);
+    for (int j = 0; j < 4; j++) {
+      const int k = 4 * q + j;
+      v[j] = (row_ok && k < kend) ? __ldg(src + (int64_t)k * d.ld) : 0.0f;
     }
-    const int off = t * 128 + ((gch ^ sw) << 4);
-    *reinterpret_cast<float4*>(hi + off) = hv;
-    if (SPLIT == 3) *reinterpret_cast<float4*>(lo + off) = lv;
+    float4 h, l;
+    h.x = tf32_round(v[0]);
+    h.y = tf32_round(v[1]);
+    h.z = tf32_round(v[2]);
+    h.w = tf32_round(v[3]);
+    *reinterpret_cast<float4*>(img + img_off(t, 4 * q)) = h;
+    if (SPLIT == 3) {
+      l.x = tf32_round(v[0] - h.x);
+      l.y = tf32_round(v[1] - h.y);
+      l.z = tf32_round(v[2] - h.z);
+      l.w = tf32_round(v[3] - h.w);
+      *reinterpret_cast<float4*>(img + IMG + img_off(t, 4 * q)) = l;
+    }
   }
+  __syncthreads();
+  float4* dst = reinterpret_cast<float4*>(pack + ((int64_t)blockIdx.y * cap + x) * 2 * IMG);
+  const float4* s4 = reinterpret_cast<const float4*>(img);
+#pragma unroll 4
+  for (int e = t; e < (SPLIT == 3 ? 2 : 1) * IMG / 16; e += 128) dst[e] = s4[e];
 }
 
 template <int SPLIT>
 __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ flist, int nf,
                                                      const FrontDev* __restrict__ fr,
-                                                     float* __restrict__ F, int K, DevError* err) {
+                                                     float* __restrict__ F, int K, int cap,
+                                                     const unsigned char* __restrict__ pack,
+                                                     DevError* err) {
   extern __shared__ unsigned char tc_raw[];
   __shared__ uint64_t full[NSTAGE], empty[NSTAGE], acc_full[NACC], acc_empty[NACC];
   __shared__ uint32_t tmem_base;
@@ -316,24 +308,17 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
     pre[0] = 0;
     for (int i = 0; i < nf; i++) {
       const FrontDev d = fr[flist[i]];
-      int t = 0;
-      if (K < d.n) {
-        const int k1 = min(K + kTcOuter, d.n);
-        if (d.N > k1) {
-          const int T = (d.N - k1 + TM - 1) / TM;
-          t = T * (T + 1) / 2;
-        }
-      }
-      acc += t;
+      const PanelGeo g = panel_geo(d.n, d.N, K);
+      acc += g.nb * (g.nb + 1) / 2;
       pre[i + 1] = acc;
     }
     for (int s = 0; s < NSTAGE; s++) {
-      mbar_init(&full[s], 128);
+      mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
     for (int b = 0; b < NACC; b++) {
       mbar_init(&acc_full[b], 1);
-      mbar_init(&acc_empty[b], 128);
+      mbar_init(&acc_empty[b], NEPI * 32);
     }
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -349,31 +334,35 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
   tc_fence_after();
   const uint32_t tmem = tmem_base;
   const int total = pre[nf];
+  constexpr uint32_t kPairBytes = SPLIT == 3 ? 2 * IMG : IMG;   // bytes copied per image pair
 
-  if (warp < MMA_WARP) {
-    // ---- loaders: group q fills stage q with chunks g = q, q + 3, ...; each
-    // chunk is 2 (diagonal tile) or 4 parts of 16 columns; the next part's
-    // global loads are issued before the current part is converted and before
-    // its stage is known to be free, so a thread always has loads in flight ----
-    const int q = warp >> 2, t = tid & 127;
-    unsigned char* st = sm + q * STAGE_BYTES;
-    LoaderIter it(pre, nf, flist, fr, F, K, total, q, t);
-    float cur[16], nxt[16];
-    LPart pc, pn;
-    bool have = it.next(pn);
-    if (have) pn.load(nxt);
-    while (have && !abort_flag) {
-      pc = pn;
-#pragma unroll
-      for (int j = 0; j < 16; j++) cur[j] = nxt[j];
-      have = it.next(pn);
-      if (have) pn.load(nxt);
-      if (pc.first && pc.use >= 1 && !mbar_wait(&empty[q], (pc.use - 1) & 1, &abort_flag)) break;
-      store_part<SPLIT>(cur, st, pc.img, pc.h, t);
-      if (pc.last) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_arrive(&full[q]);
+  if (warp == 0) {
+    // ---- producer: one thread fills the stages with the chunks' image pairs ----
+    if (lane == 0) {
+      const uint32_t sm0 = smem_u32(sm);
+      uint32_t g = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; ok && tile < total && !abort_flag; tile += gridDim.x) {
+        const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, tile);
+        const unsigned char* pa = pack + ((int64_t)ti.slot * cap + (int64_t)ti.I * ti.nch) * 2 * IMG;
+        const unsigned char* pb = pack + ((int64_t)ti.slot * cap + (int64_t)ti.J * ti.nch) * 2 * IMG;
+        for (int c = 0; c < ti.nch; c++, g++) {
+          const int s = g % NSTAGE;
+          const uint32_t u = g / NSTAGE;
+          if (u >= 1 && !mbar_wait(&empty[s], (u - 1) & 1, &abort_flag)) {
+            ok = false;
+            break;
+          }
+          const uint32_t st = sm0 + s * STAGE_BYTES;
+          mbar_expect_tx(&full[s], ti.diag ? kPairBytes : 2 * kPairBytes);
+          bulk_copy(st, pa + (int64_t)c * 2 * IMG, kPairBytes, &full[s]);
+          if (!ti.diag) bulk_copy(st + 2 * IMG, pb + (int64_t)c * 2 * IMG, kPairBytes, &full[s]);
+        }
       }
+      // the copies still in flight land before the CTA may exit
+      volatile int never = 0;
+      for (uint32_t q = g > NSTAGE ? g - NSTAGE : 0; q < g; q++)
+        mbar_wait(&full[q % NSTAGE], (q / NSTAGE) & 1, &never);
     }
   } else if (warp == MMA_WARP) {
     // ---- MMA issue ----
@@ -416,39 +405,47 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
       __syncwarp();
     }
   } else {
-    // ---- epilogue: C(tile) -= acc ----
-    const int quarter = warp & 3;   // tensor-memory lanes this warp may read
+    // ---- epilogue: C(tile) -= acc; warp w reads accumulator lanes
+    // 32 (w % 4) .. +31 (the lane quarter it may access), columns 64 h .. +63 ----
+    const int quarter = warp & 3, half = (warp - EPI_WARP0) >> 2;
     uint32_t tl = 0;
     for (int tile = blockIdx.x; tile < total && !__shfl_sync(0xffffffffu, abort_flag, 0);
          tile += gridDim.x, tl++) {
       const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, tile);
       const int b = tl % NACC;
-      const int row = ti.r0 + quarter * 32 + lane;
+      const int row = ti.r0 + quarter * 32 + lane, cb = ti.c0 + half * 64;
       const bool live = row < ti.N;
-      float* p = ti.A + row + (int64_t)ti.c0 * ti.ld;
-      float cur[16];
-      if (live) c_load(p, ti.ld, row, ti.c0, ti.N, cur);
-      if (!mbar_wait_warp(&acc_full[b], (tl / NACC) & 1, &abort_flag)) break;
-      tc_fence_after();
-      const uint32_t src = tmem + b * TN + ((uint32_t)(quarter * 32) << 16);
-#pragma unroll 1
-      for (int qb = 0; qb < TN / 16; qb++) {
-        uint32_t v[16];
-        tmem_ld16(src + qb * 16, v);
-        const int cb = ti.c0 + qb * 16;
-        float nxt[16];
-        if (live && qb + 1 < TN / 16)
-          c_load(p + (int64_t)(qb + 1) * 16 * ti.ld, ti.ld, row, cb + 16, ti.N, nxt);
-        if (live) {
+      float* p = ti.A + row + (int64_t)cb * ti.ld;
+      // entry j of the row is live when cb + j <= min(row, N - 1); the first
+      // 32 values are loaded while the tile's products are still being
+      // accumulated, the other 32 while the first are stored
+      const int jmax = live ? min(row, ti.N - 1) - cb : -1;
+      const uint32_t src = tmem + b * TN + half * 64 + ((uint32_t)(quarter * 32) << 16);
+      bool ok = true;
 #pragma unroll
-          for (int j = 0; j < 16; j++)
-            if (cb + j < ti.N && row >= cb + j)
-              p[(int64_t)(qb * 16 + j) * ti.ld] = cur[j] - __uint_as_float(v[j]);
+      for (int h2 = 0; h2 < 2; h2++) {
+        float cv[32];
+        const float* q = p + (int64_t)(32 * h2) * ti.ld;
+#pragma unroll
+        for (int j = 0; j < 32; j++, q += ti.ld) cv[j] = 32 * h2 + j <= jmax ? *q : 0.0f;
+        if (h2 == 0) {
+          if (!mbar_wait_warp(&acc_full[b], (tl / NACC) & 1, &abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
         }
-        if (qb + 1 < TN / 16)
+        float* w = p + (int64_t)(32 * h2) * ti.ld;
 #pragma unroll
-          for (int j = 0; j < 16; j++) cur[j] = nxt[j];
+        for (int qb = 0; qb < 2; qb++) {
+          uint32_t v[16];
+          tmem_ld16(src + 32 * h2 + 16 * qb, v);
+#pragma unroll
+          for (int j = 0; j < 16; j++, w += ti.ld)
+            if (32 * h2 + 16 * qb + j <= jmax) *w = cv[16 * qb + j] - __uint_as_float(v[j]);
+        }
       }
+      if (!ok) break;
       tc_fence_before();
       mbar_arrive(&acc_empty[b]);
     }
@@ -470,20 +467,26 @@ int tc_max_fronts() { return kMaxTcFronts; }
 int64_t tc_tiles(const std::vector<int>& n, const std::vector<int>& N, int K) {
   int64_t t = 0;
   for (size_t i = 0; i < n.size(); i++) {
-    if (K >= n[i]) continue;
-    const int k1 = std::min(K + kTcOuter, n[i]);
-    if (N[i] <= k1) continue;
-    const int64_t T = (N[i] - k1 + TM - 1) / TM;
-    t += T * (T + 1) / 2;
+    const PanelGeo g = panel_geo(n[i], N[i], K);
+    t += (int64_t)g.nb * (g.nb + 1) / 2;
   }
   return t;
 }
 
-cudaError_t launch_trail_tc(const int* flist, int nf, int64_t ntiles, const FrontDev* fr, float* F,
-                            int K, int split, DevError* err, cudaStream_t st) {
-  if (nf <= 0 || ntiles <= 0) return cudaSuccess;
-  if (nf > kMaxTcFronts || (split != 1 && split != 3)) return cudaErrorInvalidValue;
-  static const int sms = []() {   // thread-safe one-time set-up
+int tc_pack_cap(const std::vector<int>& n, const std::vector<int>& N, int K) {
+  int cap = 0;
+  for (size_t i = 0; i < n.size(); i++) {
+    const PanelGeo g = panel_geo(n[i], N[i], K);
+    cap = std::max(cap, g.nb * g.nch);
+  }
+  return cap;
+}
+
+size_t tc_pack_bytes(int nf, int cap) { return (size_t)nf * (size_t)cap * 2 * IMG; }
+
+namespace {
+int tc_setup() {   // thread-safe one-time set-up (static local initialisation)
+  static const int sms = []() {
     int dev = 0, n = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
@@ -491,11 +494,35 @@ cudaError_t launch_trail_tc(const int* flist, int nf, int64_t ntiles, const Fron
     cudaFuncSetAttribute(k_trail_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
     return n;
   }();
-  const int grid = (int)std::min<int64_t>(ntiles, sms);
+  return sms;
+}
+}  // namespace
+
+cudaError_t launch_tc_pack(const int* flist, int nf, int cap, const FrontDev* fr, const float* F,
+                           int K, int split, void* pack, cudaStream_t st) {
+  if (nf <= 0 || cap <= 0) return cudaSuccess;
+  if (nf > 65535 || (split != 1 && split != 3)) return cudaErrorInvalidValue;
+  const dim3 grid((unsigned)cap, (unsigned)nf);
   if (split == 3)
-    k_trail_tc<3><<<grid, TCT, kTcSmem, st>>>(flist, nf, fr, F, K, err);
+    k_tc_pack<3><<<grid, 128, 0, st>>>(flist, fr, F, K, cap, (unsigned char*)pack);
   else
-    k_trail_tc<1><<<grid, TCT, kTcSmem, st>>>(flist, nf, fr, F, K, err);
+    k_tc_pack<1><<<grid, 128, 0, st>>>(flist, fr, F, K, cap, (unsigned char*)pack);
+  g_launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_trail_tc(const int* flist, int nf, int64_t ntiles, const FrontDev* fr, float* F,
+                            int K, int split, int cap, const void* pack, DevError* err,
+                            cudaStream_t st) {
+  if (nf <= 0 || ntiles <= 0) return cudaSuccess;
+  if (nf > kMaxTcFronts || (split != 1 && split != 3) || !pack) return cudaErrorInvalidValue;
+  const int grid = (int)std::min<int64_t>(ntiles, tc_setup());
+  if (split == 3)
+    k_trail_tc<3><<<grid, TCT, kTcSmem, st>>>(flist, nf, fr, F, K, cap,
+                                              (const unsigned char*)pack, err);
+  else
+    k_trail_tc<1><<<grid, TCT, kTcSmem, st>>>(flist, nf, fr, F, K, cap,
+                                              (const unsigned char*)pack, err);
   g_launches++;
   return cudaGetLastError();
 }

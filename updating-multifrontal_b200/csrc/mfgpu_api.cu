@@ -71,6 +71,7 @@ struct Plan {
     int64_t cpref0 = 0;   // offset of the cooperative kernel's phase prefixes in cpref
     int coopItems = 0;    // largest work-item count of any cooperative phase
   };
+  size_t tcPackBytes = 0;   // largest tensor-core panel pack any level of the plan needs
   std::vector<Level> lv;
   std::vector<Task> tasks;
   std::vector<int64_t> pref;
@@ -242,6 +243,8 @@ struct mfgpu_handle {
   int64_t* d_woff = nullptr;
   DevError* d_err = nullptr;
   void* d_slots = nullptr;     // diagonal-block hand-off slots of the cooperative kernel
+  void* d_tcpack = nullptr;    // tensor-core panel images (mixed path)
+  size_t tcPackCap = 0;
   unsigned* d_gbar = nullptr;  // grid-barrier arrival counter of the cooperative kernels
   void* d_Dinv = nullptr;      // inverses of the cooperative-sweep levels' 64 x 64 pivot blocks
   int64_t* d_dinv_off = nullptr;   // per front: element offset in d_Dinv, -1 outside those levels
@@ -319,6 +322,7 @@ struct mfgpu_handle {
     cudaFree(d_fr);
     cudaFree(d_err);
     cudaFree(d_slots);
+    cudaFree(d_tcpack);
     cudaFree(d_gbar);
     cudaFree(d_Wd);
     cudaFree(d_X);
@@ -350,6 +354,7 @@ struct mfgpu_handle {
     P.cpref.clear();
     P.nfronts = 0;
     P.flops = 0;
+    P.tcPackBytes = 0;
     for (int ell = s.levels - 1; ell >= 0; ell--) {
       Plan::Level& L = P.lv[ell];
       std::vector<int> fl, sl;
@@ -392,6 +397,10 @@ struct mfgpu_handle {
         const size_t stride = fl.size() + 1;
         for (size_t q = 0; q + stride <= pp.size(); q += stride)
           L.coopItems = std::max(L.coopItems, pp[q + fl.size()]);
+        if (mixed && tcLevel(L))
+          for (int K = 0; K < L.maxn; K += mfgpu::tc_outer())
+            P.tcPackBytes = std::max(P.tcPackBytes,
+                                     mfgpu::tc_pack_bytes((int)fl.size(), mfgpu::tc_pack_cap(nn, NN, K)));
       }
     }
   }
@@ -428,6 +437,14 @@ struct mfgpu_handle {
   void runPlanT(const Plan& P) {
     const Schedule& s = *S;
     T* F = (T*)d_F;
+    if (P.tcPackBytes > tcPackCap) {   // grows once, on the first plan that needs more
+      ck(cudaStreamSynchronize(stream), "sync before growing the panel pack");
+      cudaFree(d_tcpack);
+      d_tcpack = nullptr;
+      tcPackCap = 0;
+      d_tcpack = dalloc<unsigned char>(P.tcPackBytes, "alloc tensor-core panel pack");
+      tcPackCap = P.tcPackBytes;
+    }
     ck(cudaMemsetAsync(d_err, 0, sizeof(DevError), stream), "clear error word");
     for (int ell = s.levels - 1; ell >= 0; ell--) {
       const Plan::Level& L = P.lv[ell];
@@ -517,9 +534,15 @@ struct mfgpu_handle {
             const double k1 = std::min(K + outer, nn[i]), r = NN[i] - k1;
             tc_fl += r * r * (k1 - K);
           }
+      const int cap = mfgpu::tc_pack_cap(nn, NN, K);
+      if (mfgpu::tc_pack_bytes((int)L.nf, cap) > tcPackCap)
+        throw CudaError("tensor-core panel pack larger than planned", MFGPU_ERR_STATE);
       prof.begin(MFGPU_KC_TC, stream);
-      ck(mfgpu::launch_trail_tc(P.d_ids + L.f0, (int)L.nf, nt, d_fr, (float*)d_F, K, tcSplit, d_err,
-                                stream),
+      ck(mfgpu::launch_tc_pack(P.d_ids + L.f0, (int)L.nf, cap, d_fr, (const float*)d_F, K, tcSplit,
+                               d_tcpack, stream),
+         "launch tensor-core panel pack (k_tc_pack)");
+      ck(mfgpu::launch_trail_tc(P.d_ids + L.f0, (int)L.nf, nt, d_fr, (float*)d_F, K, tcSplit, cap,
+                                d_tcpack, d_err, stream),
          "launch tensor-core trailing update (k_trail_tc)");
       prof.end(stream);
     }
