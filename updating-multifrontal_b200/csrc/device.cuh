@@ -100,35 +100,42 @@ void launch_front_small(const int* flist, int nf, int maxN, const FrontDev* fr, 
 // `phase_pref` the per-phase work-item prefixes from coop_phase_prefix.
 bool coop_fits(int nf);
 size_t coop_slot_elems();
-std::vector<int> coop_phase_prefix(const std::vector<int>& n, const std::vector<int>& N, int maxn);
+std::vector<int> coop_phase_prefix(const std::vector<int>& n, const std::vector<int>& N, int maxn,
+                                   int outer = 0);
 // max_items (> 0): the largest work-item count of any phase, to size the grid;
 // K0/K1/phase0/trailing restrict the launch to the outer panels [K0, K1)
-// (K1 < 0: to the end) and optionally leave the last trailing update out.
+// (K1 < 0: to the end) and optionally leave the last trailing update out;
+// outer (> 0) is the outer panel width, a multiple of 32 (default
+// coop_outer()), and must match the one phase_pref was built with.
 // gbar: one unsigned of device memory for the launch's grid barrier.
 template <class T>
 cudaError_t launch_level_coop(const int* flist, int nf, int maxn, const FrontDev* fr, T* F,
                               DevError* err, T* slots, const int* phase_pref, unsigned* gbar,
                               cudaStream_t st, int K0 = 0, int K1 = -1, int phase0 = 0,
-                              int trailing = 1, int max_items = 0);
-int coop_outer();                   // outer panel width of the cooperative kernel
-int coop_phases(int K, int maxn);   // phases of outer panel K in the prefix table
+                              int trailing = 1, int max_items = 0, int outer = 0);
+int coop_outer();   // default outer panel width of the cooperative kernel
+// phases of outer panel K in the prefix table built with this outer width
+int coop_phases(int K, int maxn, int outer = 0);
 
 // Tensor-core (tcgen05, TF32) trailing update of the mixed path after outer
 // panel K of every front in flist: C(k1:N, k1:N) -= P P^T with P the panel's
 // columns, split = 1 (TF32) or 3 (hi/lo three-term TF32, about FP32 accuracy).
 // launch_tc_pack first writes P, split into TF32 hi / lo tensor-core images,
-// into `pack` (tc_pack_bytes(nf, cap) bytes, cap = tc_pack_cap(n, N, K));
+// into `pack` (tc_pack_bytes(nf, cap) bytes, cap = tc_pack_cap(n, N, K, w));
 // launch_trail_tc then reads P only from there.
 int tc_outer();
 int tc_max_fronts();
-int64_t tc_tiles(const std::vector<int>& n, const std::vector<int>& N, int K);
-int tc_pack_cap(const std::vector<int>& n, const std::vector<int>& N, int K);
+// The panel is [K, K + w) (w a multiple of 32, at most tc_outer()); the
+// update covers columns below cend (cend < 0: all columns, else
+// min(cend, n) per front).
+int64_t tc_tiles(const std::vector<int>& n, const std::vector<int>& N, int K, int w, int cend);
+int tc_pack_cap(const std::vector<int>& n, const std::vector<int>& N, int K, int w);
 size_t tc_pack_bytes(int nf, int cap);
 cudaError_t launch_tc_pack(const int* flist, int nf, int cap, const FrontDev* fr, const float* F,
-                           int K, int split, void* pack, cudaStream_t st);
+                           int K, int w, int split, void* pack, cudaStream_t st);
 cudaError_t launch_trail_tc(const int* flist, int nf, int64_t ntiles, const FrontDev* fr, float* F,
-                            int K, int split, int cap, const void* pack, DevError* err,
-                            cudaStream_t st);
+                            int K, int w, int cend, int split, int cap, const void* pack,
+                            DevError* err, cudaStream_t st);
 
 // Cooperative sweeps over all fronts of one level (at most
 // solve_coop_max_fronts() fronts, nrhs <= 16): forward = gather, L11 solve

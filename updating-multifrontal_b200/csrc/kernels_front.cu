@@ -567,14 +567,15 @@ __global__ void __launch_bounds__(128) k_syrk(const int* __restrict__ flist,
 
 // ---------------------------------------------------------------------------
 // Large fronts: one cooperative persistent launch per level.  Two-level
-// blocking: outer panels of kOuter columns; inside each, 32-column steps
+// blocking: outer panels of `outer` columns (kOuter = 512 unless the caller
+// asks for narrower ones); inside each, 32-column steps
 //   A  triangular solve of the rows below the diagonal block (every work item
 //      factors the 32 x 32 diagonal block itself, from the not yet overwritten
 //      values, so no extra phase is needed),
 //   B  the diagonal block is written back and the outer panel's remaining
 //      columns are updated with the 32 new columns,
 // and after the outer panel
-//   C  the trailing matrix is updated with the whole outer panel (k = kOuter).
+//   C  the trailing matrix is updated with the whole outer panel.
 // Phases are separated by grid-wide barriers; work items (row blocks, 64 x 64
 // tiles) of all fronts of the level are spread over all CTAs.
 // ---------------------------------------------------------------------------
@@ -659,7 +660,7 @@ __device__ __forceinline__ int ceil_div(int a, int b) { return (a + b - 1) / b; 
 // phase p, pref[p * (nf + 1) + i] is the first item of front i.  Each CTA
 // copies the phase's prefix into shared memory and binary-searches it.
 //
-// One launch covers the outer panels [K0, K1) (K0 a multiple of kOuter);
+// One launch covers the outer panels [K0, K1) (K0 a multiple of outer);
 // phase0 is the index of the first phase of outer panel K0 in phase_pref.  With
 // trailing == 0 the last outer panel's phase C is left to the caller (the
 // tensor-core trailing update of the mixed path), and the next launch factors
@@ -670,7 +671,7 @@ __global__ void __launch_bounds__(kCT) k_level_coop(const int* __restrict__ flis
                                                     T* __restrict__ F, DevError* err, int maxn,
                                                     T* __restrict__ slots,
                                                     const int* __restrict__ phase_pref, int K0,
-                                                    int K1, int phase0, int trailing,
+                                                    int K1, int phase0, int trailing, int outer,
                                                     unsigned* gbar) {
   unsigned gtarget = 0;
   __shared__ T Ls[kPanel][kPanel + 1];
@@ -707,8 +708,8 @@ __global__ void __launch_bounds__(kCT) k_level_coop(const int* __restrict__ flis
                           Ls, Li, Dinv, err, f);
   }
   grid_barrier(gbar, gtarget, err);
-  for (int K = K0; K < K1 && K < maxn; K += kOuter) {
-    for (int k = K; k < K + kOuter && k < maxn; k += kPanel) {
+  for (int K = K0; K < K1 && K < maxn; K += outer) {
+    for (int k = K; k < K + outer && k < maxn; k += kPanel) {
       // ---- phase A: rows below the (already factored) diagonal block ----
       load_phase();
       for (int item = blockIdx.x; item < pre[nf]; item += gridDim.x) {
@@ -739,7 +740,7 @@ __global__ void __launch_bounds__(kCT) k_level_coop(const int* __restrict__ flis
         T* A = F + d.off;
         const int kb = min(kPanel, d.n - k);
         int local = item - pre[i];
-        const int c0 = k + kb, cmax = min(K + kOuter, d.n);
+        const int c0 = k + kb, cmax = min(K + outer, d.n);
         const int TI = ceil_div(d.N - c0, 64);
         int J = 0;
         while (local >= TI - J) {
@@ -755,13 +756,13 @@ __global__ void __launch_bounds__(kCT) k_level_coop(const int* __restrict__ flis
       grid_barrier(gbar, gtarget, err);
     }
     // ---- phase C: trailing update with the outer panel ----
-    if (!trailing && K + kOuter >= K1) break;
+    if (!trailing && K + outer >= K1) break;
     load_phase();
     for (int item = blockIdx.x; item < pre[nf]; item += gridDim.x) {
       const int i = find(item);
       const int f = flist[i];
       const FrontDev d = fr[f];
-      const int k1 = min(K + kOuter, d.n);
+      const int k1 = min(K + outer, d.n);
       int I, J;
       tri_index(item - pre[i], I, J);
       coop_tile_update(F + d.off, d.ld, d.N, d.N, k1 + I * 64, k1 + J * 64, K, k1, Xa, Xb);
@@ -1184,7 +1185,9 @@ size_t coop_slot_elems() { return (size_t)kMaxCoopFronts * kDiagSlot; }
 // Work items per phase of k_level_coop for fronts (n_i, N_i), in the kernel's
 // phase order: for each outer panel K, for each 32-column step k, phases A and
 // B; then phase C.  Returns the per-phase prefixes (nf + 1 ints each).
-std::vector<int> coop_phase_prefix(const std::vector<int>& n, const std::vector<int>& N, int maxn) {
+std::vector<int> coop_phase_prefix(const std::vector<int>& n, const std::vector<int>& N, int maxn,
+                                   int outer) {
+  if (outer <= 0) outer = kOuter;
   const int nf = (int)n.size();
   std::vector<int> out;
   auto cdiv = [](int a, int b) { return (a + b - 1) / b; };
@@ -1196,12 +1199,12 @@ std::vector<int> coop_phase_prefix(const std::vector<int>& n, const std::vector<
       out.push_back(acc);
     }
   };
-  for (int K = 0; K < maxn; K += kOuter) {
-    for (int k = K; k < K + kOuter && k < maxn; k += kPanel) {
+  for (int K = 0; K < maxn; K += outer) {
+    for (int k = K; k < K + outer && k < maxn; k += kPanel) {
       push([&](int i) { return k < n[i] ? cdiv(N[i] - k - std::min(kPanel, n[i] - k), kCT) : 0; });
       push([&](int i) {
         if (k >= n[i]) return 0;
-        const int kb = std::min(kPanel, n[i] - k), c0 = k + kb, cmax = std::min(K + kOuter, n[i]);
+        const int kb = std::min(kPanel, n[i] - k), c0 = k + kb, cmax = std::min(K + outer, n[i]);
         if (cmax <= c0) return 0;
         const int TI = cdiv(N[i] - c0, 64), TJ = cdiv(cmax - c0, 64);
         int c = 0;
@@ -1210,7 +1213,7 @@ std::vector<int> coop_phase_prefix(const std::vector<int>& n, const std::vector<
       });
     }
     push([&](int i) {
-      const int k1 = std::min(K + kOuter, n[i]);
+      const int k1 = std::min(K + outer, n[i]);
       if (K >= n[i] || N[i] <= k1) return 0;
       const int T = cdiv(N[i] - k1, 64);
       return T * (T + 1) / 2;
@@ -1221,16 +1224,19 @@ std::vector<int> coop_phase_prefix(const std::vector<int>& n, const std::vector<
 
 int coop_outer() { return kOuter; }
 
-int coop_phases(int K, int maxn) {
-  return 2 * ((std::min(kOuter, maxn - K) + kPanel - 1) / kPanel) + 1;
+int coop_phases(int K, int maxn, int outer) {
+  if (outer <= 0) outer = kOuter;
+  return 2 * ((std::min(outer, maxn - K) + kPanel - 1) / kPanel) + 1;
 }
 
 template <class T>
 cudaError_t launch_level_coop(const int* flist, int nf, int maxn, const FrontDev* fr, T* F,
                               DevError* err, T* slots, const int* phase_pref, unsigned* gbar,
                               cudaStream_t st, int K0, int K1, int phase0, int trailing,
-                              int max_items) {
+                              int max_items, int outer) {
   if (nf <= 0) return cudaSuccess;
+  if (outer <= 0) outer = kOuter;
+  if (outer % kPanel || K0 % outer) return cudaErrorInvalidValue;
   cudaError_t me = cudaMemsetAsync(gbar, 0, sizeof(unsigned), st);
   if (me != cudaSuccess) return me;
   if (K1 < 0) K1 = maxn;
@@ -1248,7 +1254,7 @@ cudaError_t launch_level_coop(const int* flist, int nf, int maxn, const FrontDev
   void* args[] = {(void*)&flist, (void*)&nf,    (void*)&fr,         (void*)&F,
                   (void*)&err,   (void*)&maxn,  (void*)&slots,      (void*)&phase_pref,
                   (void*)&K0,    (void*)&K1,    (void*)&phase0,     (void*)&trailing,
-                  (void*)&gbar};
+                  (void*)&outer, (void*)&gbar};
   // levels with little parallel work: one CTA per work item, at least an
   // eighth of the full grid (a grid barrier costs more the more CTAs arrive)
   int g = grid;
@@ -1394,7 +1400,7 @@ void launch_sep_gather(const int* slist, int ns, const SepDev* sp, const int* do
                                 const int*, const double*, const int*, const double*, cudaStream_t); \
   template cudaError_t launch_level_coop<T>(const int*, int, int, const FrontDev*, T*, DevError*,  \
                                             T*, const int*, unsigned*, cudaStream_t, int, int, int, \
-                                            int, int);                                              \
+                                            int, int, int);                                         \
   template void launch_front_small<T>(const int*, int, int, const FrontDev*, T*, DevError*,        \
                                       cudaStream_t);                                                \
   template void launch_solve_fwd<T>(const int*, int, int, const FrontDev*, const T*, const int*,   \

@@ -1,12 +1,15 @@
 // Tensor-core trailing update of the mixed-precision factorization (sm_100a).
 //
-// After an outer panel of 512 pivot columns [K, k1) of a front has been
-// factored (k1 = min(K + 512, n)), the rest of the front is updated by
-//     C(k1:N, k1:N) -= P P^T,   P = L(k1:N, K:k1)
+// After a panel of w pivot columns [K, k1) of a front has been factored
+// (k1 = min(K + w, n)), the rest of the front is updated by
+//     C(k1:N, k1:cmax) -= P P(k1:cmax)^T,   P = L(k1:N, K:k1)
 // (lower triangle only), the right-looking Cholesky step that the reference's
 // dense LU performs inside Factor() (src/DE/mf2d.cpp:792-901, via
-// LinAlg::Dense::LU).  For the large fronts of the top tree levels this is
-// nearly all of the work.
+// LinAlg::Dense::LU).  cmax = N for the trailing update after an outer panel
+// (w = 512); inside an outer panel [K0, K0 + 512) the update after each
+// 128-column sub-panel is limited to the outer panel's remaining columns,
+// cmax = min(K0 + 512, n).  For the large fronts of the top tree levels this
+// is nearly all of the work.
 //
 // Two kernels per outer panel:
 //   * k_tc_pack writes the panel once, split into TF32 "hi" and "lo" parts
@@ -76,19 +79,30 @@ __host__ __device__ constexpr int img_off(int m, int k) {
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TN >> 3) << 17) |
                             ((uint32_t)(TM >> 4) << 24);
 
-// Panel geometry of a front for outer panel K: k1, 128-row blocks below k1,
-// 32-column chunks in [K, k1); nb = 0 when the front has no trailing update.
+// Panel geometry of a front for the panel [K, K + w): k1, 128-row blocks
+// below k1, 32-column chunks in [K, k1), the column bound cmax (cend < 0: N,
+// else min(cend, n)) and the 128-column blocks of C left of it; nb = 0 when the
+// front has no update.  Tiles: block rows I < nb, block columns J <= I, J < nj.
 struct PanelGeo {
-  int k1, nb, nch;
+  int k1, nb, nch, cmax, nj;
 };
-__host__ __device__ inline PanelGeo panel_geo(int n, int N, int K) {
-  PanelGeo g{0, 0, 0};
+__host__ __device__ inline PanelGeo panel_geo(int n, int N, int K, int w, int cend) {
+  PanelGeo g{0, 0, 0, 0, 0};
   if (K >= n) return g;
-  g.k1 = n < K + kTcOuter ? n : K + kTcOuter;
+  g.k1 = n < K + w ? n : K + w;
   if (N <= g.k1) return g;
+  g.cmax = cend < 0 ? N : (cend < n ? cend : n);
+  if (g.cmax <= g.k1) return g;
   g.nb = (N - g.k1 + TM - 1) / TM;
   g.nch = (g.k1 - K + TK - 1) / TK;
+  const int nj = (g.cmax - g.k1 + TN - 1) / TN;
+  g.nj = nj < g.nb ? nj : g.nb;
   return g;
+}
+
+// Tiles of a front: the lower triangle of the first nj block columns.
+__host__ __device__ inline int geo_tiles(const PanelGeo& g) {
+  return g.nj * g.nb - g.nj * (g.nj - 1) / 2;
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -212,12 +226,13 @@ __device__ __forceinline__ void tri_ij(int t, int& I, int& J) {
 struct TileInfo {
   float* A;
   int64_t ld;
-  int N, k1, r0, c0, nch, slot, I, J;
+  int N, k1, cmax, r0, c0, nch, slot, I, J;
   bool diag;
 };
 
 __device__ __forceinline__ TileInfo tile_info(const int* pre, int nf, const int* flist,
-                                              const FrontDev* fr, float* F, int K, int tile) {
+                                              const FrontDev* fr, float* F, int K, int w, int cend,
+                                              int tile) {
   int lo = 0, hi = nf - 1;   // largest i with pre[i] <= tile
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
@@ -225,15 +240,22 @@ __device__ __forceinline__ TileInfo tile_info(const int* pre, int nf, const int*
     else hi = mid - 1;
   }
   const FrontDev d = fr[flist[lo]];
-  const PanelGeo g = panel_geo(d.n, d.N, K);
+  const PanelGeo g = panel_geo(d.n, d.N, K, w, cend);
   TileInfo t;
   t.A = F + d.off;
   t.ld = d.ld;
   t.N = d.N;
   t.k1 = g.k1;
+  t.cmax = g.cmax;
   t.nch = g.nch;
   t.slot = lo;
-  tri_ij(tile - pre[lo], t.I, t.J);
+  const int local = tile - pre[lo], tri = g.nj * (g.nj + 1) / 2;
+  if (local < tri) {
+    tri_ij(local, t.I, t.J);
+  } else {   // block rows below the first nj block columns' triangle
+    t.I = g.nj + (local - tri) / g.nj;
+    t.J = (local - tri) % g.nj;
+  }
   t.r0 = t.k1 + t.I * TM;
   t.c0 = t.k1 + t.J * TN;
   t.diag = (t.I == t.J);
@@ -247,11 +269,11 @@ __device__ __forceinline__ TileInfo tile_info(const int* pre, int nf, const int*
 template <int SPLIT>
 __global__ void __launch_bounds__(128) k_tc_pack(const int* __restrict__ flist,
                                                  const FrontDev* __restrict__ fr,
-                                                 const float* __restrict__ F, int K, int cap,
-                                                 unsigned char* __restrict__ pack) {
+                                                 const float* __restrict__ F, int K, int w,
+                                                 int cap, unsigned char* __restrict__ pack) {
   __shared__ __align__(1024) unsigned char img[SPLIT == 3 ? 2 * IMG : IMG];
   const FrontDev d = fr[flist[blockIdx.y]];
-  const PanelGeo g = panel_geo(d.n, d.N, K);
+  const PanelGeo g = panel_geo(d.n, d.N, K, w, -1);
   const int x = blockIdx.x;
   if (x >= g.nb * g.nch) return;
   const int b = x / g.nch, c = x - b * g.nch, t = threadIdx.x;
@@ -291,8 +313,8 @@ __global__ void __launch_bounds__(128) k_tc_pack(const int* __restrict__ flist,
 template <int SPLIT>
 __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ flist, int nf,
                                                      const FrontDev* __restrict__ fr,
-                                                     float* __restrict__ F, int K, int cap,
-                                                     const unsigned char* __restrict__ pack,
+                                                     float* __restrict__ F, int K, int w, int cend,
+                                                     int cap, const unsigned char* __restrict__ pack,
                                                      DevError* err) {
   extern __shared__ unsigned char tc_raw[];
   __shared__ uint64_t full[NSTAGE], empty[NSTAGE], acc_full[NACC], acc_empty[NACC];
@@ -308,8 +330,7 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
     pre[0] = 0;
     for (int i = 0; i < nf; i++) {
       const FrontDev d = fr[flist[i]];
-      const PanelGeo g = panel_geo(d.n, d.N, K);
-      acc += g.nb * (g.nb + 1) / 2;
+      acc += geo_tiles(panel_geo(d.n, d.N, K, w, cend));
       pre[i + 1] = acc;
     }
     for (int s = 0; s < NSTAGE; s++) {
@@ -343,7 +364,7 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
       uint32_t g = 0;
       bool ok = true;
       for (int tile = blockIdx.x; ok && tile < total && !abort_flag; tile += gridDim.x) {
-        const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, tile);
+        const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, w, cend, tile);
         const unsigned char* pa = pack + ((int64_t)ti.slot * cap + (int64_t)ti.I * ti.nch) * 2 * IMG;
         const unsigned char* pb = pack + ((int64_t)ti.slot * cap + (int64_t)ti.J * ti.nch) * 2 * IMG;
         for (int c = 0; c < ti.nch; c++, g++) {
@@ -369,7 +390,7 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
     uint32_t g = 0, tl = 0;
     for (int tile = blockIdx.x; tile < total && !__shfl_sync(0xffffffffu, abort_flag, 0);
          tile += gridDim.x, tl++) {
-      const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, tile);
+      const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, w, cend, tile);
       const int b = tl % NACC;
       const uint32_t v = tl / NACC;
       if (v >= 1 && !mbar_wait_warp(&acc_empty[b], (v - 1) & 1, &abort_flag)) break;
@@ -411,15 +432,15 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
     uint32_t tl = 0;
     for (int tile = blockIdx.x; tile < total && !__shfl_sync(0xffffffffu, abort_flag, 0);
          tile += gridDim.x, tl++) {
-      const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, tile);
+      const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, w, cend, tile);
       const int b = tl % NACC;
       const int row = ti.r0 + quarter * 32 + lane, cb = ti.c0 + half * 64;
       const bool live = row < ti.N;
       float* p = ti.A + row + (int64_t)cb * ti.ld;
-      // entry j of the row is live when cb + j <= min(row, N - 1); the first
+      // entry j of the row is live when cb + j <= min(row, cmax - 1); the first
       // 32 values are loaded while the tile's products are still being
       // accumulated, the other 32 while the first are stored
-      const int jmax = live ? min(row, ti.N - 1) - cb : -1;
+      const int jmax = live ? min(row, ti.cmax - 1) - cb : -1;
       const uint32_t src = tmem + b * TN + half * 64 + ((uint32_t)(quarter * 32) << 16);
       bool ok = true;
 #pragma unroll
@@ -464,19 +485,16 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
 int tc_outer() { return kTcOuter; }
 int tc_max_fronts() { return kMaxTcFronts; }
 
-int64_t tc_tiles(const std::vector<int>& n, const std::vector<int>& N, int K) {
+int64_t tc_tiles(const std::vector<int>& n, const std::vector<int>& N, int K, int w, int cend) {
   int64_t t = 0;
-  for (size_t i = 0; i < n.size(); i++) {
-    const PanelGeo g = panel_geo(n[i], N[i], K);
-    t += (int64_t)g.nb * (g.nb + 1) / 2;
-  }
+  for (size_t i = 0; i < n.size(); i++) t += geo_tiles(panel_geo(n[i], N[i], K, w, cend));
   return t;
 }
 
-int tc_pack_cap(const std::vector<int>& n, const std::vector<int>& N, int K) {
+int tc_pack_cap(const std::vector<int>& n, const std::vector<int>& N, int K, int w) {
   int cap = 0;
   for (size_t i = 0; i < n.size(); i++) {
-    const PanelGeo g = panel_geo(n[i], N[i], K);
+    const PanelGeo g = panel_geo(n[i], N[i], K, w, -1);
     cap = std::max(cap, g.nb * g.nch);
   }
   return cap;
@@ -499,29 +517,32 @@ int tc_setup() {   // thread-safe one-time set-up (static local initialisation)
 }  // namespace
 
 cudaError_t launch_tc_pack(const int* flist, int nf, int cap, const FrontDev* fr, const float* F,
-                           int K, int split, void* pack, cudaStream_t st) {
+                           int K, int w, int split, void* pack, cudaStream_t st) {
   if (nf <= 0 || cap <= 0) return cudaSuccess;
-  if (nf > 65535 || (split != 1 && split != 3)) return cudaErrorInvalidValue;
+  if (nf > 65535 || (split != 1 && split != 3) || w <= 0 || w % TK || w > kTcOuter)
+    return cudaErrorInvalidValue;
   const dim3 grid((unsigned)cap, (unsigned)nf);
   if (split == 3)
-    k_tc_pack<3><<<grid, 128, 0, st>>>(flist, fr, F, K, cap, (unsigned char*)pack);
+    k_tc_pack<3><<<grid, 128, 0, st>>>(flist, fr, F, K, w, cap, (unsigned char*)pack);
   else
-    k_tc_pack<1><<<grid, 128, 0, st>>>(flist, fr, F, K, cap, (unsigned char*)pack);
+    k_tc_pack<1><<<grid, 128, 0, st>>>(flist, fr, F, K, w, cap, (unsigned char*)pack);
   g_launches++;
   return cudaGetLastError();
 }
 
 cudaError_t launch_trail_tc(const int* flist, int nf, int64_t ntiles, const FrontDev* fr, float* F,
-                            int K, int split, int cap, const void* pack, DevError* err,
-                            cudaStream_t st) {
+                            int K, int w, int cend, int split, int cap, const void* pack,
+                            DevError* err, cudaStream_t st) {
   if (nf <= 0 || ntiles <= 0) return cudaSuccess;
-  if (nf > kMaxTcFronts || (split != 1 && split != 3) || !pack) return cudaErrorInvalidValue;
+  if (nf > kMaxTcFronts || (split != 1 && split != 3) || !pack || w <= 0 || w % TK ||
+      w > kTcOuter)
+    return cudaErrorInvalidValue;
   const int grid = (int)std::min<int64_t>(ntiles, tc_setup());
   if (split == 3)
-    k_trail_tc<3><<<grid, TCT, kTcSmem, st>>>(flist, nf, fr, F, K, cap,
+    k_trail_tc<3><<<grid, TCT, kTcSmem, st>>>(flist, nf, fr, F, K, w, cend, cap,
                                               (const unsigned char*)pack, err);
   else
-    k_trail_tc<1><<<grid, TCT, kTcSmem, st>>>(flist, nf, fr, F, K, cap,
+    k_trail_tc<1><<<grid, TCT, kTcSmem, st>>>(flist, nf, fr, F, K, w, cend, cap,
                                               (const unsigned char*)pack, err);
   g_launches++;
   return cudaGetLastError();

@@ -70,6 +70,7 @@ struct Plan {
     Group ftask, sbase, sadd0, sadd1;
     int64_t cpref0 = 0;   // offset of the cooperative kernel's phase prefixes in cpref
     int coopItems = 0;    // largest work-item count of any cooperative phase
+    int coopOuter = 0;    // outer panel width the phase prefixes were built with (0: default)
   };
   size_t tcPackBytes = 0;   // largest tensor-core panel pack any level of the plan needs
   std::vector<Level> lv;
@@ -260,6 +261,9 @@ struct mfgpu_handle {
   bool mixed = false;
   int tcMinN = 4096;               // mixed: smallest level maxN run on the tensor cores (0 = never)
   int tcSplit = 3;                 // mixed: 3 = three-term TF32 products, 1 = plain TF32
+  int tcSplit3Levels = -1;         // >= 0: three-term products only on the top levels 0 .. this - 1
+  int tcSub = 128;                 // mixed: sub-panel width inside each 512-column outer panel of a
+                                   // tensor-core level (0 or 512: no sub-panels)
   int fusedMinFronts = 148;        // fewest fronts for the one-CTA-per-front kernel
   size_t esz = sizeof(double);     // bytes per factor element
   double* d_scale = nullptr;       // s = 1/sqrt(diag(A)) of the last full factorization
@@ -390,17 +394,25 @@ struct mfgpu_handle {
           nn.push_back(s.fronts[f].n);
           NN.push_back(s.fronts[f].N);
         }
-        std::vector<int> pp = mfgpu::coop_phase_prefix(nn, NN, L.maxn);
+        const int W = mfgpu::tc_outer();
+        const bool tc = mixed && tcLevel(L);
+        L.coopOuter = tc && tcSub > 0 && tcSub < W ? tcSub : 0;
+        std::vector<int> pp = mfgpu::coop_phase_prefix(nn, NN, L.maxn, L.coopOuter);
         P.cpref.insert(P.cpref.end(), pp.begin(), pp.end());
         // the most work items any phase has: a level with little parallel work
         // runs on fewer CTAs, so its grid barriers are cheaper
         const size_t stride = fl.size() + 1;
         for (size_t q = 0; q + stride <= pp.size(); q += stride)
           L.coopItems = std::max(L.coopItems, pp[q + fl.size()]);
-        if (mixed && tcLevel(L))
-          for (int K = 0; K < L.maxn; K += mfgpu::tc_outer())
-            P.tcPackBytes = std::max(P.tcPackBytes,
-                                     mfgpu::tc_pack_bytes((int)fl.size(), mfgpu::tc_pack_cap(nn, NN, K)));
+        if (tc) {
+          const int w = L.coopOuter > 0 ? L.coopOuter : W;
+          for (int K = 0; K < L.maxn; K += w)
+            for (int ww : {w, W})
+              if (K % ww == 0)
+                P.tcPackBytes = std::max(
+                    P.tcPackBytes,
+                    mfgpu::tc_pack_bytes((int)fl.size(), mfgpu::tc_pack_cap(nn, NN, K, ww)));
+        }
       }
     }
   }
@@ -465,7 +477,7 @@ struct mfgpu_handle {
           ck(cudaGetLastError(), "launch fused front factorization (k_front_small)");
           prof.end(stream);
         } else if (sizeof(T) == sizeof(float) && tcLevel(L)) {
-          runTensorLevel(P, L, fl);
+          runTensorLevel(P, L, fl, ell);
         } else {
           prof.flops[MFGPU_KC_COOP] += fl;
           prof.begin(MFGPU_KC_COOP, stream);
@@ -506,45 +518,65 @@ struct mfgpu_handle {
     return tcMinN > 0 && L.maxN >= tcMinN && L.nf <= mfgpu::tc_max_fronts();
   }
 
-  // Profile attribution: the trailing updates' algorithmic flops,
-  // sum (N - k1)^2 (k1 - K), go to MFGPU_KC_TC, the rest of the level's flops
-  // (diagonal blocks, panel solves, in-panel updates) to MFGPU_KC_COOP.
-  void runTensorLevel(const Plan& P, const Plan::Level& L, double level_flops) {
+  // Tensor-core level (mixed path).  Per 512-column outer panel [K, K + 512):
+  // the cooperative kernel factors it one sub-panel [Ks, Ks + w) at a time
+  // (w = L.coopOuter, 32-column steps inside), and after each sub-panel the
+  // tensor cores update the outer panel's remaining columns [Ks + w, K + 512)
+  // of all rows below; then the tensor cores apply the whole outer panel to
+  // the trailing matrix.  With w = 512 (no sub-panels) only the trailing
+  // update remains.  Profile attribution: the tensor-core updates'
+  // algorithmic flops go to MFGPU_KC_TC, the rest of the level's flops
+  // (diagonal blocks, panel solves, in-sub-panel updates) to MFGPU_KC_COOP.
+  void runTensorLevel(const Plan& P, const Plan::Level& L, double level_flops, int ell) {
     const Schedule& s = *S;
+    const int split = tcSplit3Levels >= 0 && ell >= tcSplit3Levels ? 1 : tcSplit;
     std::vector<int> nn(L.nf), NN(L.nf);
     for (int64_t i = 0; i < L.nf; i++) {
       nn[i] = s.fronts[P.ids[L.f0 + i]].n;
       NN[i] = s.fronts[P.ids[L.f0 + i]].N;
     }
-    const int outer = mfgpu::coop_outer();
+    const int W = mfgpu::tc_outer(), w = L.coopOuter > 0 ? L.coopOuter : W;
     int phase0 = 0;
     double tc_fl = 0;
-    for (int K = 0; K < L.maxn; K += outer) {
-      prof.begin(MFGPU_KC_COOP, stream);
-      ck(mfgpu::launch_level_coop<float>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, (float*)d_F,
-                                         d_err, (float*)d_slots, P.d_cpref + L.cpref0, d_gbar,
-                                         stream, K, K + outer, phase0, 0, L.coopItems),
-         "launch cooperative panel factorization (k_level_coop)");
-      prof.end(stream);
-      phase0 += mfgpu::coop_phases(K, L.maxn);
-      const int64_t nt = mfgpu::tc_tiles(nn, NN, K);
+    // C(k1:N, k1:cmax) -= P P^T for the panel [K0, K0 + pw), cmax = min(cend, n) (cend < 0: N)
+    auto update = [&](int K0, int pw, int cend) {
+      const int64_t nt = mfgpu::tc_tiles(nn, NN, K0, pw, cend);
+      if (nt == 0) return;
       if (prof.on)
         for (int64_t i = 0; i < L.nf; i++)
-          if (K < nn[i]) {
-            const double k1 = std::min(K + outer, nn[i]), r = NN[i] - k1;
-            tc_fl += r * r * (k1 - K);
+          if (K0 < nn[i]) {
+            const double k1 = std::min(K0 + pw, nn[i]);
+            const double c = cend < 0 ? NN[i] : std::min(cend, nn[i]);
+            if (c <= k1) continue;
+            // lower-triangle entries of rows [k1, N) x columns [k1, c), one
+            // multiply-add per entry and panel column
+            const double r = NN[i] - k1, cw = c - k1;
+            tc_fl += 2.0 * cw * (r - 0.5 * cw) * (k1 - K0);
           }
-      const int cap = mfgpu::tc_pack_cap(nn, NN, K);
+      const int cap = mfgpu::tc_pack_cap(nn, NN, K0, pw);
       if (mfgpu::tc_pack_bytes((int)L.nf, cap) > tcPackCap)
         throw CudaError("tensor-core panel pack larger than planned", MFGPU_ERR_STATE);
       prof.begin(MFGPU_KC_TC, stream);
-      ck(mfgpu::launch_tc_pack(P.d_ids + L.f0, (int)L.nf, cap, d_fr, (const float*)d_F, K, tcSplit,
-                               d_tcpack, stream),
+      ck(mfgpu::launch_tc_pack(P.d_ids + L.f0, (int)L.nf, cap, d_fr, (const float*)d_F, K0, pw,
+                               split, d_tcpack, stream),
          "launch tensor-core panel pack (k_tc_pack)");
-      ck(mfgpu::launch_trail_tc(P.d_ids + L.f0, (int)L.nf, nt, d_fr, (float*)d_F, K, tcSplit, cap,
-                                d_tcpack, d_err, stream),
-         "launch tensor-core trailing update (k_trail_tc)");
+      ck(mfgpu::launch_trail_tc(P.d_ids + L.f0, (int)L.nf, nt, d_fr, (float*)d_F, K0, pw, cend,
+                                split, cap, d_tcpack, d_err, stream),
+         "launch tensor-core update (k_trail_tc)");
       prof.end(stream);
+    };
+    for (int K = 0; K < L.maxn; K += W) {
+      for (int Ks = K; Ks < K + W && Ks < L.maxn; Ks += w) {
+        prof.begin(MFGPU_KC_COOP, stream);
+        ck(mfgpu::launch_level_coop<float>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, (float*)d_F,
+                                           d_err, (float*)d_slots, P.d_cpref + L.cpref0, d_gbar,
+                                           stream, Ks, Ks + w, phase0, 0, L.coopItems, w),
+           "launch cooperative panel factorization (k_level_coop)");
+        prof.end(stream);
+        phase0 += mfgpu::coop_phases(Ks, L.maxn, w);
+        if (Ks + w < K + W) update(Ks, w, K + W);   // the outer panel's remaining columns
+      }
+      update(K, W, -1);   // the trailing matrix
     }
     prof.flops[MFGPU_KC_TC] += tc_fl;
     prof.flops[MFGPU_KC_COOP] += std::max(0.0, level_flops - tc_fl);
@@ -1039,6 +1071,8 @@ int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const
   if (const char* e = getenv("MFGPU_SOLVE_COOP_MIN_N")) h->solveCoopMinN = atoi(e);
   if (const char* e = getenv("MFGPU_FUSED_MIN_FRONTS")) h->fusedMinFronts = atoi(e);
   if (const char* e = getenv("MFGPU_TC_SPLIT")) h->tcSplit = atoi(e) == 1 ? 1 : 3;
+  if (const char* e = getenv("MFGPU_TC_SPLIT3_LEVELS")) h->tcSplit3Levels = atoi(e);
+  if (const char* e = getenv("MFGPU_TC_SUB")) h->tcSub = atoi(e);
   h->h_rowptr.assign(row_ptr, row_ptr + n + 1);
   h->h_colind.assign(col_ind, col_ind + h->nnz);
   int st = guarded(h.get(), [&]() {
@@ -1927,6 +1961,8 @@ std::unique_ptr<mfgpu_handle> makeView(mfgpu_handle& B) {
   H.esz = B.esz;
   H.tcMinN = B.tcMinN;
   H.tcSplit = B.tcSplit;
+  H.tcSplit3Levels = B.tcSplit3Levels;
+  H.tcSub = B.tcSub;
   H.fusedMinFronts = B.fusedMinFronts;
   H.d_scale = B.d_scale;
   H.d_iscale = B.d_iscale;
