@@ -11,32 +11,36 @@
 // cmax = min(K0 + 512, n).  For the large fronts of the top tree levels this
 // is nearly all of the work.
 //
-// Two kernels per outer panel:
+// Two kernels per panel:
 //   * k_tc_pack writes the panel once, split into TF32 "hi" and "lo" parts
-//     (x = hi + lo, both exactly representable), as 16 KB images of 128 rows x
-//     32 columns in the K-major 128-byte-swizzled layout the tensor core
-//     reads: one CTA per (128-row block, 32-column chunk) reads its block
-//     coalesced from the column-major front, splits it in shared memory and
-//     writes the hi / lo image pair out contiguously;
-//   * k_trail_tc, a persistent warp-specialised pipeline over 128 x 128 tiles
-//     of C (lower triangle only):
-//       - one producer thread brings the image pairs of each chunk (the
-//         tile's row block and, off the diagonal, its column block) into a
-//         ring of three shared-memory stages with bulk asynchronous copies
-//         (cp.async.bulk, completion counted in bytes on an mbarrier);
-//       - one MMA warp issues tcgen05.mma (kind::tf32, M = N = 128, K = 8)
-//         from an elected lane into one of two tensor-memory accumulators:
+//     (x = hi + lo, both exactly representable), as 8 KB images of 128 rows x
+//     16 columns in the K-major 64-byte-swizzled layout the tensor core reads:
+//     one CTA per (128-row block, 16-column chunk) reads its block coalesced
+//     from the column-major front and splits it in shared memory; per chunk
+//     the hi images of all row blocks are contiguous, then the lo images;
+//   * k_trail_tc, a persistent warp-specialised pipeline over 128 x 256 tiles
+//     of C (block row I of 128 rows, block column J of 256 columns, lower
+//     triangle only):
+//       - one producer thread brings each chunk's images (the tile's row
+//         block, unless it lies inside the column block, and the two row
+//         blocks of the column block) into a ring of four shared-memory
+//         stages with bulk asynchronous copies (cp.async.bulk, completion
+//         counted in bytes on an mbarrier);
+//       - one MMA warp issues tcgen05.mma (kind::tf32, M = 128, N = 256,
+//         K = 8) from an elected lane into one of two tensor-memory
+//         accumulators (256 columns each, all of tensor memory):
 //             SPLIT = 3:  acc += hi_a hi_b^T + hi_a lo_b^T + lo_a hi_b^T
 //             SPLIT = 1:  acc += hi_a hi_b^T
 //         and hands stages back to the producer with tcgen05.commit;
-//       - eight epilogue warps (two per accumulator lane quarter, 64 columns
-//         each) load their C values for a tile before its accumulator is
-//         ready, then read the accumulator with tcgen05.ld and subtract it
-//         from C in place.
-// MN-major TF32 operands would let the tensor core read the column-major
-// front directly, but they read back as zeros on sm_100a, hence the pack.
-// The three-term form keeps products to about 2^-21 relative error, close to
-// FP32.
+//       - eight epilogue warps (two per accumulator lane quarter, 128 columns
+//         each, 32 at a time) read the accumulator with tcgen05.ld and
+//         subtract it from C in place; the first 32 values of C are loaded
+//         before the accumulator is ready.
+// A 256-column tile reads 25% fewer operand bytes per product than a 128 x 128
+// one, and 16-column stages keep three stages in flight.  MN-major TF32
+// operands would let the tensor core read the column-major front directly,
+// but they read back as zeros on sm_100a, hence the pack.  The three-term form
+// keeps products to about 2^-21 relative error, close to FP32.
 //
 // Every mbarrier wait is bounded; on expiry (or once another warp gave up) the
 // kernel records error code 2 in the error word, skips the remaining work,
@@ -52,37 +56,38 @@ extern std::atomic<long long> g_launches;
 
 namespace {
 
-constexpr int TM = 128;                    // C tile rows = accumulator lanes
-constexpr int TN = 128;                    // C tile columns = accumulator columns
-constexpr int TK = 32;                     // panel columns per chunk
-constexpr int NSTAGE = 3;                  // shared-memory stages
+constexpr int TM = 128;                    // C tile rows = accumulator lanes = image rows
+constexpr int TN = 256;                    // C tile columns = accumulator columns
+constexpr int TK = 16;                     // panel columns per chunk (64-byte image rows)
+constexpr int NSTAGE = 4;                  // shared-memory stages
 constexpr int NACC = 2;                    // tensor-memory accumulators
 constexpr int MMA_WARP = 1;                // warp 0 produces, warp 1 issues the MMAs
 constexpr int EPI_WARP0 = 2;               // warps 2..9 run the epilogue
 constexpr int NEPI = 8;
 constexpr int TCT = (EPI_WARP0 + NEPI) * 32;   // 320 threads
-constexpr int IMG = TM * TK * 4;           // one image of 128 rows x 32 columns, 16 KB
-constexpr int STAGE_BYTES = 4 * IMG;       // a_hi, a_lo, b_hi, b_lo
+constexpr int IMG = TM * TK * 4;           // one image of 128 rows x 16 columns, 8 KB
+constexpr int STAGE_BYTES = 6 * IMG;       // a_hi, a_lo, b_hi (2 blocks), b_lo (2 blocks)
 constexpr int kTcSmem = NSTAGE * STAGE_BYTES + 1024;   // + alignment slack
 constexpr int kMaxTcFronts = 1024;
 constexpr int kTcOuter = 512;              // outer panel width (the cooperative kernel's)
 constexpr uint32_t kSpinLimit = 1u << 24;
 
-// Image layout (K-major, 128-byte swizzle): element (m, k) of a 128 x 32
-// image sits in 128-byte row m, 16-byte chunk (k / 4) ^ (m % 8), word k % 4;
-// 8-row groups are 1024 bytes apart.
+// Image layout (K-major, 64-byte swizzle): element (m, k) of a 128 x 16 image
+// sits in 64-byte row m, 16-byte chunk (k / 4) ^ ((m / 2) % 4), word k % 4;
+// 8-row groups are 512 bytes apart.
 __host__ __device__ constexpr int img_off(int m, int k) {
-  return m * 128 + ((((k >> 2) ^ (m & 7))) << 4) + (k & 3) * 4;
+  return m * 64 + ((((k >> 2) ^ ((m >> 1) & 3))) << 4) + (k & 3) * 4;
 }
 
-// Instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = 128.
+// Instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = 256.
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TN >> 3) << 17) |
                             ((uint32_t)(TM >> 4) << 24);
 
 // Panel geometry of a front for the panel [K, K + w): k1, 128-row blocks
-// below k1, 32-column chunks in [K, k1), the column bound cmax (cend < 0: N,
-// else min(cend, n)) and the 128-column blocks of C left of it; nb = 0 when the
-// front has no update.  Tiles: block rows I < nb, block columns J <= I, J < nj.
+// below k1, 16-column chunks in [K, k1), the column bound cmax (cend < 0: N,
+// else min(cend, n)) and the 256-column blocks of C left of it; nb = 0 when
+// the front has no update.  Tiles: block rows I < nb, block columns
+// J <= I / 2, J < nj.
 struct PanelGeo {
   int k1, nb, nch, cmax, nj;
 };
@@ -95,25 +100,45 @@ __host__ __device__ inline PanelGeo panel_geo(int n, int N, int K, int w, int ce
   if (g.cmax <= g.k1) return g;
   g.nb = (N - g.k1 + TM - 1) / TM;
   g.nch = (g.k1 - K + TK - 1) / TK;
-  const int nj = (g.cmax - g.k1 + TN - 1) / TN;
-  g.nj = nj < g.nb ? nj : g.nb;
+  g.nj = (g.cmax - g.k1 + TN - 1) / TN;   // <= (nb + 1) / 2 since cmax <= N
   return g;
 }
 
-// Tiles of a front: the lower triangle of the first nj block columns.
+// Tiles of a front: row I has min(I / 2 + 1, nj) of them.  Rows 0 .. 2 nj - 1
+// come in pairs (2p, 2p + 1) of p + 1 tiles each; the rows below have nj.
 __host__ __device__ inline int geo_tiles(const PanelGeo& g) {
-  return g.nj * g.nb - g.nj * (g.nj - 1) / 2;
+  if (g.nb <= 2 * g.nj) {
+    const int p = g.nb / 2;
+    return g.nb % 2 == 0 ? p * (p + 1) : (p + 1) * (p + 1);
+  }
+  return g.nj * (g.nj + 1) + (g.nb - 2 * g.nj) * g.nj;
+}
+
+__device__ __forceinline__ void tile_ij(int t, int nj, int& I, int& J) {
+  const int tri = nj * (nj + 1);
+  if (t < tri) {
+    int p = (int)((sqrt(4.0 * t + 1.0) - 1.0) * 0.5);
+    while (p * (p + 1) > t) p--;
+    while ((p + 1) * (p + 2) <= t) p++;
+    const int o = t - p * (p + 1);
+    I = 2 * p + o / (p + 1);
+    J = o % (p + 1);
+  } else {
+    const int t2 = t - tri;
+    I = 2 * nj + t2 / nj;
+    J = t2 % nj;
+  }
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// Shared-memory matrix descriptor of a K-major operand image with 128-byte
-// swizzle: rows of 128 bytes, 8-row groups 1024 bytes apart.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
-         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+// Shared-memory matrix descriptor of a K-major operand image with 64-byte
+// swizzle: rows of 64 bytes, 8-row groups 512 bytes apart.
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(512 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
 }
 
 // Bulk asynchronous copy global -> this CTA's shared memory; completion is
@@ -215,19 +240,11 @@ __device__ __forceinline__ float tf32_round(float x) {
   return __uint_as_float(r);
 }
 
-__device__ __forceinline__ void tri_ij(int t, int& I, int& J) {
-  I = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
-  while (I * (I + 1) / 2 > t) I--;
-  while ((I + 1) * (I + 2) / 2 <= t) I++;
-  J = t - I * (I + 1) / 2;
-}
-
-// Tile t of the launch: front slot i, block row I >= block column J.
+// Tile t of the launch: front slot i, block row I, block column J.
 struct TileInfo {
   float* A;
   int64_t ld;
-  int N, k1, cmax, r0, c0, nch, slot, I, J;
-  bool diag;
+  int N, k1, cmax, r0, c0, nch, nb, slot, I, J;
 };
 
 __device__ __forceinline__ TileInfo tile_info(const int* pre, int nf, const int* flist,
@@ -248,35 +265,30 @@ __device__ __forceinline__ TileInfo tile_info(const int* pre, int nf, const int*
   t.k1 = g.k1;
   t.cmax = g.cmax;
   t.nch = g.nch;
+  t.nb = g.nb;
   t.slot = lo;
-  const int local = tile - pre[lo], tri = g.nj * (g.nj + 1) / 2;
-  if (local < tri) {
-    tri_ij(local, t.I, t.J);
-  } else {   // block rows below the first nj block columns' triangle
-    t.I = g.nj + (local - tri) / g.nj;
-    t.J = (local - tri) % g.nj;
-  }
+  tile_ij(tile - pre[lo], g.nj, t.I, t.J);
   t.r0 = t.k1 + t.I * TM;
   t.c0 = t.k1 + t.J * TN;
-  t.diag = (t.I == t.J);
   return t;
 }
 
-// Pack: CTA (x, i) = image pair x = b * nch + c of front slot i, rows
-// k1 + 128 b + t (thread t), columns K + 32 c .. +31; zeros outside the front
-// and beyond k1.  Pair (i, x) starts at byte (i * cap + x) * 2 * IMG of pack:
-// hi image, then lo image (SPLIT = 3 only).
+// Pack: CTA (x, i) = chunk c, row block b (x = c * nb + b) of front slot i:
+// rows k1 + 128 b + t (thread t), columns K + 16 c .. +15; zeros outside the
+// front and beyond k1.  Front slot i owns bytes [i * cap * 2 * IMG, +cap * 2 *
+// IMG) of pack; inside, the hi image of (c, b) is image (2 c) * nb + b and the
+// lo image (2 c + 1) * nb + b.
 template <int SPLIT>
 __global__ void __launch_bounds__(128) k_tc_pack(const int* __restrict__ flist,
                                                  const FrontDev* __restrict__ fr,
                                                  const float* __restrict__ F, int K, int w,
                                                  int cap, unsigned char* __restrict__ pack) {
-  __shared__ __align__(1024) unsigned char img[SPLIT == 3 ? 2 * IMG : IMG];
+  __shared__ __align__(1024) unsigned char img[2 * IMG];
   const FrontDev d = fr[flist[blockIdx.y]];
   const PanelGeo g = panel_geo(d.n, d.N, K, w, -1);
   const int x = blockIdx.x;
   if (x >= g.nb * g.nch) return;
-  const int b = x / g.nch, c = x - b * g.nch, t = threadIdx.x;
+  const int c = x / g.nb, b = x - c * g.nb, t = threadIdx.x;
   const int row = g.k1 + b * TM + t, kc = K + c * TK;
   const bool row_ok = row < d.N;
   const float* src = F + d.off + (row_ok ? row : 0) + (int64_t)kc * d.ld;
@@ -304,10 +316,15 @@ __global__ void __launch_bounds__(128) k_tc_pack(const int* __restrict__ flist,
     }
   }
   __syncthreads();
-  float4* dst = reinterpret_cast<float4*>(pack + ((int64_t)blockIdx.y * cap + x) * 2 * IMG);
+  unsigned char* base = pack + (int64_t)blockIdx.y * cap * 2 * IMG;
+  float4* dh = reinterpret_cast<float4*>(base + ((int64_t)(2 * c) * g.nb + b) * IMG);
+  float4* dl = reinterpret_cast<float4*>(base + ((int64_t)(2 * c + 1) * g.nb + b) * IMG);
   const float4* s4 = reinterpret_cast<const float4*>(img);
-#pragma unroll 4
-  for (int e = t; e < (SPLIT == 3 ? 2 : 1) * IMG / 16; e += 128) dst[e] = s4[e];
+#pragma unroll
+  for (int e = t; e < IMG / 16; e += 128) {
+    dh[e] = s4[e];
+    if (SPLIT == 3) dl[e] = s4[IMG / 16 + e];
+  }
 }
 
 template <int SPLIT>
@@ -355,18 +372,21 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
   tc_fence_after();
   const uint32_t tmem = tmem_base;
   const int total = pre[nf];
-  constexpr uint32_t kPairBytes = SPLIT == 3 ? 2 * IMG : IMG;   // bytes copied per image pair
 
   if (warp == 0) {
-    // ---- producer: one thread fills the stages with the chunks' image pairs ----
+    // ---- producer: one thread fills the stages; stage layout: a_hi, a_lo,
+    // b_hi (row blocks 2J, 2J + 1), b_lo (same) ----
     if (lane == 0) {
       const uint32_t sm0 = smem_u32(sm);
       uint32_t g = 0;
       bool ok = true;
       for (int tile = blockIdx.x; ok && tile < total && !abort_flag; tile += gridDim.x) {
         const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, w, cend, tile);
-        const unsigned char* pa = pack + ((int64_t)ti.slot * cap + (int64_t)ti.I * ti.nch) * 2 * IMG;
-        const unsigned char* pb = pack + ((int64_t)ti.slot * cap + (int64_t)ti.J * ti.nch) * 2 * IMG;
+        const unsigned char* base = pack + (int64_t)ti.slot * cap * 2 * IMG;
+        const int bb = 2 * ti.J, nbb = min(2, ti.nb - bb);   // row blocks of the column block
+        const bool a_in_b = ti.I - bb < nbb;                   // row block I is one of them
+        const uint32_t bbytes = (uint32_t)nbb * IMG, abytes = a_in_b ? 0u : (uint32_t)IMG;
+        const uint32_t tx = (SPLIT == 3 ? 2 : 1) * (abytes + bbytes);
         for (int c = 0; c < ti.nch; c++, g++) {
           const int s = g % NSTAGE;
           const uint32_t u = g / NSTAGE;
@@ -375,9 +395,15 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
             break;
           }
           const uint32_t st = sm0 + s * STAGE_BYTES;
-          mbar_expect_tx(&full[s], ti.diag ? kPairBytes : 2 * kPairBytes);
-          bulk_copy(st, pa + (int64_t)c * 2 * IMG, kPairBytes, &full[s]);
-          if (!ti.diag) bulk_copy(st + 2 * IMG, pb + (int64_t)c * 2 * IMG, kPairBytes, &full[s]);
+          const unsigned char* hi = base + (int64_t)(2 * c) * ti.nb * IMG;
+          const unsigned char* lo = base + (int64_t)(2 * c + 1) * ti.nb * IMG;
+          mbar_expect_tx(&full[s], tx);
+          bulk_copy(st + 2 * IMG, hi + (int64_t)bb * IMG, bbytes, &full[s]);
+          if (SPLIT == 3) bulk_copy(st + 4 * IMG, lo + (int64_t)bb * IMG, bbytes, &full[s]);
+          if (!a_in_b) {
+            bulk_copy(st, hi + (int64_t)ti.I * IMG, IMG, &full[s]);
+            if (SPLIT == 3) bulk_copy(st + IMG, lo + (int64_t)ti.I * IMG, IMG, &full[s]);
+          }
         }
       }
       // the copies still in flight land before the CTA may exit
@@ -396,6 +422,8 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
       if (v >= 1 && !mbar_wait_warp(&acc_empty[b], (v - 1) & 1, &abort_flag)) break;
       tc_fence_after();
       const uint32_t dacc = tmem + b * TN;
+      const int bb = 2 * ti.J, nbb = min(2, ti.nb - bb);
+      const int ia = ti.I - bb;   // row block I inside the column block when 0 <= ia < nbb
       bool ok = true;
       for (int c = 0; c < ti.nch; c++, g++) {
         const int s = g % NSTAGE;
@@ -405,16 +433,17 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
         }
         tc_fence_after();
         if (lane == 0) {
-          const uint32_t a_hi = smem_u32(sm + s * STAGE_BYTES), a_lo = a_hi + IMG;
-          const uint32_t b_hi = ti.diag ? a_hi : a_hi + 2 * IMG;
-          const uint32_t b_lo = ti.diag ? a_lo : a_hi + 3 * IMG;
+          const uint32_t st = smem_u32(sm + s * STAGE_BYTES);
+          const uint32_t b_hi = st + 2 * IMG, b_lo = st + 4 * IMG;
+          const bool in = ia >= 0 && ia < nbb;
+          const uint32_t a_hi = in ? b_hi + ia * IMG : st, a_lo = in ? b_lo + ia * IMG : st + IMG;
 #pragma unroll
           for (int kk = 0; kk < TK / 8; kk++) {
             const uint32_t ko = kk * 32;   // 8 TF32 values = 32 bytes along the swizzled row
-            mma_tf32(dacc, sw128_desc(a_hi + ko), sw128_desc(b_hi + ko), (c | kk) != 0);
+            mma_tf32(dacc, sw64_desc(a_hi + ko), sw64_desc(b_hi + ko), (c | kk) != 0);
             if (SPLIT == 3) {
-              mma_tf32(dacc, sw128_desc(a_hi + ko), sw128_desc(b_lo + ko), 1u);
-              mma_tf32(dacc, sw128_desc(a_lo + ko), sw128_desc(b_hi + ko), 1u);
+              mma_tf32(dacc, sw64_desc(a_hi + ko), sw64_desc(b_lo + ko), 1u);
+              mma_tf32(dacc, sw64_desc(a_lo + ko), sw64_desc(b_hi + ko), 1u);
             }
           }
           mma_commit(&empty[s]);
@@ -427,24 +456,25 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
     }
   } else {
     // ---- epilogue: C(tile) -= acc; warp w reads accumulator lanes
-    // 32 (w % 4) .. +31 (the lane quarter it may access), columns 64 h .. +63 ----
+    // 32 (w % 4) .. +31 (the lane quarter it may access), columns 128 h .. +127,
+    // 32 at a time ----
     const int quarter = warp & 3, half = (warp - EPI_WARP0) >> 2;
     uint32_t tl = 0;
     for (int tile = blockIdx.x; tile < total && !__shfl_sync(0xffffffffu, abort_flag, 0);
          tile += gridDim.x, tl++) {
       const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, w, cend, tile);
       const int b = tl % NACC;
-      const int row = ti.r0 + quarter * 32 + lane, cb = ti.c0 + half * 64;
+      const int row = ti.r0 + quarter * 32 + lane, cb = ti.c0 + half * (TN / 2);
       const bool live = row < ti.N;
       float* p = ti.A + row + (int64_t)cb * ti.ld;
       // entry j of the row is live when cb + j <= min(row, cmax - 1); the first
       // 32 values are loaded while the tile's products are still being
-      // accumulated, the other 32 while the first are stored
+      // accumulated, each later 32 once the previous ones are stored
       const int jmax = live ? min(row, ti.cmax - 1) - cb : -1;
-      const uint32_t src = tmem + b * TN + half * 64 + ((uint32_t)(quarter * 32) << 16);
+      const uint32_t src = tmem + b * TN + half * (TN / 2) + ((uint32_t)(quarter * 32) << 16);
       bool ok = true;
-#pragma unroll
-      for (int h2 = 0; h2 < 2; h2++) {
+#pragma unroll 1
+      for (int h2 = 0; h2 < TN / 64; h2++) {
         float cv[32];
         const float* q = p + (int64_t)(32 * h2) * ti.ld;
 #pragma unroll
@@ -456,14 +486,14 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
           }
           tc_fence_after();
         }
-        float* w = p + (int64_t)(32 * h2) * ti.ld;
+        float* wp = p + (int64_t)(32 * h2) * ti.ld;
 #pragma unroll
         for (int qb = 0; qb < 2; qb++) {
           uint32_t v[16];
           tmem_ld16(src + 32 * h2 + 16 * qb, v);
 #pragma unroll
-          for (int j = 0; j < 16; j++, w += ti.ld)
-            if (32 * h2 + 16 * qb + j <= jmax) *w = cv[16 * qb + j] - __uint_as_float(v[j]);
+          for (int j = 0; j < 16; j++, wp += ti.ld)
+            if (32 * h2 + 16 * qb + j <= jmax) *wp = cv[16 * qb + j] - __uint_as_float(v[j]);
         }
       }
       if (!ok) break;
