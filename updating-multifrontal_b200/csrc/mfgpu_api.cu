@@ -514,8 +514,13 @@ struct mfgpu_handle {
   // Mixed path: levels of large fronts run the cooperative kernel one outer
   // panel at a time (diagonal blocks, panel solves and in-panel updates) and
   // the trailing update of each panel on the tensor cores.
+  // A level also goes to the tensor cores with fronts of a quarter of tcMinN
+  // when it has at least one front per SM (enough tiles to fill the GPU; 3D
+  // 127^3 level 3: 512 fronts, N <= 1981); levels with a few such fronts (the
+  // top of a 2D tree) stay on the cooperative kernel, which is faster there.
   bool tcLevel(const Plan::Level& L) const {
-    return tcMinN > 0 && L.maxN >= tcMinN && L.nf <= mfgpu::tc_max_fronts();
+    if (tcMinN <= 0 || L.nf > mfgpu::tc_max_fronts()) return false;
+    return L.maxN >= tcMinN || (L.nf >= 148 && L.maxN >= tcMinN / 4);
   }
 
   // Tensor-core level (mixed path).  Per 512-column outer panel [K, K + 512):
