@@ -1292,6 +1292,14 @@ void smemFor(int maxN, int nrhs, size_t elem, size_t& sm, int& use) {
 }
 }  // namespace
 
+// Threads per CTA of the per-front sweeps: enough warps for the level's
+// largest front (a thread per row below the diagonal block, a warp per column
+// of the block), at least two and at most ST.  Small fronts (the leaves of a
+// batch of thousands of them) then leave room for more CTAs per SM; every
+// value is computed by the same operations in the same order whatever the
+// block size, so results do not depend on it.
+inline int sweep_threads(int maxN) { return std::min(ST, std::max(64, (maxN + 31) & ~31)); }
+
 template <class T>
 void launch_solve_fwd(const int* flist, int nf, int maxN, const FrontDev* fr, const T* F,
                       const int* dofs, T* X, int64_t ldx, int nrhs, T* W, const int64_t* woff,
@@ -1300,6 +1308,7 @@ void launch_solve_fwd(const int* flist, int nf, int maxN, const FrontDev* fr, co
   size_t sm;
   int use;
   smemFor(maxN, nrhs, sizeof(T), sm, use);
+  const int threads = sweep_threads(maxN);
 #define MFGPU_FWD(NR)                                                                          \
   do {                                                                                         \
     static const bool attr_ = (cudaFuncSetAttribute(k_solve_fwd<T, NR>,                     \
@@ -1307,7 +1316,7 @@ void launch_solve_fwd(const int* flist, int nf, int maxN, const FrontDev* fr, co
                                                     kSolveSmemBytes),                             \
                                true);                                                             \
     (void)attr_;                                                                                  \
-    k_solve_fwd<T, NR><<<nf, ST, sm, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff, use);    \
+    k_solve_fwd<T, NR><<<nf, threads, sm, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff, use);\
   } while (0)
   if (nrhs == 1) MFGPU_FWD(1);
   else if (nrhs <= 4) MFGPU_FWD(4);
@@ -1325,6 +1334,7 @@ void launch_solve_bwd(const int* flist, int nf, int maxN, const FrontDev* fr, co
   size_t sm;
   int use;
   smemFor(maxN, nrhs, sizeof(T), sm, use);
+  const int threads = sweep_threads(maxN);
 #define MFGPU_BWD(NR)                                                                          \
   do {                                                                                         \
     static const bool attr_ = (cudaFuncSetAttribute(k_solve_bwd<T, NR>,                     \
@@ -1332,7 +1342,7 @@ void launch_solve_bwd(const int* flist, int nf, int maxN, const FrontDev* fr, co
                                                     kSolveSmemBytes),                             \
                                true);                                                             \
     (void)attr_;                                                                                  \
-    k_solve_bwd<T, NR><<<nf, ST, sm, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff, use);    \
+    k_solve_bwd<T, NR><<<nf, threads, sm, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff, use);\
   } while (0)
   if (nrhs == 1) MFGPU_BWD(1);
   else if (nrhs <= 4) MFGPU_BWD(4);
