@@ -211,6 +211,21 @@ int mfgpu_solve_device_noalloc(mfgpu_handle* h, const double* d_b, double* d_x, 
  * the handle's own stream. */
 int mfgpu_set_stream(mfgpu_handle* h, void* cuda_stream);
 
+/* Factor serialisation (no counterpart in the reference, whose factorization
+ * lives in process memory only; survey row "next 3": restart a serving loop
+ * without refactoring).  mfgpu_save writes a factored handle's state - front
+ * and separator arenas, CSR values, the mixed path's scaling, the cooperative
+ * sweeps' block inverses - to `path` with a header describing the problem and
+ * a checksum of the payload.  mfgpu_load restores it into a handle created
+ * for the same problem (same schedule sizes, precision and sparsity pattern);
+ * the handle is then factored: Solve, Apply and Update need no Factor().  A
+ * file that does not match the handle, or whose checksum fails, is rejected
+ * with MFGPU_ERR_ARG (after a failed checksum the handle is left unfactored).
+ * Saving an unfactored handle returns MFGPU_ERR_STATE.  Not for the serving
+ * loop's per-slot views. */
+int mfgpu_save(mfgpu_handle* h, const char* path);
+int mfgpu_load(mfgpu_handle* h, const char* path);
+
 /* Per-kernel-class device timing (no reference counterpart; the reference's
  * HASCPP11TIMING millisecond counters, src/DE/mf2d.cpp:15-18, 464-499, are the
  * closest).  When enabled, every launch group is bracketed by CUDA events on

@@ -1488,6 +1488,150 @@ int mfgpu_set_stream(mfgpu_handle* h, void* st) {
   });
 }
 
+namespace {
+
+// Factor file: FacHeader, the payload blocks of facBlocks in order, then a
+// 64-bit FNV-1a checksum of the payload (taken 8 bytes at a time).
+struct FacHeader {
+  char magic[8];
+  uint32_t version, esz, mixed, pad;
+  int64_t n, nnz, front_elems, sep_elems, dinv_elems, nfronts, nseps;
+  uint64_t pattern;   // checksum of row_ptr and col_ind
+};
+constexpr char kFacMagic[8] = {'M', 'F', 'G', 'P', 'U', 'F', 'A', 'C'};
+constexpr uint32_t kFacVersion = 1;
+constexpr uint64_t kFnvBasis = 1469598103934665603ull, kFnvPrime = 1099511628211ull;
+
+uint64_t fnv64(uint64_t h, const unsigned char* p, size_t bytes) {
+  size_t i = 0;
+  for (; i + 8 <= bytes; i += 8) {
+    uint64_t w;
+    std::memcpy(&w, p + i, 8);
+    h = (h ^ w) * kFnvPrime;
+  }
+  for (; i < bytes; i++) h = (h ^ p[i]) * kFnvPrime;
+  return h;
+}
+
+FacHeader facHeader(const mfgpu_handle* h) {
+  FacHeader f;
+  std::memset(&f, 0, sizeof f);
+  std::memcpy(f.magic, kFacMagic, 8);
+  f.version = kFacVersion;
+  f.esz = (uint32_t)h->esz;
+  f.mixed = h->mixed ? 1 : 0;
+  f.n = h->n;
+  f.nnz = h->nnz;
+  f.front_elems = h->S->front_elems;
+  f.sep_elems = h->S->sep_elems;
+  f.dinv_elems = h->dinvElems;
+  f.nfronts = (int64_t)h->S->fronts.size();
+  f.nseps = (int64_t)h->S->seps.size();
+  uint64_t c = fnv64(kFnvBasis, (const unsigned char*)h->h_rowptr.data(), h->h_rowptr.size() * 4);
+  f.pattern = fnv64(c, (const unsigned char*)h->h_colind.data(), h->h_colind.size() * 4);
+  return f;
+}
+
+// The device arrays that make up a factored handle, in file order.
+std::vector<std::pair<void*, size_t>> facBlocks(const mfgpu_handle* h) {
+  std::vector<std::pair<void*, size_t>> b = {{h->d_F, (size_t)h->S->front_elems * h->esz},
+                                             {h->d_Sep, (size_t)h->S->sep_elems * h->esz},
+                                             {h->d_val, (size_t)h->nnz * sizeof(double)}};
+  if (h->mixed) {
+    b.push_back({h->d_scale, (size_t)h->n * sizeof(double)});
+    b.push_back({h->d_iscale, (size_t)h->n * sizeof(double)});
+  }
+  if (h->dinvElems > 0) b.push_back({h->d_Dinv, (size_t)h->dinvElems * h->esz});
+  return b;
+}
+
+struct FileCloser {
+  void operator()(FILE* f) const {
+    if (f) fclose(f);
+  }
+};
+
+constexpr size_t kFacChunk = (size_t)64 << 20;   // host bounce buffer
+
+}  // namespace
+
+int mfgpu_save(mfgpu_handle* h, const char* path) {
+  if (!h) return MFGPU_ERR_ARG;
+  if (!path) return fail(h, MFGPU_ERR_ARG, "null path");
+  if (h->view) return fail(h, MFGPU_ERR_ARG, "a serving-loop view cannot be saved");
+  if (!h->factored) return fail(h, MFGPU_ERR_STATE, "save before a successful Factor()");
+  return guarded(h, [&]() {
+    ck(cudaStreamSynchronize(h->stream), "sync before save");
+    std::unique_ptr<FILE, FileCloser> f(fopen(path, "wb"));
+    if (!f) throw CudaError(std::string("cannot open ") + path + " for writing", MFGPU_ERR_ARG);
+    const FacHeader hd = facHeader(h);
+    if (fwrite(&hd, sizeof hd, 1, f.get()) != 1)
+      throw CudaError(std::string("write failed: ") + path, MFGPU_ERR_ARG);
+    std::vector<unsigned char> buf;
+    uint64_t sum = kFnvBasis;
+    for (const auto& blk : facBlocks(h)) {
+      for (size_t o = 0; o < blk.second; o += kFacChunk) {
+        const size_t len = std::min(kFacChunk, blk.second - o);
+        buf.resize(len);
+        ck(cudaMemcpy(buf.data(), (const unsigned char*)blk.first + o, len, cudaMemcpyDeviceToHost),
+           "copy factor to host");
+        sum = fnv64(sum, buf.data(), len);
+        if (fwrite(buf.data(), 1, len, f.get()) != len)
+          throw CudaError(std::string("write failed: ") + path, MFGPU_ERR_ARG);
+      }
+    }
+    if (fwrite(&sum, sizeof sum, 1, f.get()) != 1 || fflush(f.get()) != 0)
+      throw CudaError(std::string("write failed: ") + path, MFGPU_ERR_ARG);
+  });
+}
+
+int mfgpu_load(mfgpu_handle* h, const char* path) {
+  if (!h) return MFGPU_ERR_ARG;
+  if (!path) return fail(h, MFGPU_ERR_ARG, "null path");
+  if (h->view) return fail(h, MFGPU_ERR_ARG, "a serving-loop view cannot be loaded into");
+  return guarded(h, [&]() {
+    std::unique_ptr<FILE, FileCloser> f(fopen(path, "rb"));
+    if (!f) throw CudaError(std::string("cannot open ") + path, MFGPU_ERR_ARG);
+    FacHeader hd;
+    if (fread(&hd, sizeof hd, 1, f.get()) != 1 || std::memcmp(hd.magic, kFacMagic, 8) != 0 ||
+        hd.version != kFacVersion)
+      throw CudaError(std::string(path) + " is not a factor file of this library version",
+                      MFGPU_ERR_ARG);
+    const FacHeader me = facHeader(h);
+    const char* what = hd.esz != me.esz || hd.mixed != me.mixed ? "precision"
+                       : hd.n != me.n || hd.nnz != me.nnz || hd.pattern != me.pattern
+                           ? "matrix size or sparsity pattern"
+                       : hd.front_elems != me.front_elems || hd.sep_elems != me.sep_elems ||
+                               hd.dinv_elems != me.dinv_elems || hd.nfronts != me.nfronts ||
+                               hd.nseps != me.nseps
+                           ? "elimination-tree schedule"
+                           : nullptr;
+    if (what)
+      throw CudaError(std::string("factor file ") + path + " does not match this handle (" + what + ")",
+                      MFGPU_ERR_ARG);
+    ck(cudaStreamSynchronize(h->stream), "sync before load");
+    h->factored = false;
+    std::vector<unsigned char> buf;
+    uint64_t sum = kFnvBasis;
+    for (const auto& blk : facBlocks(h)) {
+      for (size_t o = 0; o < blk.second; o += kFacChunk) {
+        const size_t len = std::min(kFacChunk, blk.second - o);
+        buf.resize(len);
+        if (fread(buf.data(), 1, len, f.get()) != len)
+          throw CudaError(std::string("factor file ") + path + " is truncated", MFGPU_ERR_ARG);
+        sum = fnv64(sum, buf.data(), len);
+        ck(cudaMemcpy((unsigned char*)blk.first + o, buf.data(), len, cudaMemcpyHostToDevice),
+           "copy factor to device");
+      }
+    }
+    uint64_t want = 0;
+    if (fread(&want, sizeof want, 1, f.get()) != 1 || want != sum)
+      throw CudaError(std::string("factor file ") + path + " fails its checksum", MFGPU_ERR_ARG);
+    h->stats = mfgpu_stats{};
+    h->factored = true;
+  });
+}
+
 int mfgpu_get_info(const mfgpu_handle* h, mfgpu_info* info) {
   if (!h || !info) return MFGPU_ERR_ARG;
   const Schedule& s = *h->S;

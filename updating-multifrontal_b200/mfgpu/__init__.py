@@ -11,6 +11,7 @@ bad arguments raise ValueError.  All compute runs in libmfgpu.so on the GPU;
 there is no CPU path.
 """
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -180,6 +181,15 @@ class _MFBase:
             self._h, C.c_void_p(coef_ptr), _lib._ptr(hh), _lib._ptr(lo3), _lib._ptr(hi3),
             C.c_void_p(val_ptr), _lib._ptr(out), len(out), C.byref(cnt)))
         return out[:cnt.value]
+
+    def save(self, path):
+        """Write the factorization to a file (mfgpu_save); load() restores it
+        into a handle built for the same problem, with no Factor() needed."""
+        self._check(self._lib.mfgpu_save(self._h, os.fsencode(path)))
+
+    def load(self, path):
+        """Restore a factorization written by save() (mfgpu_load)."""
+        self._check(self._lib.mfgpu_load(self._h, os.fsencode(path)))
 
     def set_stream(self, stream_ptr):
         self._check(self._lib.mfgpu_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
