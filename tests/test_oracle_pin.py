@@ -94,3 +94,46 @@ def test_live_reference_front_blocks(tmp_path):
                 if v is None or R[p + nm].size == 0:
                     continue
                 assert np.abs(R[p + nm] - v).max() <= 1e-12 * max(1.0, np.abs(v).max())
+
+
+WIDE_CASES = [(2, (23, 19), 2, 4), (2, (30, 27), 3, 5), (2, (64, 40), 2, 6),
+              (3, (11, 9, 13), 2, 3), (3, (15, 15, 15), 3, 4)]
+
+
+@pytest.mark.skipif(not refio.have_reference(), reason="reference harness not built")
+@pytest.mark.parametrize("dim,N,w,ms", WIDE_CASES)
+def test_wide_stencils_oracle_and_schedule_match_reference(dim, N, w, ms, tmp_path):
+    """Separator widths 2 and 3 (the fixture's 9-/13-point 2D and 13-/19-point
+    3D stencils): the oracle's DOF lists and solution, and the C++ schedule's
+    DOF lists, against the reference run live on the same inputs."""
+    from mfgpu import Symbolic
+    a = stencil.loguniform_coefficients(N, 0.5, 2.0, 11, width=w)
+    A = stencil.build_laplacian(a, width=w)
+    rhs = np.random.default_rng(3).uniform(-1, 1, (1, A.n))
+    R = refio.run_reference(str(tmp_path), dim, N, w, ms, a, None, rhs)
+    L = int(R["levels"][0])
+    O = mf_oracle.MFOracle(A.to_scipy(), N, w, ms)
+    O.factor()
+    S = Symbolic(dim, N, w, ms)
+    assert O.levels == L and S.levels == L
+    f = k = 0
+    for ell in range(L):
+        nb = len([x for x in R if x.startswith(f"box.{ell}.") and x.endswith(".int")])
+        assert len(O.boxes[ell]) == nb
+        for b in range(nb):
+            ints, bds = R[f"box.{ell}.{b}.int"], R[f"box.{ell}.{b}.bd"]
+            assert np.array_equal(O.boxes[ell][b].int, ints) and np.array_equal(O.boxes[ell][b].bd, bds)
+            F = S.front(f)
+            f += 1
+            assert (F["level"], F["box"]) == (ell, b)
+            assert np.array_equal(F["dofs"][:F["n"]], ints) and np.array_equal(F["dofs"][F["n"]:], bds)
+        if ell >= 1:
+            ns = len([x for x in R if x.startswith(f"sep.{ell}.") and x.endswith(".dofs")])
+            for e in range(ns):
+                dofs = R[f"sep.{ell}.{e}.dofs"]
+                assert np.array_equal(O.seps[ell][e].dofs, dofs)
+                s = S.sep(k)
+                k += 1
+                assert (s["level"], s["idx"]) == (ell, e) and np.array_equal(s["dofs"], dofs)
+    x, xr = O.solve(rhs[0]), R["f1.solve.0"]
+    assert np.linalg.norm(x - xr) <= 1e-13 * np.linalg.norm(xr)
