@@ -1,0 +1,21 @@
+"""Host-only check of the tensor-core update's tile bookkeeping
+(csrc/kernels_tc.cu): tiles per front, tile-index decoding and pack capacity
+against a brute-force enumeration, compiled with nvcc and run on the CPU."""
+import os
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.mark.skipif(shutil.which("nvcc") is None, reason="nvcc not found")
+def test_tile_enumeration_matches_brute_force(tmp_path):
+    exe = str(tmp_path / "tc_geometry")
+    subprocess.run(["nvcc", "-std=c++17", "-O1", "-gencode", "arch=compute_100a,code=sm_100a",
+                    os.path.join(ROOT, "tests", "cpp", "tc_geometry.cu"), "-o", exe],
+                   check=True, capture_output=True, text=True, timeout=600)
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.startswith("ok")

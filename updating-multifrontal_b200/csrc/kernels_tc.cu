@@ -114,7 +114,7 @@ __host__ __device__ inline int geo_tiles(const PanelGeo& g) {
   return g.nj * (g.nj + 1) + (g.nb - 2 * g.nj) * g.nj;
 }
 
-__device__ __forceinline__ void tile_ij(int t, int nj, int& I, int& J) {
+__host__ __device__ inline void tile_ij(int t, int nj, int& I, int& J) {
   const int tri = nj * (nj + 1);
   if (t < tri) {
     int p = (int)((sqrt(4.0 * t + 1.0) - 1.0) * 0.5);
