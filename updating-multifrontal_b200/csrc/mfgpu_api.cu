@@ -289,6 +289,7 @@ struct mfgpu_handle {
   int* d_all = nullptr;      // every front id then every separator id, level order
   int64_t woffTotal = 0;     // sum over fronts of 2N
   Plan full, upd;
+  std::vector<int> tuned;    // per level of the full plan: kernel picked by mfgpu_autotune, or -1
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int64_t device_bytes = 0;
   Profiler prof;
@@ -388,7 +389,9 @@ struct mfgpu_handle {
       L.sadd0 = P.addGroup(s.sep_add_tasks, s.sep_task_ptr, sl, 0);
       L.sadd1 = P.addGroup(s.sep_add_tasks, s.sep_task_ptr, sl, 1);
       L.cpref0 = (int64_t)P.cpref.size();
-      if (!fl.empty() && !useFused((int)fl.size(), L.maxN) && mfgpu::coop_fits((int)fl.size())) {
+      // phase tables for every level the cooperative kernel can take (also the
+      // ones the size rules give to k_front_small: the autotuner may not)
+      if (!fl.empty() && mfgpu::coop_fits((int)fl.size())) {
         std::vector<int> nn, NN;
         for (int f : fl) {
           nn.push_back(s.fronts[f].n);
@@ -443,64 +446,186 @@ struct mfgpu_handle {
     return b;
   }
 
+  // Level kernels.  The size rules choose one per level; mfgpu_autotune can
+  // replace the choice for the levels of the full factorization by timing.
+  enum LevelKernel { LK_NONE = -1, LK_FUSED = 0, LK_COOP = 1, LK_TC = 2, LK_STEPPED = 3 };
+
+  int ruleKernel(const Plan::Level& L) const {
+    if (L.nf <= 0) return LK_NONE;
+    if (useFused((int)L.nf, L.maxN)) return LK_FUSED;
+    if (!mfgpu::coop_fits((int)L.nf) || (stepped && !mixed)) return LK_STEPPED;
+    if (mixed && tcLevel(L)) return LK_TC;
+    return LK_COOP;
+  }
+
+  int levelKernel(const Plan& P, const Plan::Level& L, int ell) const {
+    if (&P == &full && ell < (int)tuned.size() && tuned[ell] != LK_NONE && L.nf > 0)
+      return tuned[ell];
+    return ruleKernel(L);
+  }
+
+  // Kernels that can factor level L (autotuning candidates).
+  std::vector<int> levelCandidates(const Plan::Level& L) const {
+    std::vector<int> c;
+    if (L.nf <= 0) return c;
+    if (mfgpu::small_front_fits(L.maxN, (int)esz)) c.push_back(LK_FUSED);
+    if (mfgpu::coop_fits((int)L.nf) && !(stepped && !mixed)) {
+      c.push_back(LK_COOP);
+      if (mixed && L.nf <= mfgpu::tc_max_fronts() && L.maxN >= 1024) c.push_back(LK_TC);
+    }
+    if (c.empty()) c.push_back(ruleKernel(L));
+    return c;
+  }
+
+  // Panel-pack bytes a tensor-core run of level L needs (outer panels only when
+  // the level was planned without sub-panels).
+  size_t levelPackBytes(const Plan& P, const Plan::Level& L) const {
+    std::vector<int> nn, NN;
+    for (int64_t i = L.f0; i < L.f0 + L.nf; i++) {
+      nn.push_back(S->fronts[P.ids[i]].n);
+      NN.push_back(S->fronts[P.ids[i]].N);
+    }
+    size_t b = 0;
+    const int W = mfgpu::tc_outer(), w = L.coopOuter > 0 ? L.coopOuter : W;
+    for (int K = 0; K < L.maxn; K += w)
+      for (int ww : {w, W})
+        if (K % ww == 0)
+          b = std::max(b, mfgpu::tc_pack_bytes((int)L.nf, mfgpu::tc_pack_cap(nn, NN, K, ww)));
+    return b;
+  }
+
+  void ensurePack(size_t bytes) {
+    if (bytes <= tcPackCap) return;
+    ck(cudaStreamSynchronize(stream), "sync before growing the panel pack");
+    cudaFree(d_tcpack);
+    d_tcpack = nullptr;
+    tcPackCap = 0;
+    d_tcpack = dalloc<unsigned char>(bytes, "alloc tensor-core panel pack");
+    tcPackCap = bytes;
+  }
+
+  // Partial factorization of the fronts of level ell with kernel `kind`.
+  template <class T>
+  void runLevelKernel(const Plan& P, const Plan::Level& L, int ell, int kind) {
+    const Schedule& s = *S;
+    T* F = (T*)d_F;
+    double fl = 0;
+    if (prof.on && kind != LK_STEPPED)
+      for (int64_t i = L.f0; i < L.f0 + L.nf; i++) fl += s.front_flops(s.fronts[P.ids[i]]);
+    if (kind == LK_FUSED) {
+      prof.flops[MFGPU_KC_FRONT] += fl;
+      prof.begin(MFGPU_KC_FRONT, stream);
+      mfgpu::launch_front_small<T>(P.d_ids + L.f0, (int)L.nf, L.maxN, d_fr, F, d_err, stream);
+      ck(cudaGetLastError(), "launch fused front factorization (k_front_small)");
+      prof.end(stream);
+    } else if (kind == LK_TC) {
+      if (sizeof(T) != sizeof(float)) throw CudaError("tensor-core levels are mixed only", MFGPU_ERR_ARG);
+      runTensorLevel(P, L, fl, ell);
+    } else if (kind == LK_COOP) {
+      prof.flops[MFGPU_KC_COOP] += fl;
+      prof.begin(MFGPU_KC_COOP, stream);
+      ck(mfgpu::launch_level_coop<T>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, F, d_err,
+                                     (T*)d_slots, P.d_cpref + L.cpref0, d_gbar, stream, 0, -1, 0,
+                                     1, L.coopItems, L.coopOuter),
+         "launch cooperative level factorization (k_level_coop)");
+      prof.end(stream);
+    } else if (kind == LK_STEPPED) {
+      if (sizeof(T) != sizeof(double))
+        throw CudaError("no single-precision path for this level", MFGPU_ERR_ARG);
+      runStepped(P, L);
+    }
+  }
+
   // Run a factorization plan: per level, separator base assembly, front
   // assembly, partial Cholesky, separator accumulation (src/DE/mf2d.cpp:449-753).
   template <class T>
   void runPlanT(const Plan& P) {
     const Schedule& s = *S;
     T* F = (T*)d_F;
-    if (P.tcPackBytes > tcPackCap) {   // grows once, on the first plan that needs more
-      ck(cudaStreamSynchronize(stream), "sync before growing the panel pack");
-      cudaFree(d_tcpack);
-      d_tcpack = nullptr;
-      tcPackCap = 0;
-      d_tcpack = dalloc<unsigned char>(P.tcPackBytes, "alloc tensor-core panel pack");
-      tcPackCap = P.tcPackBytes;
-    }
+    size_t pack = P.tcPackBytes;   // tuned tensor-core levels may need more than the rules
+    if (&P == &full)
+      for (int ell = 0; ell < s.levels && ell < (int)tuned.size(); ell++)
+        if (tuned[ell] == LK_TC) pack = std::max(pack, levelPackBytes(P, P.lv[ell]));
+    ensurePack(pack);
     ck(cudaMemsetAsync(d_err, 0, sizeof(DevError), stream), "clear error word");
     for (int ell = s.levels - 1; ell >= 0; ell--) {
       const Plan::Level& L = P.lv[ell];
       prof.level = ell;
       runGroup<T>(P, L.sbase, groupBytes(P, L.sbase));
       runGroup<T>(P, L.ftask, groupBytes(P, L.ftask));
-      const bool fused = L.nf > 0 && useFused((int)L.nf, L.maxN);
-      const bool coop = L.nf > 0 && !fused && mfgpu::coop_fits((int)L.nf) &&
-                        (!stepped || sizeof(T) != sizeof(double));
-      if (fused || coop) {
-        double fl = 0;
-        if (prof.on)
-          for (int64_t i = L.f0; i < L.f0 + L.nf; i++) fl += s.front_flops(s.fronts[P.ids[i]]);
-        if (fused) {
-          prof.flops[MFGPU_KC_FRONT] += fl;
-          prof.begin(MFGPU_KC_FRONT, stream);
-          mfgpu::launch_front_small<T>(P.d_ids + L.f0, (int)L.nf, L.maxN, d_fr, F, d_err, stream);
-          ck(cudaGetLastError(), "launch fused front factorization (k_front_small)");
-          prof.end(stream);
-        } else if (sizeof(T) == sizeof(float) && tcLevel(L)) {
-          runTensorLevel(P, L, fl, ell);
-        } else {
-          prof.flops[MFGPU_KC_COOP] += fl;
-          prof.begin(MFGPU_KC_COOP, stream);
-          ck(mfgpu::launch_level_coop<T>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, F, d_err,
-                                         (T*)d_slots, P.d_cpref + L.cpref0, d_gbar, stream, 0, -1,
-                                         0, 1, L.coopItems),
-             "launch cooperative level factorization (k_level_coop)");
-          prof.end(stream);
-        }
-      } else if (L.nf > 0) {
-        if (sizeof(T) != sizeof(double))
-          throw CudaError("no single-precision path for this level", MFGPU_ERR_ARG);
-        runStepped(P, L);
-      }
-      if (L.nf > 0 && coopSweep(ell)) {   // block inverses for the cooperative sweeps
-        mfgpu::launch_diag_inv<T>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, F, (T*)d_Dinv,
-                                  d_dinv_off, stream);
-        ck(cudaGetLastError(), "launch diagonal-block inverses (k_diag_inv)");
-      }
-      runGroup<T>(P, L.sadd0, groupBytes(P, L.sadd0));
-      runGroup<T>(P, L.sadd1, groupBytes(P, L.sadd1));
+      runLevelKernel<T>(P, L, ell, levelKernel(P, L, ell));
+      finishLevel<T>(P, L, ell);
     }
     ck(cudaGetLastError(), "factor launch");
+  }
+
+  // After a level's partial factorization: the cooperative sweeps' block
+  // inverses, then the separator accumulation.
+  template <class T>
+  void finishLevel(const Plan& P, const Plan::Level& L, int ell) {
+    if (L.nf > 0 && coopSweep(ell)) {
+      mfgpu::launch_diag_inv<T>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, (T*)d_F, (T*)d_Dinv,
+                                d_dinv_off, stream);
+      ck(cudaGetLastError(), "launch diagonal-block inverses (k_diag_inv)");
+    }
+    runGroup<T>(P, L.sadd0, groupBytes(P, L.sadd0));
+    runGroup<T>(P, L.sadd1, groupBytes(P, L.sadd1));
+  }
+
+  // Full factorization that also picks each level's kernel by timing: per
+  // level, every candidate runs `reps` times on freshly assembled fronts (the
+  // assembly rewrites every front element, as localized updates rely on) and
+  // the fastest becomes the level's kernel for later full factorizations; the
+  // level is then assembled and factored once more with it.
+  template <class T>
+  void autotuneT(int reps, int* choices) {
+    const Schedule& s = *S;
+    const Plan& P = full;
+    tuned.assign(s.levels, LK_NONE);
+    size_t pack = P.tcPackBytes;
+    for (int ell = 0; ell < s.levels; ell++)
+      for (int c : levelCandidates(P.lv[ell]))
+        if (c == LK_TC) pack = std::max(pack, levelPackBytes(P, P.lv[ell]));
+    ensurePack(pack);
+    if (mixed) {
+      mfgpu::launch_diag_scale(d_rp, d_ci, d_val, n, d_scale, d_iscale, stream);
+      ck(cudaGetLastError(), "launch diagonal scaling");
+    }
+    ck(cudaMemsetAsync(d_err, 0, sizeof(DevError), stream), "clear error word");
+    const bool prof_on = prof.on;
+    prof.on = false;
+    for (int ell = s.levels - 1; ell >= 0; ell--) {
+      const Plan::Level& L = P.lv[ell];
+      runGroup<T>(P, L.sbase, groupBytes(P, L.sbase));
+      const std::vector<int> cand = levelCandidates(L);
+      if (cand.size() > 1) {
+        float best = 0;
+        for (int c : cand) {
+          float t = 0;
+          for (int r = 0; r < std::max(1, reps); r++) {
+            runGroup<T>(P, L.ftask, groupBytes(P, L.ftask));
+            ck(cudaEventRecord(ev0, stream), "event");
+            runLevelKernel<T>(P, L, ell, c);
+            ck(cudaEventRecord(ev1, stream), "event");
+            ck(cudaEventSynchronize(ev1), "autotune sync");
+            float ms = 0;
+            ck(cudaEventElapsedTime(&ms, ev0, ev1), "elapsed");
+            t = r == 0 ? ms : std::min(t, ms);
+          }
+          if (tuned[ell] == LK_NONE || t < best) {
+            tuned[ell] = c;
+            best = t;
+          }
+        }
+      }
+      runGroup<T>(P, L.ftask, groupBytes(P, L.ftask));
+      runLevelKernel<T>(P, L, ell, levelKernel(P, L, ell));
+      finishLevel<T>(P, L, ell);
+    }
+    prof.on = prof_on;
+    ck(cudaGetLastError(), "factor launch");
+    if (choices)
+      for (int ell = 0; ell < s.levels; ell++) choices[ell] = levelKernel(P, P.lv[ell], ell);
   }
 
   // One CTA per front (k_front_small) when the level has enough fronts to fill
@@ -1205,6 +1330,23 @@ static int factorImpl(mfgpu_handle* h, const double* val, int64_t nnz, bool devi
 }
 
 int mfgpu_factor(mfgpu_handle* h) { return factorImpl(h, nullptr, 0, false); }
+
+int mfgpu_autotune(mfgpu_handle* h, int reps, int* choices) {
+  if (!h) return MFGPU_ERR_ARG;
+  if (h->view) return fail(h, MFGPU_ERR_ARG, "a serving-loop view cannot be autotuned");
+  if (reps < 1 || reps > 100) return fail(h, MFGPU_ERR_ARG, "reps must be in [1, 100]");
+  return guarded(h, [&]() {
+    h->factored = false;
+    ck(cudaEventRecord(h->ev0, h->stream), "event");
+    if (h->mixed) h->autotuneT<float>(reps, choices);
+    else h->autotuneT<double>(reps, choices);
+    h->checkDevError();
+    h->stats = mfgpu_stats{};
+    h->stats.flops = h->full.flops;
+    h->stats.fronts = h->full.nfronts;
+    h->factored = true;
+  });
+}
 int mfgpu_refactor(mfgpu_handle* h, const double* val, int64_t nnz) {
   if (!val) return fail(h, MFGPU_ERR_ARG, "null values");
   return factorImpl(h, val, nnz, false);

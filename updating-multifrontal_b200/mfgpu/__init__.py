@@ -191,6 +191,16 @@ class _MFBase:
         """Restore a factorization written by save() (mfgpu_load)."""
         self._check(self._lib.mfgpu_load(self._h, os.fsencode(path)))
 
+    LEVEL_KERNELS = {-1: "none", 0: "fused", 1: "coop", 2: "tc", 3: "stepped"}
+
+    def autotune(self, reps=2):
+        """Full factorization that times each level's eligible kernels and keeps
+        the fastest for later full factorizations (mfgpu_autotune).  Returns
+        the kernel chosen per level, root first."""
+        out = np.zeros(self.info()["levels"], np.int32)
+        self._check(self._lib.mfgpu_autotune(self._h, int(reps), _lib._ptr(out)))
+        return [self.LEVEL_KERNELS[int(k)] for k in out]
+
     def set_stream(self, stream_ptr):
         self._check(self._lib.mfgpu_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
 

@@ -33,7 +33,7 @@ EXPORTED = [
     "mfgpu_symbolic_dirty", "mfgpu_batch_create", "mfgpu_batch_info",
     "mfgpu_symbolic_batch_create", "mfgpu_stencil_assemble_device", "mfgpu_stencil_update_device",
     "mfgpu_server_create", "mfgpu_server_submit", "mfgpu_server_wait", "mfgpu_server_last_error",
-    "mfgpu_server_destroy", "mfgpu_save", "mfgpu_load",
+    "mfgpu_server_destroy", "mfgpu_save", "mfgpu_load", "mfgpu_autotune",
 ]
 
 KERNEL_CLASSES = ["assemble", "potrf", "trsm", "syrk", "solve", "apply", "front", "coop", "tc"]
@@ -123,6 +123,8 @@ def load(path=None):
     lib.mfgpu_save.restype = C.c_int
     lib.mfgpu_load.argtypes = [P, C.c_char_p]
     lib.mfgpu_load.restype = C.c_int
+    lib.mfgpu_autotune.argtypes = [P, C.c_int, C.c_void_p]
+    lib.mfgpu_autotune.restype = C.c_int
     lib.mfgpu_set_stream.restype = C.c_int
     lib.mfgpu_get_info.argtypes = [P, C.POINTER(Info)]
     lib.mfgpu_get_info.restype = C.c_int
