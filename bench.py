@@ -622,6 +622,9 @@ def main():
     ap.add_argument("--no-compare", action="store_true",
                     help="skip timing the other precision for the mixed-vs-FP64 comparison")
     ap.add_argument("--json-out", default=None)
+    ap.add_argument("--autotune", type=int, default=0, metavar="REPS",
+                    help="pick each level's kernel by timing (mfgpu_autotune, REPS runs per "
+                         "candidate) during set-up, before the warm-up; 0 = size rules")
     ap.add_argument("--rate", type=float, default=4.0, help="serving: arrivals per second")
     ap.add_argument("--requests", type=int, default=24, help="serving: requests in the stream")
     ap.add_argument("--slots", type=int, default=4, help="serving: concurrent requests")
@@ -651,6 +654,7 @@ def main():
     F.set_stream(stream.cuda_stream)
     work.to_device(torch)
     torch.cuda.synchronize()
+    tuned = work.F.autotune(args.autotune) if args.autotune > 0 else None   # set-up, untimed
     step = work.step
 
     for _ in range(max(3, args.warmup)):
@@ -755,6 +759,8 @@ def main():
     # the metric compares mixed precision with FP64: time the other precision
     # on the same workload (after releasing this handle's memory)
     config = work.config(args)
+    if tuned is not None:
+        config["autotune"] = {"reps": args.autotune, "level_kernels_root_first": tuned}
     flops_bd = work.flops_breakdown()
     iters = F.stats()["iterations"] if args.precision == "mixed" else 0
     comparison = None
@@ -764,6 +770,8 @@ def main():
         torch.cuda.empty_cache()
         other = MFGPU_FP64 if prec == MFGPU_MIXED else MFGPU_MIXED
         w2 = (BatchWork if w.get("batch") else SingleWork)(w, rank, local, other)
+        if args.autotune > 0:
+            w2.F.autotune(args.autotune)
         st2 = torch.cuda.Stream()
         w2.F.set_stream(st2.cuda_stream)
         w2.to_device(torch)
