@@ -201,24 +201,25 @@ def run_reference_arm(args, w):
     fl = front_sizes(w)
     factor_fl = sum(n ** 3 / 3.0 + n * n * m + n * m * m for n, m in fl)
     threads = os.cpu_count() or 1
-    # one warm-up sample, then `steps` samples; each sample = factor + update +
-    # nrhs solves of the full workload, bounded to a few minutes in total
+    # `warmup` untimed samples, then `steps` timed ones; each sample = factor +
+    # update + nrhs solves of the full workload
+    warm = max(1, args.warmup)
     upd_fl = update_flops(w, mod)
     sfl = solve_flops(fl, w["nrhs"])
-    res = reference_time(w, a1, a2, b, threads, reps=1 + max(1, args.steps), solve_reps=1)
+    res = reference_time(w, a1, a2, b, threads, reps=warm + max(1, args.steps), solve_reps=1)
     model, ncpu = cpu_info()
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable":
                           "reference harness oracle/_ref/ref_harness not built"}))
         return 0
-    tf, tu, ts = res["factor_s"][1:], res["update_s"][1:], res["solve_s"][1:]
+    tf, tu, ts = res["factor_s"][warm:], res["update_s"][warm:], res["solve_s"][warm:]
     steps = [tf[i] + tu[i] + ts[i] for i in range(len(tf))]
     step_fl = factor_fl + upd_fl + sfl
     t = statistics.median(steps)
     value = step_fl / t / 1e12
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s",
-        "n_gpus": args.gpus, "steps": len(steps), "warmup": 1, "ms_per_step": t * 1e3,
+        "n_gpus": args.gpus, "steps": len(steps), "warmup": warm, "ms_per_step": t * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32 factor + f64 refinement",
         "data": "synthetic (seeded coefficients and right-hand sides)",
@@ -250,7 +251,8 @@ def run_reference_arm_batch(args, w):
     threads = os.cpu_count() or 1
     cache = {}
     samples = []
-    for rep in range(1 + max(1, args.steps)):
+    warm = max(1, args.warmup)
+    for rep in range(warm + max(1, args.steps)):
         t_tot, fl_tot, used = 0.0, 0.0, 0
         for dim, N, ms, a, A, b in members:
             if t_tot > 20.0:
@@ -266,7 +268,7 @@ def run_reference_arm_batch(args, w):
             fl_tot += sum(n ** 3 / 3.0 + n * n * m + n * m * m for n, m in fr)
             fl_tot += solve_flops(fr, b.shape[0])
             used += 1
-        if rep > 0:
+        if rep >= warm:
             samples.append((t_tot, fl_tot, used))
     vals = [fl / t / 1e12 for t, fl, _ in samples]
     value = statistics.median(vals)
@@ -274,7 +276,7 @@ def run_reference_arm_batch(args, w):
     t_med = statistics.median([t for t, _, _ in samples])
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s",
-        "n_gpus": args.gpus, "steps": len(samples), "warmup": 1, "ms_per_step": t_med * 1e3,
+        "n_gpus": args.gpus, "steps": len(samples), "warmup": warm, "ms_per_step": t_med * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded coefficients and right-hand sides)",
         "config": {"workload": args.workload, "precision": args.precision,
