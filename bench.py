@@ -160,6 +160,22 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
+def whole_job(local_ms, local_flops, device):
+    """Replicas on N ranks: the job's time is the slowest rank's (max over
+    ranks) and its work the sum of every rank's algorithmic flops.  Returns
+    (TFLOP/s of the whole job, max ms, total flops); every rank gets the same
+    values.  One rank: its own."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(local_ms)], dtype=torch.float64, device=device)
+    f = torch.tensor([float(local_flops)], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(f, op=dist.ReduceOp.SUM)
+    ms, fl = float(t.item()), float(f.item())
+    return fl / (ms * 1e-3) / 1e12, ms, fl
+
+
 def reference_time(w, a1, a2, b, threads, reps=1, solve_reps=1, timeout=3000):
     """Run the compiled reference (oracle/_ref) in timing mode; returns its JSON."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -696,11 +712,7 @@ def main():
     F.profile(False)
     ms_total = e0.elapsed_time(e1)
     step_ms = [a.elapsed_time(c) for a, c in per_step]
-    t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * args.steps * step_fl / (ms_max * 1e-3) / 1e12
+    value, ms_max, _ = whole_job(ms_total, args.steps * step_fl, "cuda")
 
     # end to end through the public API with pinned host buffers
     work.e2e_setup(torch)
@@ -715,10 +727,7 @@ def main():
     ee1.record(stream)
     ee1.synchronize()
     e2e_ms = ee0.elapsed_time(ee1)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps * step_fl / (float(te.item()) * 1e-3) / 1e12
+    e2e_value, _, _ = whole_job(e2e_ms, args.steps * step_fl, "cuda")
     h2d, d2h = work.e2e_bytes()
 
     # roofline of the dominant kernel class in the timed region
