@@ -513,7 +513,7 @@ class BatchWork:
 
 
 def run_serve(args, w):
-    """Update serving (the survey's configuration 5): a stream of requests with
+    """Update serving (3D 95^3 base, the serving configuration): a stream of requests with
     Poisson arrivals against a resident factorization; each request changes
     the coefficients of one box and brings right-hand sides.  Reports
     throughput and p50/p99 latency (wall clock from submission to the result

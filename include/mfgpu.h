@@ -212,8 +212,8 @@ int mfgpu_solve_device_noalloc(mfgpu_handle* h, const double* d_b, double* d_x, 
 int mfgpu_set_stream(mfgpu_handle* h, void* cuda_stream);
 
 /* Factor serialisation (no counterpart in the reference, whose factorization
- * lives in process memory only; survey row "next 3": restart a serving loop
- * without refactoring).  mfgpu_save writes a factored handle's state - front
+ * lives in process memory only; use: restart a serving loop without
+ * refactoring its base).  mfgpu_save writes a factored handle's state - front
  * and separator arenas, CSR values, the mixed path's scaling, the cooperative
  * sweeps' block inverses - to `path` with a header describing the problem and
  * a checksum of the payload.  mfgpu_load restores it into a handle created
