@@ -156,6 +156,23 @@ def test_algorithm_model_matches_oracle(dim, N, ms, lib):
     assert np.linalg.norm(x - xo) <= 1e-13 * np.linalg.norm(xo)
 
 
+@pytest.mark.parametrize("dim,N,w,ms", [(2, (31, 31), 2, 4), (2, (30, 27), 3, 5),
+                                        (3, (11, 9, 13), 2, 3), (3, (15, 15, 15), 3, 4)])
+def test_algorithm_model_wide_stencils(dim, N, w, ms, lib):
+    """Separator widths 2 and 3: with uniform coefficients the fixture's wider
+    stencils are symmetric positive definite, and the schedule's task tables
+    executed with partial Cholesky solve them as the oracle does."""
+    A = stencil.build_laplacian(stencil.uniform_coefficients(N, w), width=w).to_scipy()
+    assert (A - A.T).nnz == 0
+    b = stencil.uniform_rhs(A.shape[0], 1, 9)[0]
+    S = Symbolic(dim, N, w, ms)
+    x = _model_solve(S, taskemu.Emu(S, A), b)
+    O = mf_oracle.MFOracle(A, N, w, ms)
+    O.factor()
+    xo = O.solve(b)
+    assert np.linalg.norm(x - xo) <= 1e-13 * np.linalg.norm(xo)
+
+
 @pytest.mark.parametrize("dim,N,ms,side", [(2, (127, 127), 4, 9), (3, (23, 23, 23), 4, 4)])
 def test_update_marks_root_paths(dim, N, ms, side, lib):
     a = stencil.loguniform_coefficients(N, 0.1, 10.0, 8)
