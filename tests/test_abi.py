@@ -5,6 +5,7 @@ import ctypes as C
 import os
 import re
 
+import numpy as np
 import pytest
 
 from mfgpu import Symbolic, _lib, stencil
@@ -57,3 +58,15 @@ def test_compute_without_device_fails_loudly():
     with pytest.raises(MFError) as ei:
         MF2D(A, 31, 31, 1, 4)
     assert ei.value.status == _lib.MFGPU_ERR_CUDA
+
+
+def test_nonsymmetric_matrix_rejected_before_any_device_work():
+    # the factorization reads the lower triangle only: a nonsymmetric matrix
+    # is refused at creation (on any machine, GPU or not)
+    A = stencil.build_laplacian(stencil.uniform_coefficients((31, 31)))
+    from mfgpu import MF2D
+    bad = stencil.CSR(A.row_ptr, A.col_ind, A.val.copy(), A.n)
+    off = np.flatnonzero(np.repeat(np.arange(A.n), np.diff(A.row_ptr)) != A.col_ind)[7]
+    bad.val[off] *= 1.01
+    with pytest.raises(ValueError, match="not symmetric"):
+        MF2D(bad, 31, 31, 1, 4)

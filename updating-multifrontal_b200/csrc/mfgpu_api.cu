@@ -1109,6 +1109,32 @@ int makeSchedule(int dim, int nx, int ny, int nz, int width, int max_side,
 int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const int* col_ind,
                const double* val, const mfgpu_options* opts, mfgpu_handle** out);
 
+// The factorization reads the lower triangle only, so a matrix that is not
+// symmetric would be factored as another one.  Returns why the CSR matrix is
+// not symmetric (entries (i, j) and (j, i) both stored and equal to a
+// relative 1e-12), or nullptr.  Rows need not be sorted.
+const char* asymmetry(int n, const int* rp, const int* ci, const double* val,
+                      std::string& where) {
+  for (int i = 0; i < n; i++) {
+    if (rp[i + 1] < rp[i]) return "row pointers decrease";
+    for (int p = rp[i]; p < rp[i + 1]; p++) {
+      const int j = ci[p];
+      if (j < 0 || j >= n) return "column index out of range";
+      if (j == i) continue;
+      int q = rp[j];
+      while (q < rp[j + 1] && ci[q] != i) q++;
+      const bool ok = q < rp[j + 1] && std::fabs(val[p] - val[q]) <=
+                                           1e-12 * std::max(std::fabs(val[p]), std::fabs(val[q]));
+      if (!ok) {
+        where = " (entries (" + std::to_string(i) + ", " + std::to_string(j) + ") and (" +
+                std::to_string(j) + ", " + std::to_string(i) + "))";
+        return "the matrix is not symmetric";
+      }
+    }
+  }
+  return nullptr;
+}
+
 }  // namespace
 
 int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side, int n,
@@ -1191,6 +1217,12 @@ int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const
   const Schedule& s = *h->S;
   if ((int64_t)n != s.ndof || row_ptr[0] != 0) {
     g_create_error = "matrix dimension does not match the grid";
+    return MFGPU_ERR_ARG;
+  }
+  std::string where;
+  if (const char* why = asymmetry(n, row_ptr, col_ind, val, where)) {
+    g_create_error = std::string(why) + where +
+                     ": this library factors symmetric positive definite matrices";
     return MFGPU_ERR_ARG;
   }
   h->n = n;
