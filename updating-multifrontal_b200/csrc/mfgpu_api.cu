@@ -1370,9 +1370,14 @@ int mfgpu_autotune(mfgpu_handle* h, int reps, int* choices) {
   return guarded(h, [&]() {
     h->factored = false;
     ck(cudaEventRecord(h->ev0, h->stream), "event");
-    if (h->mixed) h->autotuneT<float>(reps, choices);
-    else h->autotuneT<double>(reps, choices);
-    h->checkDevError();
+    try {   // a tuning that fails part-way leaves the size rules in force
+      if (h->mixed) h->autotuneT<float>(reps, choices);
+      else h->autotuneT<double>(reps, choices);
+      h->checkDevError();
+    } catch (...) {
+      h->tuned.clear();
+      throw;
+    }
     h->stats = mfgpu_stats{};
     h->stats.flops = h->full.flops;
     h->stats.fronts = h->full.nfronts;
