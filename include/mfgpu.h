@@ -278,6 +278,13 @@ void mfgpu_destroy(mfgpu_handle* h);
  * AddNew*Interactions_ (src/DE/mf2d.cpp:755-901). */
 int mfgpu_symbolic_create(int dim, int nx, int ny, int nz, int width, int max_side_length,
                           mfgpu_symbolic** out);
+/* The same with task tables for nonsymmetric matrices (every block of every
+ * front and separator, both triangles, as the reference's LU-based fronts
+ * hold them): the form the separator width 2-3 stencils of the reference
+ * fixture need with variable coefficients.  Host only; the GPU factorization
+ * stores lower triangles and does not use these tables. */
+int mfgpu_symbolic_create_full(int dim, int nx, int ny, int nz, int width, int max_side_length,
+                               mfgpu_symbolic** out);
 /* The forest schedule of a batch (see mfgpu_batch_create), host only. */
 int mfgpu_symbolic_batch_create(int count, const int* dim, const int* nx, const int* ny,
                                 const int* nz, const int* width, const int* max_side,

@@ -87,6 +87,17 @@ class Emu:
         view = self.F[off:off + ld * N].reshape(N, ld).T
         view[:N, :N] = np.tril(M)
 
+    def block_full(self, f):
+        """Front f as stored (both triangles; full-storage tables)."""
+        F = self.fronts[f]
+        N, ld, off = F["n"] + F["m"], F["ld"], F["off"]
+        return self.F[off:off + ld * N].reshape(N, ld).T[:N, :N].copy()
+
+    def set_block_full(self, f, M):
+        F = self.fronts[f]
+        N, ld, off = F["n"] + F["m"], F["ld"], F["off"]
+        self.F[off:off + ld * N].reshape(N, ld).T[:N, :N] = M
+
     def sep_block(self, k):
         s = self.seps[k]
         n, ld, off = s["size"], s["ld"], s["off"]

@@ -173,6 +173,77 @@ def test_algorithm_model_wide_stencils(dim, N, w, ms, lib):
     assert np.linalg.norm(x - xo) <= 1e-13 * np.linalg.norm(xo)
 
 
+def _model_solve_lu(S, E, b):
+    """Algorithm model for nonsymmetric matrices: full-storage tables + partial
+    LU with row pivoting inside each pivot block + solve sweeps (numpy)."""
+    fac = {}
+    for ell in range(S.levels - 1, -1, -1):
+        fl, sl = E.level_fronts(ell), E.level_seps(ell)
+        E.run(E.stasks, sl)
+        E.run(E.ftasks, fl)
+        for f in fl:
+            n = E.fronts[f]["n"]
+            M = E.block_full(f)
+            lu, piv = sla.lu_factor(M[:n, :n])
+            U = np.triu(lu)
+            L = np.tril(lu, -1) + np.eye(n)
+            M12 = M[:n, n:].copy()
+            for i, p in enumerate(piv):               # the row swaps of the pivot block
+                M12[[i, p]] = M12[[p, i]]
+            L21 = sla.solve_triangular(U, M[n:, :n].T, trans=1, lower=False).T
+            U12 = sla.solve_triangular(L, M12, lower=True, unit_diagonal=True)
+            M[n:, n:] -= L21 @ U12
+            E.set_block_full(f, M)
+            fac[f] = (lu, piv, L21, U12)
+        E.run(E.atasks[0::2], sl)
+        E.run(E.atasks[1::2], sl)
+    X, W, Fr = b.copy(), {}, E.fronts
+    for ell in range(S.levels - 1, 0, -1):
+        for f in E.level_fronts(ell):
+            n, d = Fr[f]["n"], Fr[f]["dofs"]
+            lu, piv, L21, U12 = fac[f]
+            y = X[d[:n]].copy()
+            for i, p in enumerate(piv):
+                y[[i, p]] = y[[p, i]]
+            y = sla.solve_triangular(lu, y, lower=True, unit_diagonal=True)
+            X[d[:n]] = y
+            W[f] = -(L21 @ y)
+        for k in E.level_seps(ell):
+            s = E.seps[k]
+            (b0, b1), (r0, r1) = s["boxes"], s["rows"]
+            d, n0, n1 = s["dofs"], Fr[b0]["n"], Fr[b1]["n"]
+            X[d] = (X[d] + W[b0][r0 - n0:r0 - n0 + len(d)]) + W[b1][r1 - n1:r1 - n1 + len(d)]
+    d = Fr[0]["dofs"]
+    X[d] = sla.lu_solve(fac[0][:2], X[d])
+    for ell in range(1, S.levels):
+        for f in E.level_fronts(ell):
+            n, d = Fr[f]["n"], Fr[f]["dofs"]
+            lu, piv, L21, U12 = fac[f]
+            X[d[:n]] = sla.solve_triangular(lu, X[d[:n]] - U12 @ X[d[n:]], lower=False)
+    return X
+
+
+@pytest.mark.parametrize("dim,N,w,ms", [(2, (31, 31), 2, 4), (2, (30, 27), 3, 5),
+                                        (3, (11, 9, 13), 2, 3), (3, (15, 15, 15), 3, 4),
+                                        (2, (31, 31), 1, 4)])
+def test_full_storage_tables_solve_nonsymmetric_stencils(dim, N, w, ms, lib):
+    """Variable coefficients make the fixture's width-2/3 stencils
+    nonsymmetric: the full-storage task tables executed with pivoted partial
+    LU (the reference's factorization) solve them as the oracle does."""
+    a = stencil.loguniform_coefficients(N, 0.5, 2.0, 5, width=w)
+    A = stencil.build_laplacian(a, width=w).to_scipy()
+    if w > 1:
+        assert abs(A - A.T).max() > 1e-6 * abs(A).max()
+    b = stencil.uniform_rhs(A.shape[0], 1, 9)[0]
+    S = Symbolic(dim, N, w, ms, full=True)
+    x = _model_solve_lu(S, taskemu.Emu(S, A), b)
+    O = mf_oracle.MFOracle(A, N, w, ms)
+    O.factor()
+    xo = O.solve(b)
+    assert np.linalg.norm(x - xo) <= 1e-12 * np.linalg.norm(xo)
+    assert np.linalg.norm(A @ x - b) <= 1e-12 * np.linalg.norm(b)
+
+
 @pytest.mark.parametrize("dim,N,ms,side", [(2, (127, 127), 4, 9), (3, (23, 23, 23), 4, 4)])
 def test_update_marks_root_paths(dim, N, ms, side, lib):
     a = stencil.loguniform_coefficients(N, 0.1, 10.0, 8)

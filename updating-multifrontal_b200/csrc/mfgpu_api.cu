@@ -1852,14 +1852,14 @@ struct mfgpu_symbolic {
   std::unique_ptr<Schedule> S;
 };
 
-int mfgpu_symbolic_create(int dim, int nx, int ny, int nz, int width, int max_side,
+static int symbolicCreate(int dim, int nx, int ny, int nz, int width, int max_side, bool full,
                           mfgpu_symbolic** out) {
   if (!out) return MFGPU_ERR_ARG;
   *out = nullptr;
   g_sym_error.clear();
   try {
     std::unique_ptr<mfgpu_symbolic> s(new mfgpu_symbolic());
-    s->S.reset(new Schedule(dim, nx, ny, nz, width, max_side));
+    s->S.reset(new Schedule(dim, nx, ny, nz, width, max_side, full));
     *out = s.release();
     return MFGPU_OK;
   } catch (const std::invalid_argument& e) {
@@ -1872,6 +1872,16 @@ int mfgpu_symbolic_create(int dim, int nx, int ny, int nz, int width, int max_si
   } catch (const std::bad_alloc&) {
     return MFGPU_ERR_OOM;
   }
+}
+
+int mfgpu_symbolic_create(int dim, int nx, int ny, int nz, int width, int max_side,
+                          mfgpu_symbolic** out) {
+  return symbolicCreate(dim, nx, ny, nz, width, max_side, false, out);
+}
+
+int mfgpu_symbolic_create_full(int dim, int nx, int ny, int nz, int width, int max_side,
+                               mfgpu_symbolic** out) {
+  return symbolicCreate(dim, nx, ny, nz, width, max_side, true, out);
 }
 
 int mfgpu_symbolic_batch_create(int count, const int* dim, const int* nx, const int* ny,

@@ -271,8 +271,8 @@ std::vector<int> Schedule::sepCenters(int e, int ell) const {
   return out;
 }
 
-Schedule::Schedule(int dim_, int nx, int ny, int nz, int width_, int max_side)
-    : dim(dim_), width(width_) {
+Schedule::Schedule(int dim_, int nx, int ny, int nz, int width_, int max_side, bool full_storage_)
+    : dim(dim_), width(width_), full_storage(full_storage_) {
   if (dim != 2 && dim != 3) throw std::invalid_argument("dim must be 2 or 3");
   N[0] = nx;
   N[1] = ny;
@@ -535,7 +535,7 @@ void Schedule::buildTasks() {
         Task tk = mk(TK_COPY, AR_FRONT, F.off + rowpos + (int64_t)colpos * F.ld, F.ld, rows, cols);
         tk.src_arena = AR_FRONT;
         tk.src_ld = C.ld;
-        if (os > ot) {
+        if (os > ot || full_storage) {   // the child holds block (s, t) itself
           tk.src_off = C.off + (C.n + os) + (int64_t)(C.n + ot) * C.ld;
         } else {
           tk.trans = 1;
@@ -548,13 +548,13 @@ void Schedule::buildTasks() {
       return false;
     };
     for (size_t a = 0; a < segs.size(); a++) {
-      for (size_t bb = 0; bb <= a; bb++) {
+      for (size_t bb = 0; bb < (full_storage ? segs.size() : a + 1); bb++) {
         const Seg& R = segs[a];
         const Seg& C = segs[bb];
         const int64_t doff = F.off + R.pos + (int64_t)C.pos * F.ld;
         Task t = mk(TK_ZERO, AR_FRONT, doff, F.ld, R.len, C.len);
         t.owner = (int)fi;
-        t.lower = (a == bb) ? 1 : 0;
+        t.lower = (a == bb && !full_storage) ? 1 : 0;
         auto sparse = [&]() {
           t.kind = TK_SPARSE;
           t.row_dof = (int32_t)(F.dof_off + R.pos);
@@ -594,6 +594,12 @@ void Schedule::buildTasks() {
           } else if (C.kind == SG_CSEP && childBlock(R.id, C.id, R.pos, C.pos, R.len, C.len)) {
             continue;
           }
+        } else if (R.piv && !C.piv) {               // A21 (full storage only): A12's mirror
+          if (C.kind == SG_ECENTER) {
+            sparse();
+          } else if (R.kind == SG_CSEP && childBlock(R.id, C.id, R.pos, C.pos, R.len, C.len)) {
+            continue;
+          }
         } else {                                    // A11 (boundary x boundary)
           if (R.parent != C.parent && R.kind == SG_CSEP && C.kind == SG_CSEP &&
               childBlock(R.id, C.id, R.pos, C.pos, R.len, C.len))
@@ -618,7 +624,7 @@ void Schedule::buildTasks() {
       return t;
     };
     if (ell == levels - 1) {
-      sep_tasks.push_back(base(TK_SPARSE, 0, 0, S.s, S.s, 1));
+      sep_tasks.push_back(base(TK_SPARSE, 0, 0, S.s, S.s, full_storage ? 0 : 1));
     } else {
       const SepSym& sy = S_[ell][S.idx];
       struct P { int pos, len, kid; };
@@ -631,14 +637,14 @@ void Schedule::buildTasks() {
       }
       if (sy.ncenter) parts.push_back({pos, sy.ncenter, -1});
       for (size_t a = 0; a < parts.size(); a++)
-        for (size_t bb = 0; bb <= a; bb++) {
+        for (size_t bb = 0; bb < (full_storage ? parts.size() : a + 1); bb++) {
           const P& R = parts[a];
           const P& C = parts[bb];
           if (R.kid < 0 || C.kid < 0) {
-            sep_tasks.push_back(base(TK_SPARSE, R.pos, C.pos, R.len, C.len, a == bb));
+            sep_tasks.push_back(base(TK_SPARSE, R.pos, C.pos, R.len, C.len, a == bb && !full_storage));
           } else if (a == bb) {
             const Sep& K = seps[lv[ell + 1].sep0 + R.kid];
-            Task t = base(TK_COPY, R.pos, R.pos, R.len, R.len, 1);
+            Task t = base(TK_COPY, R.pos, R.pos, R.len, R.len, full_storage ? 0 : 1);
             t.src_arena = AR_SEP;
             t.src_off = K.off;
             t.src_ld = K.ld;
@@ -653,7 +659,7 @@ void Schedule::buildTasks() {
     for (int k = 0; k < 2; k++) {
       const Front& F = fronts[S.box[k]];
       Task t = mk(TK_ADD, AR_SEP, S.off, S.ld, S.s, S.s);
-      t.lower = 1;
+      t.lower = full_storage ? 0 : 1;
       t.src_arena = AR_FRONT;
       t.src_off = F.off + S.bdpos[k] + (int64_t)S.bdpos[k] * F.ld;
       t.src_ld = F.ld;

@@ -70,7 +70,10 @@ struct LevelInfo {
 class Schedule {
  public:
   // Throws std::runtime_error with the reference's messages on bad parameters.
-  Schedule(int dim, int nx, int ny, int nz, int width, int max_side);
+  // full_storage: task tables for nonsymmetric matrices (every block of every
+  // front and separator, both triangles); by default the tables fill the lower
+  // triangles only, which is all the Cholesky kernels read.
+  Schedule(int dim, int nx, int ny, int nz, int width, int max_side, bool full_storage = false);
 
   // A batch of independent problems as one forest over their block-diagonal
   // matrix.  Levels are aligned at the leaves: part p's level l is level
@@ -88,6 +91,7 @@ class Schedule {
   bool forest() const { return !parts.empty(); }
 
   int dim, N[3], width, levels;
+  bool full_storage = false;   // tables fill both triangles (nonsymmetric matrices)
   int bw[3];                        // leaf box widths
   int64_t ndof;
   std::vector<LevelInfo> lv;        // index = level (0 = root)

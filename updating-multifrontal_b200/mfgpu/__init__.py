@@ -374,9 +374,11 @@ class MF3D(_MFBase):
 class Symbolic:
     """Host-only view of the schedule: DOF lists and assembly tasks."""
 
-    def __init__(self, dim, N, width=1, max_side_length=4, batch=None):
+    def __init__(self, dim, N, width=1, max_side_length=4, batch=None, full=False):
         """One problem, or with batch=[(dim, N, width, maxSideLength), ...] the
-        forest schedule of a batch (dim, N, width, max_side_length ignored)."""
+        forest schedule of a batch (dim, N, width, max_side_length ignored).
+        full=True: task tables for nonsymmetric matrices (both triangles of
+        every block; mfgpu_symbolic_create_full)."""
         lib = _lib.load()
         h = C.c_void_p()
         if batch is not None:
@@ -386,7 +388,8 @@ class Symbolic:
                                                  C.byref(h))
         else:
             Nz = N[2] if dim == 3 else 1
-            st = lib.mfgpu_symbolic_create(dim, N[0], N[1], Nz, width, max_side_length, C.byref(h))
+            create = lib.mfgpu_symbolic_create_full if full else lib.mfgpu_symbolic_create
+            st = create(dim, N[0], N[1], Nz, width, max_side_length, C.byref(h))
         if st != _lib.MFGPU_OK:
             _raise(st, lib.mfgpu_symbolic_error().decode())
         self._h, self._lib = h, lib

@@ -33,7 +33,7 @@ EXPORTED = [
     "mfgpu_symbolic_dirty", "mfgpu_batch_create", "mfgpu_batch_info",
     "mfgpu_symbolic_batch_create", "mfgpu_stencil_assemble_device", "mfgpu_stencil_update_device",
     "mfgpu_server_create", "mfgpu_server_submit", "mfgpu_server_wait", "mfgpu_server_last_error",
-    "mfgpu_server_destroy", "mfgpu_save", "mfgpu_load", "mfgpu_autotune",
+    "mfgpu_server_destroy", "mfgpu_save", "mfgpu_load", "mfgpu_autotune", "mfgpu_symbolic_create_full",
 ]
 
 KERNEL_CLASSES = ["assemble", "potrf", "trsm", "syrk", "solve", "apply", "front", "coop", "tc"]
@@ -136,6 +136,8 @@ def load(path=None):
     lib.mfgpu_destroy.restype = None
     lib.mfgpu_symbolic_create.argtypes = [C.c_int] * 6 + [C.POINTER(P)]
     lib.mfgpu_symbolic_create.restype = C.c_int
+    lib.mfgpu_symbolic_create_full.argtypes = [C.c_int] * 6 + [C.POINTER(P)]
+    lib.mfgpu_symbolic_create_full.restype = C.c_int
     lib.mfgpu_symbolic_batch_create.argtypes = [C.c_int] + [C.c_void_p] * 6 + [C.POINTER(P)]
     lib.mfgpu_symbolic_batch_create.restype = C.c_int
     lib.mfgpu_server_create.argtypes = [P, C.c_void_p, C.c_void_p, C.c_int, C.c_int64,
