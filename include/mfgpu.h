@@ -214,6 +214,24 @@ int mfgpu_solve_device_noalloc(mfgpu_handle* h, const double* d_b, double* d_x, 
  * the handle's own stream. */
 int mfgpu_set_stream(mfgpu_handle* h, void* cuda_stream);
 
+/* Failure handling (no reference counterpart: the reference has no device
+ * waits, and its LAPACK failures abort through assert, include/LinAlg/dense.hpp:187).
+ * Every device wait of this library is bounded: the grid barriers of the
+ * cooperative kernels give up after 2^25 polls, the tensor-core pipeline's
+ * mbarrier waits after 2^24; a wait that gives up makes the call return
+ * MFGPU_ERR_TIMEOUT, and the handle stays usable (the next call starts from a
+ * clean error word and barrier counter; refactor before solving again if the
+ * timeout hit a factorization).  mfgpu_set_wait_limit sets the poll limit of
+ * this handle's later launches (0 restores the built-in limits); serving-loop
+ * views created afterwards inherit it.  Waits that drain work already in
+ * flight before a kernel exits keep the built-in limit. */
+int mfgpu_set_wait_limit(mfgpu_handle* h, unsigned polls);
+/* Host-side fault injection for tests: the next `after` device allocations of
+ * the library succeed and the one after fails as if the device were out of
+ * memory (the call returns MFGPU_ERR_OOM), then injection disarms itself.
+ * after < 0 disarms it. */
+void mfgpu_inject_alloc_failure(long long after);
+
 /* Factor serialisation (no counterpart in the reference, whose factorization
  * lives in process memory only; use: restart a serving loop without
  * refactoring its base).  mfgpu_save writes a factored handle's state - front

@@ -214,8 +214,73 @@ int runAll(const Input& in, const char* outPath, SMat M1, SMat M2, MF* F, SepGet
   return 0;
 }
 
+// Algorithmic work of the timed calls, counted from the reference's own front
+// sizes after Factor (n = |intDOFs|, m = |bdDOFs| of every box) in the
+// Cholesky form the GPU path reports: factor sum(n^3/3 + n^2 m + n m^2), solve
+// sum 2(n^2 + 2 n m) per right-hand side, update the factor sum over the root
+// paths of the leaves that Update() marks (the leaf of a DOF by the integer
+// division of src/DE/mf2d.cpp:163-174 / mf3d.cpp:223-240, clamped to the last
+// box; parents by the reference's getParentIdxFromBoxIdx_).
+struct Work {
+  double factor = 0, update = 0, solve_per_rhs = 0;
+  long fronts = 0, dirty = 0;
+};
+
+double frontFlops(double n, double m) { return n * n * n / 3.0 + n * n * m + n * m * m; }
+
+template <class MF, class LeafOf, class ParentOf>
+Work workOf(MF& F, const std::set<int>& mod, LeafOf leafOf, ParentOf parentOf) {
+  Work w;
+  for (int ell = 0; ell < F.levels_; ell++)
+    for (auto& b : F.boxData_[ell]) {
+      const double n = (double)b.intDOFs.size(), m = (double)b.bdDOFs.size();
+      w.factor += frontFlops(n, m);
+      w.solve_per_rhs += 2.0 * (n * n + 2.0 * n * m);
+      w.fronts++;
+    }
+  std::set<int> marked;
+  for (int d : mod) marked.insert(leafOf(d));
+  for (int ell = F.levels_ - 1; ell >= 0 && !marked.empty(); ell--) {
+    std::set<int> up;
+    for (int b : marked) {
+      auto& box = F.boxData_[ell][b];
+      w.update += frontFlops((double)box.intDOFs.size(), (double)box.bdDOFs.size());
+      w.dirty++;
+      if (ell > 0) up.insert(parentOf(b, ell));
+    }
+    marked.swap(up);
+  }
+  return w;
+}
+
+Work work2(TreeFactor2D::MF2D<double>& F, const std::set<int>& mod) {
+  const int bps = 1 << (F.levels_ - 1);
+  auto leaf = [&](int idx) {
+    const int i = idx % F.Nx_, j = idx / F.Nx_;
+    const int ib = std::min(i / (F.boxWidthXBottom_ + F.width_), bps - 1);
+    const int jb = std::min(j / (F.boxWidthYBottom_ + F.width_), bps - 1);
+    return TreeFactor2D::TensorIdx2D(ib, jb, bps, bps).LinearIndex();
+  };
+  return workOf(F, mod, leaf, [](int b, int ell) { return TreeFactor2D::getParentIdxFromBoxIdx_(b, ell); });
+}
+
+Work work3(TreeFactor3D::MF3D<double>& F, const std::set<int>& mod) {
+  const int bps = 1 << (F.levels_ - 1);
+  auto leaf = [&](int idx) {
+    const int i = idx % F.Nx_, j = (idx / F.Nx_) % F.Ny_, k = idx / F.Nx_ / F.Ny_;
+    const int ib = std::min(i / (F.boxWidthXBottom_ + F.width_), bps - 1);
+    const int jb = std::min(j / (F.boxWidthYBottom_ + F.width_), bps - 1);
+    const int kb = std::min(k / (F.boxWidthZBottom_ + F.width_), bps - 1);
+    return TreeFactor3D::TensorIdx3D(ib, jb, kb, bps, bps, bps).LinearIndex();
+  };
+  return workOf(F, mod, leaf, [](int b, int ell) { return TreeFactor3D::getParentIdxFromBoxIdx_(b, ell); });
+}
+
+Work workFor(TreeFactor2D::MF2D<double>& F, const std::set<int>& mod) { return work2(F, mod); }
+Work workFor(TreeFactor3D::MF3D<double>& F, const std::set<int>& mod) { return work3(F, mod); }
+
 // Timing mode for the CPU baseline: repeated Factor, Update, Solve on the same
-// inputs, one JSON line on stdout.
+// inputs, one JSON line on stdout (seconds per call and the work figures).
 template <class MF>
 int runTiming(const Input& in, SMat& M1, SMat& M2, MF* F) {
   size_t n = (size_t)M1.m();
@@ -226,6 +291,7 @@ int runTiming(const Input& in, SMat& M1, SMat& M2, MF* F) {
   for (size_t i = 0; i < n; i++) b(i) = in.nrhs ? in.rhs[i] : 1.0;
   std::set<int> all;
   for (size_t i = 0; i < n; i++) all.insert((int)i);
+  Work work;
   for (int r = 0; r < std::max(1, in.timeReps); r++) {
     auto a = std::chrono::steady_clock::now();
     if (r > 0) {
@@ -237,6 +303,7 @@ int runTiming(const Input& in, SMat& M1, SMat& M2, MF* F) {
     }
     auto bt = std::chrono::steady_clock::now();
     tf.push_back(secs(a, bt));
+    if (r == 0) work = workFor(*F, mod);
     if (in.doUpdate) {
       auto c = std::chrono::steady_clock::now();
       F->Update(M2, mod);
@@ -262,8 +329,11 @@ int runTiming(const Input& in, SMat& M1, SMat& M2, MF* F) {
     }
     return s + "]";
   };
-  printf("{\"factor_s\": %s, \"update_s\": %s, \"solve_s\": %s}\n", js(tf).c_str(),
-         js(tu).c_str(), js(ts).c_str());
+  printf("{\"factor_s\": %s, \"update_s\": %s, \"solve_s\": %s, \"factor_flops\": %.9g, "
+         "\"update_flops\": %.9g, \"solve_flops_per_rhs\": %.9g, \"fronts\": %ld, "
+         "\"dirty_fronts\": %ld, \"n\": %zu, \"nnz\": %d}\n",
+         js(tf).c_str(), js(tu).c_str(), js(ts).c_str(), work.factor, work.update,
+         work.solve_per_rhs, work.fronts, work.dirty, n, M1.nnz());
   return 0;
 }
 

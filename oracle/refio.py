@@ -80,14 +80,17 @@ def read_records(path):
 
 
 def run_reference(workdir, dim, N, width, max_side, coef1, coef2=None, rhs=None,
-                  h=(1.0, 1.0, 1.0), dump_symbolic=1, dump_fronts=0, timeout=3600):
-    """Run the compiled reference once and return its records."""
+                  h=(1.0, 1.0, 1.0), dump_symbolic=1, dump_fronts=0, timeout=3600, threads=None):
+    """Run the compiled reference once and return its records (BLAS threads:
+    `threads`, else OPENBLAS_NUM_THREADS from the environment, else 1)."""
     os.makedirs(workdir, exist_ok=True)
     inp = os.path.join(workdir, "in.bin")
     outp = os.path.join(workdir, "out.bin")
     write_input(inp, dim, N, width, max_side, coef1, coef2, rhs, h,
                 dump_symbolic, dump_fronts)
     env = dict(os.environ)
+    if threads is not None:
+        env["OPENBLAS_NUM_THREADS"] = str(threads)
     env.setdefault("OPENBLAS_NUM_THREADS", "1")
     subprocess.run([REF_BIN, "dump", inp, outp], check=True, env=env, timeout=timeout)
     return read_records(outp)

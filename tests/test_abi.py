@@ -24,7 +24,7 @@ def test_every_declared_symbol_is_exported(lib):
     assert len(names) >= 25
     for nm in names:
         assert hasattr(lib, nm), nm
-    assert set(names) <= set(_lib.EXPORTED) | {"mfgpu_solve_device_noalloc"}
+    assert set(names) <= set(_lib.EXPORTED)
 
 
 def test_status_strings_and_options(lib):

@@ -14,7 +14,17 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "updating-multifrontal_b200")
-REF = "/root/reference"
+
+
+def _reference_dir():
+    """Where the reference sources are: the REF variable of oracle/Makefile
+    (the environment's REF overrides its default, as make does)."""
+    p = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "print-ref"],
+                       capture_output=True, text=True)
+    return p.stdout.strip() if p.returncode == 0 else ""
+
+
+REF = _reference_dir()
 REFBIN = os.path.join(ROOT, "oracle", "_ref")
 FLAGS = ["-O2", "-std=c++17", f"-I{PKG}/include/LinAlg", f"-I{PKG}/include/DE",
          f"-I{ROOT}/include", f"-I{ROOT}/tests/cpp"]

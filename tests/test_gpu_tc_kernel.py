@@ -10,8 +10,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.skipif(shutil.which("nvcc") is None, reason="nvcc not found")
 def test_tc_update_matches_fp64_reference(tmp_path):
+    # nvcc ships with the image; a missing compiler is a failure, not a skip
+    assert shutil.which("nvcc"), "nvcc not found on PATH"
     exe = str(tmp_path / "tc_kernel_check")
     subprocess.run(["nvcc", "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a",
                     os.path.join(ROOT, "tests", "cpp", "tc_kernel_check.cu"), "-o", exe],

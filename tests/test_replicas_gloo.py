@@ -34,7 +34,7 @@ def _rank(rank, world, port, q):
         ms, fl = [120.0, 300.0][rank], [2e12, 5e12][rank]
         rate, mx, tot = bench.whole_job(ms, fl, "cpu")
         w = bench.WORKLOADS["3d-63"]
-        a1, a2, A1, A2, mod, b = bench.make_problem(w, rank)
+        a1, a2, A1, A2, mod, b, _ = bench.make_problem(w, rank)
         again = bench.make_problem(w, rank)
         same = bool(np.array_equal(a1, again[0]) and np.array_equal(b, again[5]))
         q.put((rank, rate, mx, tot, float(np.sum(a1)), tuple(mod[:5]), same))

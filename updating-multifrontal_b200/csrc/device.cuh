@@ -26,22 +26,34 @@ struct SepDev {
 };
 static_assert(sizeof(SepDev) == 32, "SepDev layout");
 
-// Error word written by kernels: first failing front, column and code.
+// Error word written by kernels: first failing front, column and code.  The
+// host also places the poll limit of the bounded waits in it (0: the built-in
+// limits), so a launch reads the limit from the word it reports into.
 struct DevError {
-  int code;     // 0 ok, 1 non-positive pivot, 2 tensor-core wait, 3 grid barrier timed out
+  int code;        // 0 ok, 1 non-positive pivot, 2 tensor-core wait, 3 grid barrier timed out,
+                   // 4 zero pivot column of an LU front
   int front;
   int col;
-  int pad;
+  unsigned limit;  // polls before a bounded wait gives up; 0 = the built-in limit
 };
+static_assert(sizeof(DevError) == 16, "DevError layout");
+
+// Poll limit of a bounded wait: the host-set one from the error word, else dflt.
+__device__ __forceinline__ unsigned wait_limit(const DevError* err, unsigned dflt) {
+  if (!err) return dflt;
+  const unsigned l = *reinterpret_cast<const volatile unsigned*>(&err->limit);
+  return l ? l : dflt;
+}
 
 // Grid-wide barrier of the cooperative kernels, with a bounded wait.  `count`
 // (one unsigned per launch, zeroed before the launch on the launch's stream)
 // counts arrivals; `target` is private to each thread and advances by the grid
-// size at every barrier.  A wait that gives up records error code 3 in the
-// error word; every later barrier of any CTA then passes at once, so the
-// launch always ends.  The fences follow the usual grid-barrier pattern: the
-// CTA's writes are ordered before thread 0's arrival, and thread 0's
-// observation of the last arrival before the CTA's later reads.
+// size at every barrier.  A wait that gives up (after the error word's poll
+// limit, default kBarrierSpin) records error code 3 in the error word; every
+// later barrier of any CTA then passes at once, so the launch always ends.
+// The fences follow the usual grid-barrier pattern: the CTA's writes are
+// ordered before thread 0's arrival, and thread 0's observation of the last
+// arrival before the CTA's later reads.
 constexpr unsigned kBarrierSpin = 1u << 25;
 __device__ __forceinline__ void grid_barrier(unsigned* count, unsigned& target, DevError* err) {
   __syncthreads();
@@ -51,15 +63,14 @@ __device__ __forceinline__ void grid_barrier(unsigned* count, unsigned& target, 
     atomicAdd(count, 1u);
     volatile unsigned* c = count;
     volatile int* code = err ? &err->code : nullptr;
+    const unsigned lim = wait_limit(err, kBarrierSpin);
     unsigned it = 0;
     while (*c < target) {
-      if ((++it & 1023u) == 0) {
-        if (code && *code == 3) break;              // another CTA gave up
-        if (it > kBarrierSpin) {
-          if (err) atomicCAS(&err->code, 0, 3);
-          break;
-        }
+      if (++it > lim) {
+        if (err) atomicCAS(&err->code, 0, 3);
+        break;
       }
+      if ((it & 1023u) == 0 && code && *code == 3) break;   // another CTA gave up
       __nanosleep(64);
     }
     __threadfence();
@@ -154,6 +165,24 @@ constexpr int kDinvBlock = 64;   // diagonal-block size of the cooperative sweep
 template <class T>
 void launch_diag_inv(const int* flist, int nf, int maxn, const FrontDev* fr, const T* F, T* Dv,
                      const int64_t* dinv_off, cudaStream_t st);
+
+// Pivoted LU of nonsymmetric fronts (separator width 2-3), FP64
+// (kernels_lu.cu).  One 32-column step k of every front in flist: phase 0
+// factors the panel (pivots among the pivot rows, recorded in ipiv at the
+// front's DOF offset), phase 1 applies its row swaps to the other columns and
+// solves the block row, phase 2 updates the trailing matrix.  maxN: the
+// level's largest front.
+void launch_lu_step(const int* flist, int nf, int maxN, const FrontDev* fr, double* F, int* ipiv,
+                    int k, DevError* err, cudaStream_t st, int phase);
+// Sweeps of LU fronts (nrhs <= 16): forward = gather, row swaps, unit-L11
+// solve and boundary update; backward = gather, U12 update and U11 solve.
+void launch_lu_solve(bool forward, const int* flist, int nf, int maxN, const FrontDev* fr,
+                     const double* F, const int* ipiv, const int* dofs, double* X, int64_t ldx,
+                     int nrhs, double* W, const int64_t* woff, cudaStream_t st);
+// Apply, upward part, of LU fronts (the downward part is launch_apply_down).
+void launch_lu_apply_up(const int* flist, int nf, const FrontDev* fr, const double* F,
+                        const int* ipiv, const int* dofs, double* X, int64_t ldx, int nrhs,
+                        double* W, const int64_t* woff, double* Tb, cudaStream_t st);
 
 // Stencil assembly (width 1): recompute the CSR values of the rows of the
 // cells in [lo, hi) from the node coefficients; with `flag`, record which rows

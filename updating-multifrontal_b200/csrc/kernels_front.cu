@@ -783,7 +783,9 @@ constexpr int ST = 256;
 // Forward solve with the front's first n columns, right-looking over 32-column
 // blocks.  On exit W[0,n) = L11^{-1} b_piv and W[n,N) = -L21 W[0,n).  W is the
 // front's right-hand-side block (N x nrhs, ld N) in shared or global memory.
-template <class T, int NR>
+// UNIT: L11 has a unit diagonal (the L of a pivoted LU front) and its stored
+// diagonal, U's, is not read.
+template <class T, int NR, bool UNIT = false>
 __device__ void front_forward(const FrontDev& d, const T* __restrict__ A, T* W,
                               int nrhs) {
   __shared__ T Ls[kPanel][kPanel + 1];
@@ -804,7 +806,7 @@ __device__ void front_forward(const FrontDev& d, const T* __restrict__ A, T* W,
     if (warp == 0) {
       // column-oriented substitution: lane i owns row i of the block
       for (int j = 0; j < kb; j++) {
-        if (lane == j) {
+        if (!UNIT && lane == j) {
           const T djj = Ls[j][j];
 #pragma unroll
           for (int c = 0; c < NR; c++)
@@ -1135,6 +1137,214 @@ __global__ void __launch_bounds__(ST) k_root_apply(int f, const FrontDev* __rest
   }
 }
 
+// ---------------------------------------------------------------------------
+// Sweeps of pivoted LU fronts (nonsymmetric problems, FP64; factors from
+// kernels_lu.cu: P A22 = L11 U11, L21 = A12 U11^{-1}, U12 = L11^{-1} P A21).
+// The reference's upward step b_sk -= XL b_rd, b_rd <- A22^{-1} b_rd and
+// downward step b_rd -= XR b_sk (src/DE/mf2d.cpp:976-1054) become
+//   forward:  y = L11^{-1} P b_piv (kept as the pivot part), W[n,N) = -L21 y
+//   backward: x_piv = U11^{-1} (y - U12 x_bd)
+// since XL = L21 L11^{-1} P and XR = U11^{-1} U12.
+// ---------------------------------------------------------------------------
+
+// Backward solve: W[0,n) <- U11^{-1} (W[0,n) - U12 W[n,N)), upward over
+// 32-row blocks; U(k block, right of it) is read a column at a time (lanes
+// along the block's rows), warps splitting the columns.
+template <int NR>
+__device__ void front_backward_lu(const FrontDev& d, const double* __restrict__ A, double* W,
+                                  int nrhs) {
+  __shared__ double Us[kPanel][kPanel + 1];
+  __shared__ double xs[kPanel][NR + 1];
+  __shared__ double part[ST / 32][kPanel];
+  const int N = d.N, n = d.n, ld = d.ld, tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int nblk = (n + kPanel - 1) / kPanel;
+  for (int bk = nblk - 1; bk >= 0; bk--) {
+    const int k = bk * kPanel, kb = min(kPanel, n - k);
+    for (int idx = tid; idx < kb * kb; idx += blockDim.x) {
+      const int i = idx % kb, j = idx / kb;
+      if (i <= j) Us[i][j] = A[(k + i) + (int64_t)(k + j) * ld];
+    }
+    double acc[NR];
+#pragma unroll
+    for (int c = 0; c < NR; c++) acc[c] = 0.0;
+    if (lane < kb)
+      for (int r = k + kb + warp; r < N; r += nw) {
+        const double u = A[(k + lane) + (int64_t)r * ld];
+#pragma unroll
+        for (int c = 0; c < NR; c++)
+          if (c < nrhs) acc[c] = fma(u, W[r + (int64_t)c * N], acc[c]);
+      }
+#pragma unroll
+    for (int c = 0; c < NR; c++) {
+      if (c < nrhs) {
+        part[warp][lane] = acc[c];
+        __syncthreads();
+        if (warp == 0 && lane < kb) {
+          double s = 0.0;
+          for (int w = 0; w < nw; w++) s += part[w][lane];
+          xs[lane][c] = W[k + lane + (int64_t)c * N] - s;
+        }
+        __syncthreads();
+      }
+    }
+    if (warp == 0) {
+      for (int j = kb - 1; j >= 0; j--) {
+        if (lane == j) {
+          const double ujj = Us[j][j];
+#pragma unroll
+          for (int c = 0; c < NR; c++)
+            if (c < nrhs) xs[j][c] = xs[j][c] / ujj;
+        }
+        __syncwarp();
+        if (lane < j) {
+          const double u = Us[lane][j];
+#pragma unroll
+          for (int c = 0; c < NR; c++)
+            if (c < nrhs) xs[lane][c] -= u * xs[j][c];
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < kb * nrhs; idx += blockDim.x) {
+      const int i = idx % kb, c = idx / kb;
+      W[k + i + (int64_t)c * N] = xs[i][c];
+    }
+    __syncthreads();
+  }
+}
+
+template <int NR>
+__global__ void __launch_bounds__(ST) k_lu_solve_fwd(const int* __restrict__ flist,
+                                                     const FrontDev* __restrict__ fr,
+                                                     const double* __restrict__ F,
+                                                     const int* __restrict__ ipiv,
+                                                     const int* __restrict__ dofs, double* X,
+                                                     int64_t ldx, int nrhs, double* Wb,
+                                                     const int64_t* __restrict__ woff,
+                                                     int use_smem) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double* smW = reinterpret_cast<double*>(smraw);
+  const int f = flist[blockIdx.x];
+  const FrontDev d = fr[f];
+  double* Wg = Wb + woff[f] * nrhs;
+  double* W = use_smem ? smW : Wg;
+  const int* dl = dofs + d.dof_off;
+  const int* pv = ipiv + d.dof_off;
+  for (int idx = threadIdx.x; idx < d.N * nrhs; idx += blockDim.x) {
+    const int i = idx % d.N, c = idx / d.N;
+    W[idx] = i < d.n ? X[dl[i] + (int64_t)c * ldx] : 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x < nrhs) {   // b_piv <- P b_piv: the swaps in factorization order
+    double* w = W + (int64_t)threadIdx.x * d.N;
+    for (int j = 0; j < d.n; j++) {
+      const int p = pv[j];
+      if (p != j) {
+        const double t = w[j];
+        w[j] = w[p];
+        w[p] = t;
+      }
+    }
+  }
+  __syncthreads();
+  front_forward<double, NR, true>(d, F + d.off, W, nrhs);
+  for (int idx = threadIdx.x; idx < d.N * nrhs; idx += blockDim.x) {
+    const int i = idx % d.N, c = idx / d.N;
+    if (i < d.n) X[dl[i] + (int64_t)c * ldx] = W[idx];
+    else if (use_smem) Wg[idx] = W[idx];    // boundary part for the separator gather
+  }
+}
+
+template <int NR>
+__global__ void __launch_bounds__(ST) k_lu_solve_bwd(const int* __restrict__ flist,
+                                                     const FrontDev* __restrict__ fr,
+                                                     const double* __restrict__ F,
+                                                     const int* __restrict__ dofs, double* X,
+                                                     int64_t ldx, int nrhs, double* Wb,
+                                                     const int64_t* __restrict__ woff,
+                                                     int use_smem) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double* smW = reinterpret_cast<double*>(smraw);
+  const int f = flist[blockIdx.x];
+  const FrontDev d = fr[f];
+  double* W = use_smem ? smW : Wb + woff[f] * nrhs;
+  const int* dl = dofs + d.dof_off;
+  for (int idx = threadIdx.x; idx < d.N * nrhs; idx += blockDim.x) {
+    const int i = idx % d.N, c = idx / d.N;
+    W[idx] = X[dl[i] + (int64_t)c * ldx];
+  }
+  __syncthreads();
+  front_backward_lu<NR>(d, F + d.off, W, nrhs);
+  for (int idx = threadIdx.x; idx < d.n * nrhs; idx += blockDim.x) {
+    const int i = idx % d.n, c = idx / d.n;
+    X[dl[i] + (int64_t)c * ldx] = W[i + (int64_t)c * d.N];
+  }
+}
+
+// Apply, upward part, of a pivoted LU front: u = U11 b_piv + U12 b_bd,
+// b_piv <- P^T L11 u (= A22 t with t = b_piv + XR b_bd), T(piv) = u; the
+// downward part W[n,N) = L21 u (= XL A22 t) is k_apply_down's.
+__global__ void __launch_bounds__(ST) k_lu_apply_up(const int* __restrict__ flist,
+                                                    const FrontDev* __restrict__ fr,
+                                                    const double* __restrict__ F,
+                                                    const int* __restrict__ ipiv,
+                                                    const int* __restrict__ dofs, double* X,
+                                                    int64_t ldx, int nrhs, double* Wb,
+                                                    const int64_t* __restrict__ woff, double* Tb) {
+  const int f = flist[blockIdx.x];
+  const FrontDev d = fr[f];
+  double* W = Wb + woff[f] * nrhs;
+  const int* dl = dofs + d.dof_off;
+  const int* pv = ipiv + d.dof_off;
+  const double* A = F + d.off;
+  const int N = d.N, n = d.n, ld = d.ld;
+  for (int idx = threadIdx.x; idx < N * nrhs; idx += blockDim.x) {
+    const int i = idx % N, c = idx / N;
+    W[idx] = X[dl[i] + (int64_t)c * ldx];
+  }
+  __syncthreads();
+  double* u = W + (int64_t)N * nrhs;   // second half of the front's workspace (n x nrhs, ld n)
+  // u(j) = sum_{c >= j} U(j, c) W(c): columns in order, rows across threads
+  for (int idx = threadIdx.x; idx < n * nrhs; idx += blockDim.x) {
+    const int j = idx % n, c = idx / n;
+    const double* w = W + (int64_t)c * N;
+    double s = 0.0;
+    // from the warp's first row, so that a warp's loads of a column coalesce
+    for (int col = j & ~31; col < N; col++)
+      if (col >= j) s += A[j + (int64_t)col * ld] * w[col];
+    u[j + (int64_t)c * n] = s;
+  }
+  __syncthreads();
+  // v(r) = u(r) + sum_{j < r} L(r, j) u(j)
+  for (int idx = threadIdx.x; idx < n * nrhs; idx += blockDim.x) {
+    const int r = idx % n, c = idx / n;
+    const double* uc = u + (int64_t)c * n;
+    double s = uc[r];
+    for (int j = 0; j < r; j++) s += A[r + (int64_t)j * ld] * uc[j];
+    W[r + (int64_t)c * N] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < nrhs) {   // P^T: the swaps undone in reverse order
+    double* w = W + (int64_t)threadIdx.x * N;
+    for (int j = n - 1; j >= 0; j--) {
+      const int p = pv[j];
+      if (p != j) {
+        const double t = w[j];
+        w[j] = w[p];
+        w[p] = t;
+      }
+    }
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < n * nrhs; idx += blockDim.x) {
+    const int i = idx % n, c = idx / n;
+    X[dl[i] + (int64_t)c * ldx] = W[i + (int64_t)c * N];
+    Tb[dl[i] + (int64_t)c * ldx] = u[i + (int64_t)c * n];
+  }
+}
+
 }  // namespace
 
 template <class T>
@@ -1402,6 +1612,49 @@ void launch_sep_gather(const int* slist, int ns, const SepDev* sp, const int* do
                        cudaStream_t st) {
   if (ns <= 0) return;
   k_sep_gather<T><<<ns, ST, 0, st>>>(slist, sp, dofs, X, ldx, nrhs, W, woff, fr);
+  g_launches++;
+}
+
+void launch_lu_solve(bool forward, const int* flist, int nf, int maxN, const FrontDev* fr,
+                     const double* F, const int* ipiv, const int* dofs, double* X, int64_t ldx,
+                     int nrhs, double* W, const int64_t* woff, cudaStream_t st) {
+  if (nf <= 0) return;
+  size_t sm;
+  int use;
+  smemFor(maxN, nrhs, sizeof(double), sm, use);
+  const int threads = sweep_threads(maxN);
+#define MFGPU_LU(NR)                                                                             \
+  do {                                                                                           \
+    if (forward) {                                                                               \
+      static const bool attr_ = (cudaFuncSetAttribute(k_lu_solve_fwd<NR>,                        \
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                                      kSolveSmemBytes),                            \
+                                 true);                                                            \
+      (void)attr_;                                                                               \
+      k_lu_solve_fwd<NR><<<nf, threads, sm, st>>>(flist, fr, F, ipiv, dofs, X, ldx, nrhs, W, woff, \
+                                                  use);                                          \
+    } else {                                                                                     \
+      static const bool attr_ = (cudaFuncSetAttribute(k_lu_solve_bwd<NR>,                        \
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                                      kSolveSmemBytes),                            \
+                                 true);                                                            \
+      (void)attr_;                                                                               \
+      k_lu_solve_bwd<NR><<<nf, threads, sm, st>>>(flist, fr, F, dofs, X, ldx, nrhs, W, woff, use); \
+    }                                                                                            \
+  } while (0)
+  if (nrhs == 1) MFGPU_LU(1);
+  else if (nrhs <= 4) MFGPU_LU(4);
+  else if (nrhs <= 8) MFGPU_LU(8);
+  else MFGPU_LU(16);
+#undef MFGPU_LU
+  g_launches++;
+}
+
+void launch_lu_apply_up(const int* flist, int nf, const FrontDev* fr, const double* F,
+                        const int* ipiv, const int* dofs, double* X, int64_t ldx, int nrhs,
+                        double* W, const int64_t* woff, double* Tb, cudaStream_t st) {
+  if (nf <= 0) return;
+  k_lu_apply_up<<<nf, ST, 0, st>>>(flist, fr, F, ipiv, dofs, X, ldx, nrhs, W, woff, Tb);
   g_launches++;
 }
 

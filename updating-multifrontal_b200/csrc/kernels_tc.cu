@@ -42,9 +42,11 @@
 // but they read back as zeros on sm_100a, hence the pack.  The three-term form
 // keeps products to about 2^-21 relative error, close to FP32.
 //
-// Every mbarrier wait is bounded; on expiry (or once another warp gave up) the
-// kernel records error code 2 in the error word, skips the remaining work,
-// waits for its own copies in flight, releases its tensor memory and returns.
+// Every mbarrier wait is bounded (kSpinLimit polls, or the limit the host put
+// in the error word); on expiry (or once another warp gave up) the kernel
+// records error code 2 in the error word, skips the remaining work, waits for
+// its own copies and products in flight, releases its tensor memory and
+// returns.
 #include <atomic>
 #include <cstdint>
 
@@ -168,10 +170,11 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 }
 
 // Wait for completion of the mbarrier phase with the given parity.  Bounded:
-// returns false after kSpinLimit polls or as soon as *abort is set.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
+// returns false after `limit` polls or as soon as *abort is set.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort,
+                                          uint32_t limit) {
   const uint32_t a = smem_u32(bar);
-  for (uint32_t it = 0; it < kSpinLimit; it++) {
+  for (uint32_t it = 0; it < limit; it++) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -189,9 +192,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
 
 // Warp-uniform wait: lane 0 polls, the outcome is broadcast to the warp so that
 // the warp's collective tcgen05 instructions stay converged.
-__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity, volatile int* abort) {
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity, volatile int* abort,
+                                               uint32_t limit) {
   bool ok = true;
-  if ((threadIdx.x & 31) == 0) ok = mbar_wait(bar, parity, abort);
+  if ((threadIdx.x & 31) == 0) ok = mbar_wait(bar, parity, abort, limit);
   return __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
 }
 
@@ -334,11 +338,14 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
                                                      int cap, const unsigned char* __restrict__ pack,
                                                      DevError* err) {
   extern __shared__ unsigned char tc_raw[];
-  __shared__ uint64_t full[NSTAGE], empty[NSTAGE], acc_full[NACC], acc_empty[NACC];
+  __shared__ uint64_t full[NSTAGE], empty[NSTAGE], acc_full[NACC], acc_empty[NACC], drain;
   __shared__ uint32_t tmem_base;
   __shared__ int pre[kMaxTcFronts + 1];
   __shared__ volatile int abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // pipeline waits give up after this many polls (host-settable); the waits
+  // that drain work already issued before the CTA exits keep kSpinLimit
+  const uint32_t lim = wait_limit(err, kSpinLimit);
   unsigned char* sm =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(tc_raw) + 1023) & ~(uintptr_t)1023);
 
@@ -358,6 +365,7 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
       mbar_init(&acc_full[b], 1);
       mbar_init(&acc_empty[b], NEPI * 32);
     }
+    mbar_init(&drain, 1);
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -390,7 +398,7 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
         for (int c = 0; c < ti.nch; c++, g++) {
           const int s = g % NSTAGE;
           const uint32_t u = g / NSTAGE;
-          if (u >= 1 && !mbar_wait(&empty[s], (u - 1) & 1, &abort_flag)) {
+          if (u >= 1 && !mbar_wait(&empty[s], (u - 1) & 1, &abort_flag, lim)) {
             ok = false;
             break;
           }
@@ -409,7 +417,7 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
       // the copies still in flight land before the CTA may exit
       volatile int never = 0;
       for (uint32_t q = g > NSTAGE ? g - NSTAGE : 0; q < g; q++)
-        mbar_wait(&full[q % NSTAGE], (q / NSTAGE) & 1, &never);
+        mbar_wait(&full[q % NSTAGE], (q / NSTAGE) & 1, &never, kSpinLimit);
     }
   } else if (warp == MMA_WARP) {
     // ---- MMA issue ----
@@ -419,7 +427,7 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
       const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, w, cend, tile);
       const int b = tl % NACC;
       const uint32_t v = tl / NACC;
-      if (v >= 1 && !mbar_wait_warp(&acc_empty[b], (v - 1) & 1, &abort_flag)) break;
+      if (v >= 1 && !mbar_wait_warp(&acc_empty[b], (v - 1) & 1, &abort_flag, lim)) break;
       tc_fence_after();
       const uint32_t dacc = tmem + b * TN;
       const int bb = 2 * ti.J, nbb = min(2, ti.nb - bb);
@@ -427,7 +435,7 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
       bool ok = true;
       for (int c = 0; c < ti.nch; c++, g++) {
         const int s = g % NSTAGE;
-        if (!mbar_wait_warp(&full[s], (g / NSTAGE) & 1, &abort_flag)) {
+        if (!mbar_wait_warp(&full[s], (g / NSTAGE) & 1, &abort_flag, lim)) {
           ok = false;
           break;
         }
@@ -453,6 +461,14 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
       if (!ok) break;
       if (lane == 0) mma_commit(&acc_full[b]);
       __syncwarp();
+    }
+    // after an abort, products already issued may still be running: a commit
+    // tracks all of them, and tensor memory is released only once it fired
+    if (abort_flag && g > 0) {
+      if (lane == 0) mma_commit(&drain);
+      __syncwarp();
+      volatile int never = 0;
+      mbar_wait_warp(&drain, 0, &never, kSpinLimit);
     }
   } else {
     // ---- epilogue: C(tile) -= acc; warp w reads accumulator lanes
@@ -480,7 +496,7 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
 #pragma unroll
         for (int j = 0; j < 32; j++, q += ti.ld) cv[j] = 32 * h2 + j <= jmax ? *q : 0.0f;
         if (h2 == 0) {
-          if (!mbar_wait_warp(&acc_full[b], (tl / NACC) & 1, &abort_flag)) {
+          if (!mbar_wait_warp(&acc_full[b], (tl / NACC) & 1, &abort_flag, lim)) {
             ok = false;
             break;
           }

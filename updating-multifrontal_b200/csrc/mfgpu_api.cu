@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -42,10 +43,25 @@ void ck(cudaError_t e, const char* what) {
   }
 }
 
+// Host-side fault injection (mfgpu_inject_alloc_failure): the number of
+// device allocations that still succeed before one is failed; -1 = disarmed.
+std::atomic<long long> g_alloc_budget{-1};
+
+// True when this allocation is the one chosen to fail (disarms the injection).
+bool injectedAllocFailure() {
+  long long k = g_alloc_budget.load();
+  while (k >= 0) {
+    if (g_alloc_budget.compare_exchange_weak(k, k - 1)) return k == 0;
+  }
+  return false;
+}
+
 template <class T>
 T* dalloc(size_t count, const char* what) {
   void* p = nullptr;
   if (count == 0) count = 1;
+  if (injectedAllocFailure())
+    throw CudaError(std::string(what) + ": injected device allocation failure", MFGPU_ERR_OOM);
   ck(cudaMalloc(&p, count * sizeof(T)), what);
   return static_cast<T*>(p);
 }
@@ -243,6 +259,7 @@ struct mfgpu_handle {
   SepDev* d_sp = nullptr;
   int64_t* d_woff = nullptr;
   DevError* d_err = nullptr;
+  DevError errInit{};              // what d_err is reset to before a call: code 0, the poll limit
   void* d_slots = nullptr;     // diagonal-block hand-off slots of the cooperative kernel
   void* d_tcpack = nullptr;    // tensor-core panel images (mixed path)
   size_t tcPackCap = 0;
@@ -297,6 +314,11 @@ struct mfgpu_handle {
   std::vector<int> lvMaxn;   // largest pivot count per level
   int solveCoopMinN = 1024;  // levels with a front this large use the cooperative sweeps
   bool stepped = false;      // MFGPU_STEPPED=1: per-step launches instead of the cooperative kernel
+  // Separator widths 2-3: the operators are nonsymmetric, every front is
+  // stored whole and factored by pivoted LU (FP64), pivots in d_ipiv beside
+  // each front's pivot DOFs.
+  bool lu = false;
+  int* d_ipiv = nullptr;
   // A view (the serving loop's per-slot handle) shares the base handle's
   // schedule, arenas, matrix pattern and tables and owns only its stream, its
   // front table, values, error word, scratch and workspaces.
@@ -321,6 +343,7 @@ struct mfgpu_handle {
       cudaFree(d_segchunk);
       cudaFree(d_all);
       cudaFree(d_dinv_off);
+      cudaFree(d_ipiv);
     }
     cudaFree(d_Dinv);
     cudaFree(d_val);
@@ -448,10 +471,11 @@ struct mfgpu_handle {
 
   // Level kernels.  The size rules choose one per level; mfgpu_autotune can
   // replace the choice for the levels of the full factorization by timing.
-  enum LevelKernel { LK_NONE = -1, LK_FUSED = 0, LK_COOP = 1, LK_TC = 2, LK_STEPPED = 3 };
+  enum LevelKernel { LK_NONE = -1, LK_FUSED = 0, LK_COOP = 1, LK_TC = 2, LK_STEPPED = 3, LK_LU = 4 };
 
   int ruleKernel(const Plan::Level& L) const {
     if (L.nf <= 0) return LK_NONE;
+    if (lu) return LK_LU;
     if (useFused((int)L.nf, L.maxN)) return LK_FUSED;
     if (!mfgpu::coop_fits((int)L.nf) || (stepped && !mixed)) return LK_STEPPED;
     if (mixed && tcLevel(L)) return LK_TC;
@@ -533,6 +557,40 @@ struct mfgpu_handle {
       if (sizeof(T) != sizeof(double))
         throw CudaError("no single-precision path for this level", MFGPU_ERR_ARG);
       runStepped(P, L);
+    } else if (kind == LK_LU) {
+      if (sizeof(T) != sizeof(double)) throw CudaError("LU fronts are FP64 only", MFGPU_ERR_ARG);
+      runLU(P, L);
+    }
+  }
+
+  // Pivoted LU of a level's fronts (nonsymmetric problems): per 32-column
+  // step the panel, the row swaps and block-row solve, the trailing update
+  // (kernels_lu.cu).  Flops: the LU form of a partial factorization,
+  // 2n^3/3 + 2n^2 m + 2n m^2 per front, under the three profiling classes.
+  void runLU(const Plan& P, const Plan::Level& L) {
+    const Schedule& s = *S;
+    double* F = (double*)d_F;
+    const int* fl = P.d_ids + L.f0;
+    for (int k = 0; k < L.maxn; k += mfgpu::kPanel) {
+      if (prof.on) {
+        for (int64_t i = L.f0; i < L.f0 + L.nf; i++) {
+          const mfgpu::Front& f = s.fronts[P.ids[i]];
+          if (k >= f.n) continue;
+          const double kb = std::min(mfgpu::kPanel, f.n - k), M = f.N - k - kb;
+          prof.flops[MFGPU_KC_POTRF] += kb * kb * kb / 3.0 + M * kb * kb;
+          prof.flops[MFGPU_KC_TRSM] += M * kb * kb;
+          prof.flops[MFGPU_KC_SYRK] += 2.0 * M * M * kb;
+        }
+      }
+      const int cls[3] = {MFGPU_KC_POTRF, MFGPU_KC_TRSM, MFGPU_KC_SYRK};
+      const char* what[3] = {"launch LU panel (k_lu_panel)", "launch LU swaps + block row (k_lu_swap_trsm)",
+                             "launch LU trailing update (k_lu_gemm)"};
+      for (int ph = 0; ph < 3; ph++) {
+        prof.begin(cls[ph], stream);
+        mfgpu::launch_lu_step(fl, (int)L.nf, L.maxN, d_fr, F, d_ipiv, k, d_err, stream, ph);
+        ck(cudaGetLastError(), what[ph]);
+        prof.end(stream);
+      }
     }
   }
 
@@ -547,7 +605,7 @@ struct mfgpu_handle {
       for (int ell = 0; ell < s.levels && ell < (int)tuned.size(); ell++)
         if (tuned[ell] == LK_TC) pack = std::max(pack, levelPackBytes(P, P.lv[ell]));
     ensurePack(pack);
-    ck(cudaMemsetAsync(d_err, 0, sizeof(DevError), stream), "clear error word");
+    clearErr();
     for (int ell = s.levels - 1; ell >= 0; ell--) {
       const Plan::Level& L = P.lv[ell];
       prof.level = ell;
@@ -591,7 +649,7 @@ struct mfgpu_handle {
       mfgpu::launch_diag_scale(d_rp, d_ci, d_val, n, d_scale, d_iscale, stream);
       ck(cudaGetLastError(), "launch diagonal scaling");
     }
-    ck(cudaMemsetAsync(d_err, 0, sizeof(DevError), stream), "clear error word");
+    clearErr();
     const bool prof_on = prof.on;
     prof.on = false;
     for (int ell = s.levels - 1; ell >= 0; ell--) {
@@ -764,6 +822,14 @@ struct mfgpu_handle {
     runPlan(P);
   }
 
+  // Reset the error word before a call's launches; it also carries the poll
+  // limit of the bounded device waits (mfgpu_set_wait_limit).  errInit lives as
+  // long as the handle, so the asynchronous copy may read it late.
+  void clearErr() {
+    ck(cudaMemcpyAsync(d_err, &errInit, sizeof(DevError), cudaMemcpyHostToDevice, stream),
+       "clear error word");
+  }
+
   void checkDevError() {
     DevError e;
     ck(cudaMemcpyAsync(&e, d_err, sizeof(e), cudaMemcpyDeviceToHost, stream), "read error word");
@@ -772,6 +838,15 @@ struct mfgpu_handle {
       throw CudaError(e.code == 2 ? "a tensor-core pipeline wait gave up (k_trail_tc)"
                                   : "a cooperative kernel's grid barrier gave up",
                       MFGPU_ERR_TIMEOUT);
+    }
+    if (e.code == 4) {
+      const mfgpu::Front& f = S->fronts[e.front];
+      char buf[256];
+      snprintf(buf, sizeof buf,
+               "zero pivot column in front %d (level %d, box %d) at pivot column %d: the front's "
+               "pivot block is singular",
+               e.front, f.level, f.box, e.col);
+      throw CudaError(buf, MFGPU_ERR_PIVOT);
     }
     if (e.code == 1) {
       const mfgpu::Front& f = S->fronts[e.front];
@@ -835,7 +910,13 @@ struct mfgpu_handle {
     const T* F = (const T*)d_F;
     const int* fl = d_all + s.lv[ell].front0;
     const int nf = s.lv[ell].nbox;
-    if (coopSweep(ell)) {
+    if (lu) {
+      if (sizeof(T) != sizeof(double)) throw CudaError("LU fronts are FP64 only", MFGPU_ERR_ARG);
+      mfgpu::launch_lu_solve(forward, fl, nf, lvMaxN[ell], d_fr, (const double*)F, d_ipiv, d_dofs,
+                             (double*)X, ldx, nrhs, (double*)W, d_woff, stream);
+      ck(cudaGetLastError(), forward ? "launch LU forward sweep (k_lu_solve_fwd)"
+                                     : "launch LU backward sweep (k_lu_solve_bwd)");
+    } else if (coopSweep(ell)) {
       ck(mfgpu::launch_solve_coop<T>(forward, fl, nf, lvMaxn[ell], d_fr, F, d_dofs, X, ldx, nrhs, W,
                                      d_woff, (const T*)d_Dinv, d_dinv_off, d_gbar, d_err, stream),
          forward ? "launch cooperative forward sweep (k_solve_coop_fwd)"
@@ -868,7 +949,7 @@ struct mfgpu_handle {
       ck(cudaGetLastError(), "launch separator gather (k_sep_gather)");
     }
     vmark(true, 0);
-    if (coopSweep(0) || s.lv[0].nbox > 1) {   // several roots (a batch): generic sweeps
+    if (lu || coopSweep(0) || s.lv[0].nbox > 1) {   // several roots (a batch), LU: generic sweeps
       sweepLevel<T>(true, 0, X, ldx, nrhs, W);
       sweepLevel<T>(false, 0, X, ldx, nrhs, W);
     } else {
@@ -888,12 +969,22 @@ struct mfgpu_handle {
   void applySweeps(T* X, int64_t ldx, int nrhs, T* W, T* Tb) {
     const Schedule& s = *S;
     const T* F = (const T*)d_F;
-    for (int ell = s.levels - 1; ell >= 1; ell--) {
-      mfgpu::launch_apply_up<T>(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, F, d_dofs, X, ldx,
-                                nrhs, W, d_woff, Tb, stream);
-      ck(cudaGetLastError(), "launch apply up (k_apply_up)");
-    }
-    if (s.lv[0].nbox > 1) {   // several roots (a batch)
+    auto up = [&](int ell) {
+      if (lu) {
+        mfgpu::launch_lu_apply_up(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, (const double*)F,
+                                  d_ipiv, d_dofs, (double*)X, ldx, nrhs, (double*)W, d_woff,
+                                  (double*)Tb, stream);
+        ck(cudaGetLastError(), "launch LU apply up (k_lu_apply_up)");
+      } else {
+        mfgpu::launch_apply_up<T>(d_all + s.lv[ell].front0, s.lv[ell].nbox, d_fr, F, d_dofs, X, ldx,
+                                  nrhs, W, d_woff, Tb, stream);
+        ck(cudaGetLastError(), "launch apply up (k_apply_up)");
+      }
+    };
+    for (int ell = s.levels - 1; ell >= 1; ell--) up(ell);
+    if (lu) {
+      up(0);
+    } else if (s.lv[0].nbox > 1) {   // several roots (a batch)
       mfgpu::launch_apply_up<T>(d_all, s.lv[0].nbox, d_fr, F, d_dofs, X, ldx, nrhs, W, d_woff, Tb,
                                 stream);
       ck(cudaGetLastError(), "launch apply up (k_apply_up)");
@@ -1087,14 +1178,19 @@ namespace {
 
 // Schedule of one problem; the reference's constructor exceptions become
 // status codes (src/DE/mf2d.cpp:38-43 recursion depth, :60-66 leaf math).
+// Separator widths 2-3 (the reference fixture's wider stencils,
+// test_include/DE/buildLaplacian.hpp:18-35) give nonsymmetric operators: their
+// schedule carries full-storage task tables and the handle factors by pivoted
+// LU.  Batches take width 1 only.
 int makeSchedule(int dim, int nx, int ny, int nz, int width, int max_side,
-                 std::unique_ptr<Schedule>& out) {
-  if (width != 1) {
-    g_create_error = "only separator width 1 (5-/7-point stencils) is supported";
+                 std::unique_ptr<Schedule>& out, bool allow_wide = true) {
+  if (width < 1 || width > 3 || (!allow_wide && width != 1)) {
+    g_create_error = allow_wide ? "separator width must be 1, 2 or 3"
+                                : "batch members must have separator width 1";
     return MFGPU_ERR_ARG;
   }
   try {
-    out.reset(new Schedule(dim, nx, ny, nz, width, max_side));
+    out.reset(new Schedule(dim, nx, ny, nz, width, max_side, /*full_storage=*/width > 1));
   } catch (const std::invalid_argument& e) {
     g_create_error = e.what();
     return MFGPU_ERR_ARG;
@@ -1169,7 +1265,7 @@ int mfgpu_batch_create(int count, const int* dim, const int* nx, const int* ny, 
   parts.reserve(count);
   for (int p = 0; p < count; p++) {
     std::unique_ptr<Schedule> one;
-    const int st = makeSchedule(dim[p], nx[p], ny[p], nz[p], width[p], max_side[p], one);
+    const int st = makeSchedule(dim[p], nx[p], ny[p], nz[p], width[p], max_side[p], one, false);
     if (st != MFGPU_OK) {
       g_create_error = "batch member " + std::to_string(p) + ": " + g_create_error;
       return st;
@@ -1219,12 +1315,19 @@ int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const
     g_create_error = "matrix dimension does not match the grid";
     return MFGPU_ERR_ARG;
   }
-  std::string where;
-  if (const char* why = asymmetry(n, row_ptr, col_ind, val, where)) {
-    g_create_error = std::string(why) + where +
-                     ": this library factors symmetric positive definite matrices";
+  h->lu = s.full_storage;
+  if (h->lu && h->opt.precision != MFGPU_FP64) {
+    g_create_error = "separator widths 2-3 (nonsymmetric operators, pivoted LU) are FP64 only";
     return MFGPU_ERR_ARG;
   }
+  std::string where;
+  if (!h->lu)
+    if (const char* why = asymmetry(n, row_ptr, col_ind, val, where)) {
+      g_create_error = std::string(why) + where +
+                       ": this library factors symmetric positive definite matrices with "
+                       "separator width 1 (widths 2-3 are factored by pivoted LU)";
+      return MFGPU_ERR_ARG;
+    }
   h->n = n;
   h->nnz = row_ptr[n];
   if (const char* e = getenv("MFGPU_STEPPED")) h->stepped = e[0] == '1';
@@ -1235,6 +1338,7 @@ int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const
   if (const char* e = getenv("MFGPU_TC_SPLIT")) h->tcSplit = atoi(e) == 1 ? 1 : 3;
   if (const char* e = getenv("MFGPU_TC_SPLIT3_LEVELS")) h->tcSplit3Levels = atoi(e);
   if (const char* e = getenv("MFGPU_TC_SUB")) h->tcSub = atoi(e);
+  if (h->lu) h->solveCoopMinN = 0;   // LU fronts use the per-front sweeps
   h->h_rowptr.assign(row_ptr, row_ptr + n + 1);
   h->h_colind.assign(col_ind, col_ind + h->nnz);
   int st = guarded(h.get(), [&]() {
@@ -1315,6 +1419,7 @@ int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const
     H.d_slots = dalloc<unsigned char>(mfgpu::coop_slot_elems() * H.esz, "alloc diagonal slots");
     H.d_gbar = dalloc<unsigned>(1, "alloc grid barrier");
     H.d_all = dalloc<int>(all.size(), "alloc id list");
+    if (H.lu) H.d_ipiv = dalloc<int>(s.dofs.size(), "alloc LU pivots");
     ck(cudaMemcpy(H.d_val, val, H.nnz * sizeof(double), cudaMemcpyHostToDevice), "upload val");
     ck(cudaMemcpy(H.d_rp, row_ptr, (n + 1) * sizeof(int), cudaMemcpyHostToDevice), "upload rows");
     ck(cudaMemcpy(H.d_ci, col_ind, H.nnz * sizeof(int), cudaMemcpyHostToDevice), "upload cols");
@@ -1367,6 +1472,7 @@ int mfgpu_autotune(mfgpu_handle* h, int reps, int* choices) {
   if (!h) return MFGPU_ERR_ARG;
   if (h->view) return fail(h, MFGPU_ERR_ARG, "a serving-loop view cannot be autotuned");
   if (reps < 1 || reps > 100) return fail(h, MFGPU_ERR_ARG, "reps must be in [1, 100]");
+  if (h->lu) return fail(h, MFGPU_ERR_ARG, "LU handles (separator widths 2-3) have one kernel per level");
   return guarded(h, [&]() {
     h->factored = false;
     ck(cudaEventRecord(h->ev0, h->stream), "event");
@@ -1384,8 +1490,22 @@ int mfgpu_autotune(mfgpu_handle* h, int reps, int* choices) {
     h->factored = true;
   });
 }
+// Host values replace the matrix: refuse a nonsymmetric one as mfgpu_create
+// does (device-resident values are not checked).
+static int checkSymmetric(mfgpu_handle* h, const double* val) {
+  if (h->lu) return MFGPU_OK;   // widths 2-3: nonsymmetric by nature, factored by LU
+  std::string where;
+  if (const char* why = asymmetry(h->n, h->h_rowptr.data(), h->h_colind.data(), val, where))
+    return fail(h, MFGPU_ERR_ARG, std::string(why) + where +
+                                      ": this library factors symmetric positive definite matrices");
+  return MFGPU_OK;
+}
+
 int mfgpu_refactor(mfgpu_handle* h, const double* val, int64_t nnz) {
+  if (!h) return MFGPU_ERR_ARG;
   if (!val) return fail(h, MFGPU_ERR_ARG, "null values");
+  if (nnz != h->nnz) return fail(h, MFGPU_ERR_ARG, "values must match the pattern given at creation");
+  if (int st = checkSymmetric(h, val)) return st;
   return factorImpl(h, val, nnz, false);
 }
 int mfgpu_refactor_device(mfgpu_handle* h, const double* d_val, int64_t nnz) {
@@ -1401,6 +1521,8 @@ static int updateImpl(mfgpu_handle* h, const double* val, int64_t nnz, const int
     return fail(h, MFGPU_ERR_ARG, "Update(): values must match the factored pattern");
   for (int i = 0; i < nmod; i++)
     if (mod[i] < 0 || mod[i] >= h->n) return fail(h, MFGPU_ERR_ARG, "modified DOF out of range");
+  if (!device)
+    if (int st = checkSymmetric(h, val)) return st;
   return guarded(h, [&]() {
     const Schedule& s = *h->S;
     std::vector<char> dirty;
@@ -1465,7 +1587,7 @@ static int solveOrApply(mfgpu_handle* h, const double* in, double* out, int nrhs
     const int chunk = 16;
     h->stats.iterations = 0;
     h->stats.residual = 0;
-    ck(cudaMemsetAsync(h->d_err, 0, sizeof(DevError), h->stream), "clear error word");
+    h->clearErr();
     ck(cudaEventRecord(h->ev0, h->stream), "event");
     for (int c0 = 0; c0 < nrhs; c0 += chunk) {
       const int nc = std::min(chunk, nrhs - c0);
@@ -1578,6 +1700,9 @@ int mfgpu_solve_device_noalloc(mfgpu_handle* h, const double* d_b, double* d_x, 
   return guarded(h, [&]() {
     double* W = noallocScratch(h->device);
     const int chunk = (int)std::min<int64_t>(16, (int64_t)kNoAllocScratchDoubles / per_rhs);
+    // the error word reports a cooperative sweep's grid barrier that gave up
+    h->clearErr();
+    ck(cudaEventRecord(h->ev0, h->stream), "event");
     for (int c0 = 0; c0 < nrhs; c0 += chunk) {
       const int nc = std::min(chunk, nrhs - c0);
       double* X = d_x + (int64_t)c0 * ld;
@@ -1588,7 +1713,16 @@ int mfgpu_solve_device_noalloc(mfgpu_handle* h, const double* d_b, double* d_x, 
              "copy rhs");
       h->solveChunkScratch(X, ld, nc, W);
     }
-    ck(cudaStreamSynchronize(h->stream), "solve");
+    ck(cudaEventRecord(h->ev1, h->stream), "event");
+    h->checkDevError();   // synchronises the stream
+    float ms = 0;
+    ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "elapsed");
+    h->stats.seconds = ms * 1e-3;
+    double fl = 0;
+    for (const mfgpu::Front& f : h->S->fronts) fl += 2.0 * ((double)f.n * f.n + 2.0 * f.n * f.m);
+    h->stats.flops = fl * nrhs;
+    h->stats.iterations = 0;
+    h->stats.residual = 0;
   });
 }
 
@@ -1659,6 +1793,14 @@ int mfgpu_stencil_update_device(mfgpu_handle* h, const double* d_coef, const dou
   });
 }
 
+int mfgpu_set_wait_limit(mfgpu_handle* h, unsigned polls) {
+  if (!h) return MFGPU_ERR_ARG;
+  h->errInit.limit = polls;
+  return MFGPU_OK;
+}
+
+void mfgpu_inject_alloc_failure(long long after) { g_alloc_budget.store(after < 0 ? -1 : after); }
+
 int mfgpu_set_stream(mfgpu_handle* h, void* st) {
   if (!h) return MFGPU_ERR_ARG;
   return guarded(h, [&]() {
@@ -1721,6 +1863,7 @@ std::vector<std::pair<void*, size_t>> facBlocks(const mfgpu_handle* h) {
     b.push_back({h->d_iscale, (size_t)h->n * sizeof(double)});
   }
   if (h->dinvElems > 0) b.push_back({h->d_Dinv, (size_t)h->dinvElems * h->esz});
+  if (h->lu) b.push_back({h->d_ipiv, h->S->dofs.size() * sizeof(int)});
   return b;
 }
 
@@ -2314,6 +2457,7 @@ std::unique_ptr<mfgpu_handle> makeView(mfgpu_handle& B) {
   H.lvMaxn = B.lvMaxn;
   H.solveCoopMinN = B.solveCoopMinN;
   H.stepped = B.stepped;
+  H.errInit = B.errInit;
   ck(cudaStreamCreateWithFlags(&H.own, cudaStreamNonBlocking), "create stream");
   H.stream = H.own;
   ck(cudaEventCreate(&H.ev0), "event");

@@ -20,7 +20,13 @@ from ._lib import MFGPU_FP64, MFGPU_MIXED, TASK_DTYPE
 from .stencil import CSR, build_laplacian
 
 __all__ = ["MF2D", "MF3D", "MFBatch", "Server", "Symbolic", "CSR", "build_laplacian", "MFGPU_FP64",
-           "MFGPU_MIXED", "MFError"]
+           "MFGPU_MIXED", "MFError", "inject_alloc_failure"]
+
+
+def inject_alloc_failure(after):
+    """Test hook: the next `after` device allocations succeed, the one after
+    fails as out of memory (MFGPU_ERR_OOM); after < 0 disarms."""
+    _lib.load().mfgpu_inject_alloc_failure(int(after))
 
 
 class MFError(RuntimeError):
@@ -203,6 +209,11 @@ class _MFBase:
 
     def set_stream(self, stream_ptr):
         self._check(self._lib.mfgpu_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def set_wait_limit(self, polls):
+        """Poll limit of the bounded device waits of later calls (0: built-in);
+        a wait that gives up raises MFError with status MFGPU_ERR_TIMEOUT."""
+        self._check(self._lib.mfgpu_set_wait_limit(self._h, int(polls)))
 
     def info(self):
         inf = _lib.Info()

@@ -34,6 +34,7 @@ EXPORTED = [
     "mfgpu_symbolic_batch_create", "mfgpu_stencil_assemble_device", "mfgpu_stencil_update_device",
     "mfgpu_server_create", "mfgpu_server_submit", "mfgpu_server_wait", "mfgpu_server_last_error",
     "mfgpu_server_destroy", "mfgpu_save", "mfgpu_load", "mfgpu_autotune", "mfgpu_symbolic_create_full",
+    "mfgpu_solve_device_noalloc", "mfgpu_set_wait_limit", "mfgpu_inject_alloc_failure",
 ]
 
 KERNEL_CLASSES = ["assemble", "potrf", "trsm", "syrk", "solve", "apply", "front", "coop", "tc"]
@@ -119,6 +120,12 @@ def load(path=None):
     lib.mfgpu_kernel_launches.argtypes = []
     lib.mfgpu_kernel_launches.restype = C.c_longlong
     lib.mfgpu_set_stream.argtypes = [P, C.c_void_p]
+    lib.mfgpu_solve_device_noalloc.argtypes = [P, C.c_void_p, C.c_void_p, C.c_int, C.c_int64]
+    lib.mfgpu_solve_device_noalloc.restype = C.c_int
+    lib.mfgpu_set_wait_limit.argtypes = [P, C.c_uint]
+    lib.mfgpu_set_wait_limit.restype = C.c_int
+    lib.mfgpu_inject_alloc_failure.argtypes = [C.c_longlong]
+    lib.mfgpu_inject_alloc_failure.restype = None
     lib.mfgpu_save.argtypes = [P, C.c_char_p]
     lib.mfgpu_save.restype = C.c_int
     lib.mfgpu_load.argtypes = [P, C.c_char_p]
