@@ -77,10 +77,16 @@ const char* mfgpu_status_string(int status);
 /* MF2D(const Sparse&, Nx, Ny, width, maxSideLength) — include/DE/mf.hpp:74;
  * MF3D(const Sparse&, Nx, Ny, Nz, width, maxSideLength) — include/DE/mf.hpp:180.
  * dim = 2 ignores nz.  The CSR (row_ptr[n+1], col_ind[nnz], val[nnz]) is copied.
- * Only width = 1 (5-/7-point stencils) is supported on the GPU path.  The
- * matrix must be symmetric positive definite: one that is not symmetric (to a
+ * width = 1 (5-/7-point stencils): the matrix must be symmetric positive
+ * definite and is factored by Cholesky; one that is not symmetric (to a
  * relative 1e-12) is refused with MFGPU_ERR_ARG, naming the first unequal
- * pair; indefiniteness surfaces as MFGPU_ERR_PIVOT in the factorization. */
+ * pair; indefiniteness surfaces as MFGPU_ERR_PIVOT in the factorization.
+ * width = 2 or 3 (the reference fixture's wider stencils, nonsymmetric with
+ * variable coefficients): every front is factored by LU with partial pivoting
+ * inside its pivot block, as the reference's dgetrf on A22
+ * (include/LinAlg/dense.hpp:180-227); FP64 only (MFGPU_ERR_ARG otherwise), no
+ * batches, serving loop or autotuner; a singular pivot block surfaces as
+ * MFGPU_ERR_PIVOT. */
 int mfgpu_create(int dim, int nx, int ny, int nz, int width, int max_side_length, int n,
                  const int* row_ptr, const int* col_ind, const double* val,
                  const mfgpu_options* opts, mfgpu_handle** out);

@@ -148,19 +148,26 @@ cudaError_t launch_trail_tc(const int* flist, int nf, int64_t ntiles, const Fron
                             int K, int w, int cend, int split, int cap, const void* pack,
                             DevError* err, cudaStream_t st);
 
-// Cooperative sweeps over all fronts of one level (at most
-// solve_coop_max_fronts() fronts, nrhs <= 16): forward = gather, L11 solve
-// and boundary update; backward = gather, L21^T update and L11^T solve.
+// Cooperative sweeps over all fronts of one level (nrhs <= 16), ordered by
+// ready flags instead of grid barriers: forward = L11 solve and boundary update
+// b_bd -= L21 y, backward = L21^T update and L11^T solve, both gathering from
+// and scattering to X themselves.  flow_tasks builds a level's task lists
+// (front slot, block) pairs, forward R-major and backward by distance from
+// each front's last block, and the per-front offsets of the ready flags
+// (flagoff[nf] = flags needed); `flags` is cleared before every launch.
 int solve_coop_max_fronts();
-// The cooperative sweeps apply each 64 x 64 pivot block through its explicit
-// inverse (Dv, per front at dinv_off, written by launch_diag_inv after the
-// front is factored) and keep solved blocks in the second half of the front's
-// workspace, so a step needs no single-CTA substitution.
+void flow_tasks(const std::vector<int>& n, const std::vector<int>& N, std::vector<int>& fwd,
+                std::vector<int>& bwd, std::vector<int>& flagoff);
+// The sweeps apply each 64 x 64 pivot block through its explicit inverse (Dv,
+// per front at dinv_off, written by launch_diag_inv after the front is
+// factored) and keep solved blocks in the second half of the front's
+// workspace, where other tasks read them.
 template <class T>
-cudaError_t launch_solve_coop(bool forward, const int* flist, int nf, int maxn, const FrontDev* fr,
-                              const T* F, const int* dofs, T* X, int64_t ldx, int nrhs, T* W,
+cudaError_t launch_solve_flow(bool forward, const int* flist, const FrontDev* fr, const T* F,
+                              const int* dofs, T* X, int64_t ldx, int nrhs, T* W,
                               const int64_t* woff, const T* Dv, const int64_t* dinv_off,
-                              unsigned* gbar, DevError* err, cudaStream_t st);
+                              const int* tasks, int ntasks, const int* flagoff, int* flags,
+                              int nflags, DevError* err, cudaStream_t st);
 constexpr int kDinvBlock = 64;   // diagonal-block size of the cooperative sweeps
 template <class T>
 void launch_diag_inv(const int* flist, int nf, int maxn, const FrontDev* fr, const T* F, T* Dv,

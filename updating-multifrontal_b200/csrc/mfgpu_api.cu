@@ -264,6 +264,16 @@ struct mfgpu_handle {
   void* d_tcpack = nullptr;    // tensor-core panel images (mixed path)
   size_t tcPackCap = 0;
   unsigned* d_gbar = nullptr;  // grid-barrier arrival counter of the cooperative kernels
+  // Cooperative (flag-ordered) sweeps: per level, its forward / backward task
+  // lists and flag offsets in d_flow; the ready flags of one launch in d_flags.
+  struct FlowLevel {
+    int64_t fwd = 0, bwd = 0, flagoff = 0;
+    int nfwd = 0, nbwd = 0, nflags = 0;
+  };
+  std::vector<FlowLevel> flow;
+  int* d_flow = nullptr;       // shared with serving-loop views
+  int* d_flags = nullptr;      // per handle (views have their own)
+  int maxFlags = 0;
   void* d_Dinv = nullptr;      // inverses of the cooperative-sweep levels' 64 x 64 pivot blocks
   int64_t* d_dinv_off = nullptr;   // per front: element offset in d_Dinv, -1 outside those levels
   int64_t dinvElems = 0;
@@ -344,7 +354,9 @@ struct mfgpu_handle {
       cudaFree(d_all);
       cudaFree(d_dinv_off);
       cudaFree(d_ipiv);
+      cudaFree(d_flow);
     }
+    cudaFree(d_flags);
     cudaFree(d_Dinv);
     cudaFree(d_val);
     cudaFree(d_fr);
@@ -599,7 +611,6 @@ struct mfgpu_handle {
   template <class T>
   void runPlanT(const Plan& P) {
     const Schedule& s = *S;
-    T* F = (T*)d_F;
     size_t pack = P.tcPackBytes;   // tuned tensor-core levels may need more than the rules
     if (&P == &full)
       for (int ell = 0; ell < s.levels && ell < (int)tuned.size(); ell++)
@@ -917,10 +928,13 @@ struct mfgpu_handle {
       ck(cudaGetLastError(), forward ? "launch LU forward sweep (k_lu_solve_fwd)"
                                      : "launch LU backward sweep (k_lu_solve_bwd)");
     } else if (coopSweep(ell)) {
-      ck(mfgpu::launch_solve_coop<T>(forward, fl, nf, lvMaxn[ell], d_fr, F, d_dofs, X, ldx, nrhs, W,
-                                     d_woff, (const T*)d_Dinv, d_dinv_off, d_gbar, d_err, stream),
-         forward ? "launch cooperative forward sweep (k_solve_coop_fwd)"
-                 : "launch cooperative backward sweep (k_solve_coop_bwd)");
+      const FlowLevel& q = flow[ell];
+      ck(mfgpu::launch_solve_flow<T>(forward, fl, d_fr, F, d_dofs, X, ldx, nrhs, W, d_woff,
+                                     (const T*)d_Dinv, d_dinv_off,
+                                     d_flow + (forward ? q.fwd : q.bwd), forward ? q.nfwd : q.nbwd,
+                                     d_flow + q.flagoff, d_flags, q.nflags, d_err, stream),
+         forward ? "launch cooperative forward sweep (k_solve_flow_fwd)"
+                 : "launch cooperative backward sweep (k_solve_flow_bwd)");
     } else if (forward) {
       mfgpu::launch_solve_fwd<T>(fl, nf, lvMaxN[ell], d_fr, F, d_dofs, X, ldx, nrhs, W, d_woff,
                                  stream);
@@ -1400,6 +1414,35 @@ int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const
         }
       H.dinvElems = cur;
       H.d_Dinv = dalloc<unsigned char>(std::max<int64_t>(cur, 1) * H.esz, "alloc block inverses");
+      // task lists of the cooperative sweeps, per level
+      std::vector<int> tab;
+      H.flow.assign(s.levels, mfgpu_handle::FlowLevel());
+      for (int ell = 0; ell < s.levels; ell++) {
+        if (!H.coopSweep(ell)) continue;
+        std::vector<int> nn, NN, fw, bw, fo;
+        for (int b = 0; b < s.lv[ell].nbox; b++) {
+          nn.push_back(s.fronts[s.lv[ell].front0 + b].n);
+          NN.push_back(s.fronts[s.lv[ell].front0 + b].N);
+        }
+        mfgpu::flow_tasks(nn, NN, fw, bw, fo);
+        mfgpu_handle::FlowLevel& q = H.flow[ell];
+        q.fwd = (int64_t)tab.size();
+        q.nfwd = (int)fw.size() / 2;
+        tab.insert(tab.end(), fw.begin(), fw.end());
+        q.bwd = (int64_t)tab.size();
+        q.nbwd = (int)bw.size() / 2;
+        tab.insert(tab.end(), bw.begin(), bw.end());
+        q.flagoff = (int64_t)tab.size();
+        q.nflags = fo.back();
+        tab.insert(tab.end(), fo.begin(), fo.end());
+        H.maxFlags = std::max(H.maxFlags, q.nflags);
+        if (tab.size() % 2) tab.push_back(0);   // keep the next level's pairs 8-byte aligned
+      }
+      H.d_flow = dalloc<int>(std::max<size_t>(tab.size(), 2), "alloc sweep task lists");
+      if (!tab.empty())
+        ck(cudaMemcpy(H.d_flow, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice),
+           "upload sweep task lists");
+      H.d_flags = dalloc<int>(std::max(H.maxFlags, 1), "alloc sweep ready flags");
       H.d_dinv_off = dalloc<int64_t>(doff.size(), "alloc block inverse offsets");
       ck(cudaMemcpy(H.d_dinv_off, doff.data(), doff.size() * sizeof(int64_t),
                     cudaMemcpyHostToDevice), "upload block inverse offsets");
@@ -2469,6 +2512,10 @@ std::unique_ptr<mfgpu_handle> makeView(mfgpu_handle& B) {
   H.d_gbar = dalloc<unsigned>(1, "alloc grid barrier");
   H.dinvElems = B.dinvElems;
   H.d_dinv_off = B.d_dinv_off;
+  H.flow = B.flow;
+  H.d_flow = B.d_flow;
+  H.maxFlags = B.maxFlags;
+  H.d_flags = dalloc<int>(std::max(B.maxFlags, 1), "alloc sweep ready flags");
   H.d_Dinv = dalloc<unsigned char>(std::max<int64_t>(B.dinvElems, 1) * H.esz, "alloc block inverses");
   if (H.mixed) {
     H.d_sc = dalloc<double>(80 * (size_t)H.nseg, "alloc refinement scalars");
