@@ -220,6 +220,18 @@ int mfgpu_solve_device_noalloc(mfgpu_handle* h, const double* d_b, double* d_x, 
  * the handle's own stream. */
 int mfgpu_set_stream(mfgpu_handle* h, void* cuda_stream);
 
+/* CUDA graphs (no reference counterpart).  A handle replays the launches of
+ * its full factorization (every level's assembly, partial factorization and
+ * separator accumulation: the level schedule) as one captured CUDA graph from
+ * the second full factorization on, and likewise the solve sweeps (FP64) or
+ * the preconditioner applications of the refinement (mixed) per right-hand-
+ * side buffer and count from their second use; localized updates, whose fronts
+ * change from call to call, and the no-allocation solve launch directly.
+ * Results are bit-identical either way.  MFGPU_GRAPHS=0 in the environment at
+ * creation turns graphs off.  mfgpu_graphs reports whether the factorization
+ * graph exists and how many sweep graphs are held. */
+int mfgpu_graphs(const mfgpu_handle* h, int* factor_graph, int* sweep_graphs);
+
 /* Failure handling (no reference counterpart: the reference has no device
  * waits, and its LAPACK failures abort through assert, include/LinAlg/dense.hpp:187).
  * Every device wait of this library is bounded: the grid barriers of the

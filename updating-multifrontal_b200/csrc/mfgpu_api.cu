@@ -5,12 +5,14 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <memory>
 #include <mutex>
 #include <chrono>
 #include <map>
+#include <tuple>
 #include <deque>
 #include <condition_variable>
 #include <thread>
@@ -259,7 +261,17 @@ struct mfgpu_handle {
   SepDev* d_sp = nullptr;
   int64_t* d_woff = nullptr;
   DevError* d_err = nullptr;
-  DevError errInit{};              // what d_err is reset to before a call: code 0, the poll limit
+  unsigned waitLimit = 0;          // poll limit of the bounded device waits (0: built-in), kept in d_err
+  // CUDA graphs: the full factorization's level schedule and the solve sweeps
+  // (FP64) / preconditioner applications (mixed) per right-hand-side buffer
+  // and count, captured once their launches have run eagerly and replayed
+  // with one cudaGraphLaunch.  MFGPU_GRAPHS=0 turns them off; a capture the
+  // runtime refuses turns them off for the handle.
+  bool graphs = true;
+  int fullRuns = 0;
+  cudaGraphExec_t fullGraph = nullptr;
+  std::map<std::tuple<const void*, const void*, int>, cudaGraphExec_t> sweepGraphs;
+  std::map<std::tuple<const void*, const void*, int>, int> sweepSeen;
   void* d_slots = nullptr;     // diagonal-block hand-off slots of the cooperative kernel
   void* d_tcpack = nullptr;    // tensor-core panel images (mixed path)
   size_t tcPackCap = 0;
@@ -378,6 +390,7 @@ struct mfgpu_handle {
     cudaFree(d_active);
     cudaFree(d_flag);
     cudaFree(d_modbuf);
+    dropGraphs(true, true);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (own) cudaStreamDestroy(own);
@@ -530,8 +543,64 @@ struct mfgpu_handle {
     return b;
   }
 
+  void dropGraphs(bool factor, bool sweep) {
+    if (factor && fullGraph) {
+      cudaGraphExecDestroy(fullGraph);
+      fullGraph = nullptr;
+    }
+    if (sweep) {
+      for (auto& kv : sweepGraphs)
+        if (kv.second) cudaGraphExecDestroy(kv.second);
+      sweepGraphs.clear();
+      sweepSeen.clear();
+    }
+  }
+
+  // The work fn enqueues on the stream, captured as an executable graph; null
+  // (and graphs off for this handle) when the runtime refuses the capture.
+  template <class Fn>
+  cudaGraphExec_t capture(Fn&& fn) {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      graphs = false;
+      return nullptr;
+    }
+    bool ok = true;
+    try {
+      fn();
+    } catch (const CudaError&) {
+      ok = false;
+    }
+    if (cudaStreamEndCapture(stream, &g) != cudaSuccess || !ok || !g ||
+        cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) {
+      ex = nullptr;
+      graphs = false;
+    }
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();   // a refused capture leaves its error behind
+    return ex;
+  }
+
+  // Launch the graph of (a, b, nc), capturing it on the second call with that
+  // key; otherwise run fn directly.
+  template <class Fn>
+  void sweepGraph(const void* a, const void* b, int nc, Fn&& fn) {
+    if (!graphs || prof.verbose) return fn();
+    const auto key = std::make_tuple(a, b, nc);
+    auto it = sweepGraphs.find(key);
+    if (it == sweepGraphs.end() && ++sweepSeen[key] >= 2) {
+      cudaGraphExec_t ex = capture(fn);
+      if (ex) it = sweepGraphs.emplace(key, ex).first;
+    }
+    if (it == sweepGraphs.end()) return fn();
+    ck(cudaGraphLaunch(it->second, stream), "launch sweep graph");
+  }
+
   void ensurePack(size_t bytes) {
     if (bytes <= tcPackCap) return;
+    dropGraphs(true, false);   // the captured factorization reads the old pack
     ck(cudaStreamSynchronize(stream), "sync before growing the panel pack");
     cudaFree(d_tcpack);
     d_tcpack = nullptr;
@@ -616,6 +685,20 @@ struct mfgpu_handle {
       for (int ell = 0; ell < s.levels && ell < (int)tuned.size(); ell++)
         if (tuned[ell] == LK_TC) pack = std::max(pack, levelPackBytes(P, P.lv[ell]));
     ensurePack(pack);
+    // the full factorization's schedule as one graph, from its second run on
+    if (&P == &full && graphs && !prof.on && fullRuns++ > 0) {
+      if (!fullGraph) fullGraph = capture([&] { enqueuePlanT<T>(P); });
+      if (fullGraph) {
+        ck(cudaGraphLaunch(fullGraph, stream), "launch factorization graph");
+        return;
+      }
+    }
+    enqueuePlanT<T>(P);
+  }
+
+  template <class T>
+  void enqueuePlanT(const Plan& P) {
+    const Schedule& s = *S;
     clearErr();
     for (int ell = s.levels - 1; ell >= 0; ell--) {
       const Plan::Level& L = P.lv[ell];
@@ -833,12 +916,16 @@ struct mfgpu_handle {
     runPlan(P);
   }
 
-  // Reset the error word before a call's launches; it also carries the poll
-  // limit of the bounded device waits (mfgpu_set_wait_limit).  errInit lives as
-  // long as the handle, so the asynchronous copy may read it late.
+  // Reset the error word before a call's launches (a memset, so it can be
+  // captured in a graph); its poll-limit field is written only by setLimit.
   void clearErr() {
-    ck(cudaMemcpyAsync(d_err, &errInit, sizeof(DevError), cudaMemcpyHostToDevice, stream),
-       "clear error word");
+    ck(cudaMemsetAsync(d_err, 0, offsetof(DevError, limit), stream), "clear error word");
+  }
+  void setLimit(unsigned polls) {
+    waitLimit = polls;
+    ck(cudaMemcpyAsync(&d_err->limit, &waitLimit, sizeof(unsigned), cudaMemcpyHostToDevice, stream),
+       "set wait limit");
+    ck(cudaStreamSynchronize(stream), "set wait limit");
   }
 
   void checkDevError() {
@@ -874,6 +961,7 @@ struct mfgpu_handle {
   template <class P>
   void growBuf(P*& p, size_t& cap, size_t need, const char* what) {
     if (need <= cap) return;
+    dropGraphs(false, true);   // captured sweeps read the old buffers
     cudaFree(p);
     p = nullptr;
     p = dalloc<P>(need, what);
@@ -1018,9 +1106,11 @@ struct mfgpu_handle {
 
   // z = M^{-1} r with the scaled FP32 factorization: z = s .* (S^{-1} (s .* r)).
   void precond(const double* r, double* z, int nc) {
-    mfgpu::launch_scale_to<float>(r, n, d_x32, n, d_scale, n, nc, stream);
-    sweeps<float>(d_x32, n, nc, (float*)d_Wd);
-    mfgpu::launch_scale_from<float>(d_x32, n, z, n, d_scale, n, nc, stream);
+    sweepGraph(r, z, nc, [&] {
+      mfgpu::launch_scale_to<float>(r, n, d_x32, n, d_scale, n, nc, stream);
+      sweeps<float>(d_x32, n, nc, (float*)d_Wd);
+      mfgpu::launch_scale_from<float>(d_x32, n, z, n, d_scale, n, nc, stream);
+    });
   }
 
   void dots(const double* x, const double* y, int nc, double* out) {
@@ -1105,7 +1195,7 @@ struct mfgpu_handle {
   // Solve in place on device data X (n x nrhs, ld = n), nrhs <= 16.
   void solveChunk(double* X, int nrhs) {
     if (mixed) pcg(X, nrhs);
-    else sweeps<double>(X, n, nrhs, (double*)d_Wd);
+    else sweepGraph(X, d_Wd, nrhs, [&] { sweeps<double>(X, n, nrhs, (double*)d_Wd); });
     ck(cudaGetLastError(), "solve launch");
   }
 
@@ -1352,6 +1442,7 @@ int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const
   if (const char* e = getenv("MFGPU_TC_SPLIT")) h->tcSplit = atoi(e) == 1 ? 1 : 3;
   if (const char* e = getenv("MFGPU_TC_SPLIT3_LEVELS")) h->tcSplit3Levels = atoi(e);
   if (const char* e = getenv("MFGPU_TC_SUB")) h->tcSub = atoi(e);
+  if (const char* e = getenv("MFGPU_GRAPHS")) h->graphs = e[0] != '0';
   if (h->lu) h->solveCoopMinN = 0;   // LU fronts use the per-front sweeps
   h->h_rowptr.assign(row_ptr, row_ptr + n + 1);
   h->h_colind.assign(col_ind, col_ind + h->nnz);
@@ -1459,6 +1550,7 @@ int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const
     H.d_sp = dalloc<SepDev>(std::max<size_t>(1, sp.size()), "alloc seps");
     H.d_woff = dalloc<int64_t>(woff.size(), "alloc woff");
     H.d_err = dalloc<DevError>(1, "alloc error word");
+    ck(cudaMemset(H.d_err, 0, sizeof(DevError)), "clear error word");
     H.d_slots = dalloc<unsigned char>(mfgpu::coop_slot_elems() * H.esz, "alloc diagonal slots");
     H.d_gbar = dalloc<unsigned>(1, "alloc grid barrier");
     H.d_all = dalloc<int>(all.size(), "alloc id list");
@@ -1520,6 +1612,8 @@ int mfgpu_autotune(mfgpu_handle* h, int reps, int* choices) {
     h->factored = false;
     ck(cudaEventRecord(h->ev0, h->stream), "event");
     try {   // a tuning that fails part-way leaves the size rules in force
+      h->dropGraphs(true, false);   // the level kernels change
+      h->fullRuns = 0;
       if (h->mixed) h->autotuneT<float>(reps, choices);
       else h->autotuneT<double>(reps, choices);
       h->checkDevError();
@@ -1838,7 +1932,13 @@ int mfgpu_stencil_update_device(mfgpu_handle* h, const double* d_coef, const dou
 
 int mfgpu_set_wait_limit(mfgpu_handle* h, unsigned polls) {
   if (!h) return MFGPU_ERR_ARG;
-  h->errInit.limit = polls;
+  return guarded(h, [&]() { h->setLimit(polls); });
+}
+
+int mfgpu_graphs(const mfgpu_handle* h, int* factor_graph, int* sweep_graphs) {
+  if (!h) return MFGPU_ERR_ARG;
+  if (factor_graph) *factor_graph = h->fullGraph ? 1 : 0;
+  if (sweep_graphs) *sweep_graphs = (int)h->sweepGraphs.size();
   return MFGPU_OK;
 }
 
@@ -2500,7 +2600,6 @@ std::unique_ptr<mfgpu_handle> makeView(mfgpu_handle& B) {
   H.lvMaxn = B.lvMaxn;
   H.solveCoopMinN = B.solveCoopMinN;
   H.stepped = B.stepped;
-  H.errInit = B.errInit;
   ck(cudaStreamCreateWithFlags(&H.own, cudaStreamNonBlocking), "create stream");
   H.stream = H.own;
   ck(cudaEventCreate(&H.ev0), "event");
@@ -2508,6 +2607,8 @@ std::unique_ptr<mfgpu_handle> makeView(mfgpu_handle& B) {
   H.d_fr = dalloc<FrontDev>(B.S->fronts.size(), "alloc view front table");
   H.d_val = dalloc<double>(B.nnz, "alloc view values");
   H.d_err = dalloc<DevError>(1, "alloc error word");
+  ck(cudaMemsetAsync(H.d_err, 0, sizeof(DevError), H.stream), "clear error word");
+  H.setLimit(B.waitLimit);   // the base's poll limit
   H.d_slots = dalloc<unsigned char>(mfgpu::coop_slot_elems() * H.esz, "alloc diagonal slots");
   H.d_gbar = dalloc<unsigned>(1, "alloc grid barrier");
   H.dinvElems = B.dinvElems;

@@ -210,6 +210,12 @@ class _MFBase:
     def set_stream(self, stream_ptr):
         self._check(self._lib.mfgpu_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
 
+    def graphs(self):
+        """(factorization graph captured, number of sweep graphs held)."""
+        fg, sg = C.c_int(), C.c_int()
+        self._check(self._lib.mfgpu_graphs(self._h, C.byref(fg), C.byref(sg)))
+        return bool(fg.value), sg.value
+
     def set_wait_limit(self, polls):
         """Poll limit of the bounded device waits of later calls (0: built-in);
         a wait that gives up raises MFError with status MFGPU_ERR_TIMEOUT."""

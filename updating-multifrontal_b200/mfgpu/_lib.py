@@ -35,6 +35,7 @@ EXPORTED = [
     "mfgpu_server_create", "mfgpu_server_submit", "mfgpu_server_wait", "mfgpu_server_last_error",
     "mfgpu_server_destroy", "mfgpu_save", "mfgpu_load", "mfgpu_autotune", "mfgpu_symbolic_create_full",
     "mfgpu_solve_device_noalloc", "mfgpu_set_wait_limit", "mfgpu_inject_alloc_failure",
+    "mfgpu_graphs",
 ]
 
 KERNEL_CLASSES = ["assemble", "potrf", "trsm", "syrk", "solve", "apply", "front", "coop", "tc"]
@@ -126,6 +127,8 @@ def load(path=None):
     lib.mfgpu_set_wait_limit.restype = C.c_int
     lib.mfgpu_inject_alloc_failure.argtypes = [C.c_longlong]
     lib.mfgpu_inject_alloc_failure.restype = None
+    lib.mfgpu_graphs.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    lib.mfgpu_graphs.restype = C.c_int
     lib.mfgpu_save.argtypes = [P, C.c_char_p]
     lib.mfgpu_save.restype = C.c_int
     lib.mfgpu_load.argtypes = [P, C.c_char_p]
