@@ -883,7 +883,7 @@ def roofline(torch, dom, P, peaks, peak_src, args):
               "traffic": traffic_for(kern, args.workload, args.precision)}
     ach = P["flops"] / (P["ms"] * 1e-3) / 1e12
     if dom == "tc":
-        split = int(os.environ.get("MFGPU_TC_SPLIT", "3"))
+        split = {"1": 1, "tf32": 1, "bf16": 1}.get(os.environ.get("MFGPU_TC_SPLIT", "3"), 3)
         pk = float(peaks["bf16_tflops"]) / 2.0
         return dict(common, bound="tensor", achieved=ach, peak=pk, unit="TFLOP/s", frac=ach / pk,
                     achieved_executed=ach * split,

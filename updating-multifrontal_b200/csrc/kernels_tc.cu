@@ -31,6 +31,8 @@
 //         accumulators (256 columns each, all of tensor memory):
 //             SPLIT = 3:  acc += hi_a hi_b^T + hi_a lo_b^T + lo_a hi_b^T
 //             SPLIT = 1:  acc += hi_a hi_b^T
+//             SPLIT = 2:  acc += a b^T in BF16 (kind::f16, K = 16; the pack
+//                         writes BF16 images of 32 columns, the same 8 KB size)
 //         and hands stages back to the producer with tcgen05.commit;
 //       - eight epilogue warps (two per accumulator lane quarter, 128 columns
 //         each, 32 at a time) read the accumulator with tcgen05.ld and
@@ -47,6 +49,8 @@
 // records error code 2 in the error word, skips the remaining work, waits for
 // its own copies and products in flight, releases its tensor memory and
 // returns.
+#include <cuda_bf16.h>
+
 #include <atomic>
 #include <cstdint>
 
@@ -60,7 +64,8 @@ namespace {
 
 constexpr int TM = 128;                    // C tile rows = accumulator lanes = image rows
 constexpr int TN = 256;                    // C tile columns = accumulator columns
-constexpr int TK = 16;                     // panel columns per chunk (64-byte image rows)
+constexpr int TK = 16;                     // TF32: panel columns per chunk (64-byte image rows)
+constexpr int TK16 = 32;                   // BF16: panel columns per chunk (64-byte image rows)
 constexpr int NSTAGE = 4;                  // shared-memory stages
 constexpr int NACC = 2;                    // tensor-memory accumulators
 constexpr int MMA_WARP = 1;                // warp 0 produces, warp 1 issues the MMAs
@@ -81,9 +86,16 @@ __host__ __device__ constexpr int img_off(int m, int k) {
   return m * 64 + ((((k >> 2) ^ ((m >> 1) & 3))) << 4) + (k & 3) * 4;
 }
 
-// Instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = 256.
+// Instruction descriptors: D = F32, both operands K-major, M = 128, N = 256;
+// A = B = TF32 (kind::tf32) or A = B = BF16 (kind::f16; never mixed types).
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TN >> 3) << 17) |
                             ((uint32_t)(TM >> 4) << 24);
+constexpr uint32_t kIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                                ((uint32_t)(TM >> 4) << 24);
+
+// Panel columns per chunk of each mode: SPLIT = 3 three-term TF32, 1 plain
+// TF32 (16 columns), 2 plain BF16 (one product, 32 columns).
+__host__ __device__ constexpr int chunk_cols(int split) { return split == 2 ? TK16 : TK; }
 
 // Panel geometry of a front for the panel [K, K + w): k1, 128-row blocks
 // below k1, 16-column chunks in [K, k1), the column bound cmax (cend < 0: N,
@@ -93,7 +105,7 @@ constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TN 
 struct PanelGeo {
   int k1, nb, nch, cmax, nj;
 };
-__host__ __device__ inline PanelGeo panel_geo(int n, int N, int K, int w, int cend) {
+__host__ __device__ inline PanelGeo panel_geo(int n, int N, int K, int w, int cend, int tk = TK) {
   PanelGeo g{0, 0, 0, 0, 0};
   if (K >= n) return g;
   g.k1 = n < K + w ? n : K + w;
@@ -101,7 +113,7 @@ __host__ __device__ inline PanelGeo panel_geo(int n, int N, int K, int w, int ce
   g.cmax = cend < 0 ? N : (cend < n ? cend : n);
   if (g.cmax <= g.k1) return g;
   g.nb = (N - g.k1 + TM - 1) / TM;
-  g.nch = (g.k1 - K + TK - 1) / TK;
+  g.nch = (g.k1 - K + tk - 1) / tk;
   g.nj = (g.cmax - g.k1 + TN - 1) / TN;   // <= (nb + 1) / 2 since cmax <= N
   return g;
 }
@@ -213,6 +225,14 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b
       "l"(a), "l"(b), "r"(kIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(kIdescBf16), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                    smem_u32(bar))
@@ -253,7 +273,7 @@ struct TileInfo {
 
 __device__ __forceinline__ TileInfo tile_info(const int* pre, int nf, const int* flist,
                                               const FrontDev* fr, float* F, int K, int w, int cend,
-                                              int tile) {
+                                              int tile, int tk) {
   int lo = 0, hi = nf - 1;   // largest i with pre[i] <= tile
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
@@ -261,7 +281,7 @@ __device__ __forceinline__ TileInfo tile_info(const int* pre, int nf, const int*
     else hi = mid - 1;
   }
   const FrontDev d = fr[flist[lo]];
-  const PanelGeo g = panel_geo(d.n, d.N, K, w, cend);
+  const PanelGeo g = panel_geo(d.n, d.N, K, w, cend, tk);
   TileInfo t;
   t.A = F + d.off;
   t.ld = d.ld;
@@ -289,14 +309,33 @@ __global__ void __launch_bounds__(128) k_tc_pack(const int* __restrict__ flist,
                                                  int cap, unsigned char* __restrict__ pack) {
   __shared__ __align__(1024) unsigned char img[2 * IMG];
   const FrontDev d = fr[flist[blockIdx.y]];
-  const PanelGeo g = panel_geo(d.n, d.N, K, w, -1);
+  constexpr int tk = chunk_cols(SPLIT);
+  const PanelGeo g = panel_geo(d.n, d.N, K, w, -1, tk);
   const int x = blockIdx.x;
   if (x >= g.nb * g.nch) return;
   const int c = x / g.nb, b = x - c * g.nb, t = threadIdx.x;
-  const int row = g.k1 + b * TM + t, kc = K + c * TK;
+  const int row = g.k1 + b * TM + t, kc = K + c * tk;
   const bool row_ok = row < d.N;
   const float* src = F + d.off + (row_ok ? row : 0) + (int64_t)kc * d.ld;
   const int kend = g.k1 - kc;   // columns of this chunk inside the panel
+  if (SPLIT == 2) {
+    // BF16 (round to nearest even): 32 columns, 16-byte chunks of 8 values,
+    // the 64-byte swizzle of the TF32 images on 16-byte units
+#pragma unroll
+    for (int q = 0; q < TK16 / 8; q++) {
+      uint32_t pk[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int k0 = 8 * q + 2 * j;
+        const float v0 = (row_ok && k0 < kend) ? __ldg(src + (int64_t)k0 * d.ld) : 0.0f;
+        const float v1 = (row_ok && k0 + 1 < kend) ? __ldg(src + (int64_t)(k0 + 1) * d.ld) : 0.0f;
+        const __nv_bfloat162 h2 = __floats2bfloat162_rn(v0, v1);   // .x = v0 at the lower address
+        pk[j] = *reinterpret_cast<const uint32_t*>(&h2);
+      }
+      *reinterpret_cast<uint4*>(img + t * 64 + ((q ^ ((t >> 1) & 3)) << 4)) =
+          make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    }
+  } else {
 #pragma unroll
   for (int q = 0; q < TK / 4; q++) {
     float v[4];
@@ -318,6 +357,7 @@ __global__ void __launch_bounds__(128) k_tc_pack(const int* __restrict__ flist,
       l.w = tf32_round(v[3] - h.w);
       *reinterpret_cast<float4*>(img + IMG + img_off(t, 4 * q)) = l;
     }
+  }
   }
   __syncthreads();
   unsigned char* base = pack + (int64_t)blockIdx.y * cap * 2 * IMG;
@@ -389,7 +429,7 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
       uint32_t g = 0;
       bool ok = true;
       for (int tile = blockIdx.x; ok && tile < total && !abort_flag; tile += gridDim.x) {
-        const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, w, cend, tile);
+        const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, w, cend, tile, chunk_cols(SPLIT));
         const unsigned char* base = pack + (int64_t)ti.slot * cap * 2 * IMG;
         const int bb = 2 * ti.J, nbb = min(2, ti.nb - bb);   // row blocks of the column block
         const bool a_in_b = ti.I - bb < nbb;                   // row block I is one of them
@@ -424,7 +464,7 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
     uint32_t g = 0, tl = 0;
     for (int tile = blockIdx.x; tile < total && !__shfl_sync(0xffffffffu, abort_flag, 0);
          tile += gridDim.x, tl++) {
-      const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, w, cend, tile);
+      const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, w, cend, tile, chunk_cols(SPLIT));
       const int b = tl % NACC;
       const uint32_t v = tl / NACC;
       if (v >= 1 && !mbar_wait_warp(&acc_empty[b], (v - 1) & 1, &abort_flag, lim)) break;
@@ -446,8 +486,13 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
           const bool in = ia >= 0 && ia < nbb;
           const uint32_t a_hi = in ? b_hi + ia * IMG : st, a_lo = in ? b_lo + ia * IMG : st + IMG;
 #pragma unroll
-          for (int kk = 0; kk < TK / 8; kk++) {
-            const uint32_t ko = kk * 32;   // 8 TF32 values = 32 bytes along the swizzled row
+          for (int kk = 0; kk < 2; kk++) {
+            // K = 8 TF32 or K = 16 BF16 values: 32 bytes along the swizzled row
+            const uint32_t ko = kk * 32;
+            if (SPLIT == 2) {
+              mma_bf16(dacc, sw64_desc(a_hi + ko), sw64_desc(b_hi + ko), (c | kk) != 0);
+              continue;
+            }
             mma_tf32(dacc, sw64_desc(a_hi + ko), sw64_desc(b_hi + ko), (c | kk) != 0);
             if (SPLIT == 3) {
               mma_tf32(dacc, sw64_desc(a_hi + ko), sw64_desc(b_lo + ko), 1u);
@@ -478,7 +523,7 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
     uint32_t tl = 0;
     for (int tile = blockIdx.x; tile < total && !__shfl_sync(0xffffffffu, abort_flag, 0);
          tile += gridDim.x, tl++) {
-      const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, w, cend, tile);
+      const TileInfo ti = tile_info(pre, nf, flist, fr, F, K, w, cend, tile, chunk_cols(SPLIT));
       const int b = tl % NACC;
       const int row = ti.r0 + quarter * 32 + lane, cb = ti.c0 + half * (TN / 2);
       const bool live = row < ti.N;
@@ -555,6 +600,7 @@ int tc_setup() {   // thread-safe one-time set-up (static local initialisation)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
     cudaFuncSetAttribute(k_trail_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+    cudaFuncSetAttribute(k_trail_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
     cudaFuncSetAttribute(k_trail_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
     return n;
   }();
@@ -565,11 +611,13 @@ int tc_setup() {   // thread-safe one-time set-up (static local initialisation)
 cudaError_t launch_tc_pack(const int* flist, int nf, int cap, const FrontDev* fr, const float* F,
                            int K, int w, int split, void* pack, cudaStream_t st) {
   if (nf <= 0 || cap <= 0) return cudaSuccess;
-  if (nf > 65535 || (split != 1 && split != 3) || w <= 0 || w % TK || w > kTcOuter)
+  if (nf > 65535 || split < 1 || split > 3 || w <= 0 || w % chunk_cols(split) || w > kTcOuter)
     return cudaErrorInvalidValue;
   const dim3 grid((unsigned)cap, (unsigned)nf);
   if (split == 3)
     k_tc_pack<3><<<grid, 128, 0, st>>>(flist, fr, F, K, w, cap, (unsigned char*)pack);
+  else if (split == 2)
+    k_tc_pack<2><<<grid, 128, 0, st>>>(flist, fr, F, K, w, cap, (unsigned char*)pack);
   else
     k_tc_pack<1><<<grid, 128, 0, st>>>(flist, fr, F, K, w, cap, (unsigned char*)pack);
   g_launches++;
@@ -580,12 +628,15 @@ cudaError_t launch_trail_tc(const int* flist, int nf, int64_t ntiles, const Fron
                             int K, int w, int cend, int split, int cap, const void* pack,
                             DevError* err, cudaStream_t st) {
   if (nf <= 0 || ntiles <= 0) return cudaSuccess;
-  if (nf > kMaxTcFronts || (split != 1 && split != 3) || !pack || w <= 0 || w % TK ||
-      w > kTcOuter)
+  if (nf > kMaxTcFronts || split < 1 || split > 3 || !pack || w <= 0 ||
+      w % chunk_cols(split) || w > kTcOuter)
     return cudaErrorInvalidValue;
   const int grid = (int)std::min<int64_t>(ntiles, tc_setup());
   if (split == 3)
     k_trail_tc<3><<<grid, TCT, kTcSmem, st>>>(flist, nf, fr, F, K, w, cend, cap,
+                                              (const unsigned char*)pack, err);
+  else if (split == 2)
+    k_trail_tc<2><<<grid, TCT, kTcSmem, st>>>(flist, nf, fr, F, K, w, cend, cap,
                                               (const unsigned char*)pack, err);
   else
     k_trail_tc<1><<<grid, TCT, kTcSmem, st>>>(flist, nf, fr, F, K, w, cend, cap,

@@ -299,8 +299,9 @@ struct mfgpu_handle {
   // mixed precision: scaling and refinement buffers
   bool mixed = false;
   int tcMinN = 4096;               // mixed: smallest level maxN run on the tensor cores (0 = never)
-  int tcSplit = 3;                 // mixed: 3 = three-term TF32 products, 1 = plain TF32
-  int tcSplit3Levels = -1;         // >= 0: three-term products only on the top levels 0 .. this - 1
+  int tcSplit = 3;                 // mixed: 3 = three-term TF32 products, 1 = plain TF32, 2 = BF16
+  int tcSplit3Levels = -1;         // >= 0: tcSplit only on the top levels 0 .. this - 1,
+  int tcSplitLow = 1;              //   tcSplitLow (plain TF32 or BF16) below them
   int tcSub = 128;                 // mixed: sub-panel width inside each 512-column outer panel of a
                                    // tensor-core level (0 or 512: no sub-panels)
   int fusedMinFronts = 148;        // fewest fronts for the one-CTA-per-front kernel
@@ -811,7 +812,7 @@ struct mfgpu_handle {
   // (diagonal blocks, panel solves, in-sub-panel updates) to MFGPU_KC_COOP.
   void runTensorLevel(const Plan& P, const Plan::Level& L, double level_flops, int ell) {
     const Schedule& s = *S;
-    const int split = tcSplit3Levels >= 0 && ell >= tcSplit3Levels ? 1 : tcSplit;
+    const int split = tcSplit3Levels >= 0 && ell >= tcSplit3Levels ? tcSplitLow : tcSplit;
     std::vector<int> nn(L.nf), NN(L.nf);
     for (int64_t i = 0; i < L.nf; i++) {
       nn[i] = s.fronts[P.ids[L.f0 + i]].n;
@@ -1439,7 +1440,12 @@ int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const
   if (const char* e = getenv("MFGPU_TC_MIN_N")) h->tcMinN = atoi(e);
   if (const char* e = getenv("MFGPU_SOLVE_COOP_MIN_N")) h->solveCoopMinN = atoi(e);
   if (const char* e = getenv("MFGPU_FUSED_MIN_FRONTS")) h->fusedMinFronts = atoi(e);
-  if (const char* e = getenv("MFGPU_TC_SPLIT")) h->tcSplit = atoi(e) == 1 ? 1 : 3;
+  auto splitOf = [](const char* e, int dflt) {
+    const std::string v(e);
+    return v == "1" || v == "tf32" ? 1 : v == "bf16" ? 2 : v == "3" ? 3 : dflt;
+  };
+  if (const char* e = getenv("MFGPU_TC_SPLIT")) h->tcSplit = splitOf(e, 3);
+  if (const char* e = getenv("MFGPU_TC_LOW")) h->tcSplitLow = splitOf(e, 1);
   if (const char* e = getenv("MFGPU_TC_SPLIT3_LEVELS")) h->tcSplit3Levels = atoi(e);
   if (const char* e = getenv("MFGPU_TC_SUB")) h->tcSub = atoi(e);
   if (const char* e = getenv("MFGPU_GRAPHS")) h->graphs = e[0] != '0';
@@ -2586,6 +2592,7 @@ std::unique_ptr<mfgpu_handle> makeView(mfgpu_handle& B) {
   H.tcMinN = B.tcMinN;
   H.tcSplit = B.tcSplit;
   H.tcSplit3Levels = B.tcSplit3Levels;
+  H.tcSplitLow = B.tcSplitLow;
   H.tcSub = B.tcSub;
   H.fusedMinFronts = B.fusedMinFronts;
   H.d_scale = B.d_scale;
