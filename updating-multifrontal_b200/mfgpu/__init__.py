@@ -23,6 +23,17 @@ __all__ = ["MF2D", "MF3D", "MFBatch", "Server", "Symbolic", "CSR", "build_laplac
            "MFGPU_MIXED", "MFError", "inject_alloc_failure"]
 
 
+def _as_csr(A):
+    """A as this package's CSR: a CSR (of this or another copy of the stencil
+    module: anything with row_ptr / col_ind / val / n) or a scipy sparse matrix."""
+    if isinstance(A, CSR):
+        return A
+    if all(hasattr(A, k) for k in ("row_ptr", "col_ind", "val", "n")):
+        return CSR(A.row_ptr, A.col_ind, A.val, A.n)
+    A = A.tocsr()
+    return CSR(A.indptr, A.indices, A.data, A.shape[0])
+
+
 def inject_alloc_failure(after):
     """Test hook: the next `after` device allocations succeed, the one after
     fails as out of memory (MFGPU_ERR_OOM); after < 0 disarms."""
@@ -49,8 +60,7 @@ class _MFBase:
     def __init__(self, A, N, width=1, max_side_length=4, precision=MFGPU_FP64, device=0,
                  refine_tol=1e-10, refine_maxit=50):
         lib = _lib.load()
-        if not isinstance(A, CSR):
-            A = CSR(A.indptr, A.indices, A.data, A.shape[0])
+        A = _as_csr(A)
         self.A = A
         self.N = tuple(int(x) for x in N)
         opts = _lib.default_options(precision, device, refine_tol, refine_maxit)
@@ -84,8 +94,7 @@ class _MFBase:
         self._check(self._lib.mfgpu_factor(self._h))
 
     def Update(self, A, modifiedDOFs):
-        if not isinstance(A, CSR):
-            A = CSR(A.indptr, A.indices, A.data, A.shape[0])
+        A = _as_csr(A)
         mod = np.ascontiguousarray(sorted(set(int(d) for d in modifiedDOFs)), np.int32)
         self._check(self._lib.mfgpu_update(self._h, _lib._ptr(A.val), A.nnz, _lib._ptr(mod),
                                            len(mod)))
@@ -248,8 +257,7 @@ class MFBatch(_MFBase):
         lib = _lib.load()
         mats, geo = [], []
         for A, N, width, ms in problems:
-            if not isinstance(A, CSR):
-                A = CSR(A.indptr, A.indices, A.data, A.shape[0])
+            A = _as_csr(A)
             N = tuple(int(x) for x in N)
             mats.append(A)
             geo.append((len(N), N[0], N[1], N[2] if len(N) == 3 else 1, int(width), int(ms)))
@@ -288,8 +296,7 @@ class MFBatch(_MFBase):
     def Update(self, A_list, mods):
         """A_list[p]: new matrix of problem p (same pattern) or None; mods[p]: its
         modified DOFs (local numbering)."""
-        mats = [self.mats[p] if A is None else (A if isinstance(A, CSR) else
-                CSR(A.indptr, A.indices, A.data, A.shape[0])) for p, A in enumerate(A_list)]
+        mats = [self.mats[p] if A is None else _as_csr(A) for p, A in enumerate(A_list)]
         allmod = []
         for p, m in enumerate(mods):
             allmod.extend(int(d) + int(self.offsets[p]) for d in (m if m is not None else ()))
