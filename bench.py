@@ -714,7 +714,7 @@ def main():
                          "candidate) during set-up, before the warm-up; 0 = size rules")
     ap.add_argument("--rate", type=float, default=4.0, help="serving: arrivals per second")
     ap.add_argument("--requests", type=int, default=24, help="serving: requests in the stream")
-    ap.add_argument("--slots", type=int, default=4, help="serving: concurrent requests")
+    ap.add_argument("--slots", type=int, default=8, help="serving: requests per batch")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -952,8 +952,9 @@ def run_serve(args, w):
     fronts = [S.front(f) for f in range(S.n_fronts)]
     solve_unit = sum(2.0 * (f["n"] ** 2 + 2.0 * f["n"] * f["m"]) for f in fronts)
     free_gb = torch.cuda.mem_get_info()[0] / 2 ** 30
-    slot_gb = 2.5 * (1 if prec == MFGPU_MIXED else 2)     # views: values, workspaces, scratch
-    pool_gb = max(4.0, free_gb - 6.0 - args.slots * slot_gb)
+    # per batch member: values, coefficients, block inverses; the view's workspaces
+    slot_gb = 0.25 * (1 if prec == MFGPU_MIXED else 2)
+    pool_gb = max(4.0, free_gb - 8.0 - args.slots * slot_gb)
     srv = Server(F, a, slots=args.slots, pool_gb=pool_gb)
     # one warm-up request outside the measurement
     srv.wait(srv.submit(reqs[0][0], reqs[0][1], reqs[0][2], reqs[0][3][:, :1]))
@@ -1007,12 +1008,15 @@ def run_serve(args, w):
                                f"maxSideLength {w['max_side']}; {len(reqs)} requests, Poisson "
                                f"arrivals at {args.rate}/s, box side {w['side'][0]}-{w['side'][1]}, "
                                f"{w['nrhs'][0]}-{w['nrhs'][1]} RHS)",
-                   "slots": args.slots, "pool_gb": round(pool_gb, 1), "precision": args.precision,
+                   "batch_capacity": args.slots, "pool_gb": round(pool_gb, 1),
+                   "precision": args.precision,
                    "timing": "wall clock, submission to result on the host"},
         "requests_per_s": len(reqs) / makespan,
         "latency_s": {"p50": statistics.median(lat), "p99": pct(lat, 99), "max": max(lat)},
         "queued_s_p50": statistics.median(r[1]["queued_seconds"] for r in results),
         "fronts_per_request_p50": statistics.median(r[1]["fronts"] for r in results),
+        "batch_size": {"p50": statistics.median(r[1]["batch"] for r in results),
+                       "max": max(r[1]["batch"] for r in results)},
         "resid": resid, "clocks": clk,
         "e2e": {"value": work / makespan / 1e12, "unit": "TFLOP/s",
                 "h2d_bytes_per_step": int(np.mean([b.nbytes for *_, b in reqs])),

@@ -112,20 +112,25 @@ int mfgpu_stencil_update_device(mfgpu_handle* h, const double* d_coef, const dou
  * A factored handle stays resident; each request multiplies the coefficients
  * of one box of cells [box_lo, box_hi) by `factor` and solves the changed
  * system for its right-hand sides.  Requests are independent of each other
- * (each answer is that of the base matrix under its own change), refactor only
- * the root paths of the leaves their box touches (the reference's Update,
- * src/DE/mf2d.cpp:150-181) into private copies held in a device pool of
- * pool_bytes, and run concurrently in `slots` slots, each a worker thread with
- * its own stream.  A request is admitted when a slot is free and the pool has
- * room for its private fronts; until then it waits, in arrival order.
+ * (each answer is that of the base matrix under its own change) and refactor
+ * only the root paths of the leaves their box touches (the reference's
+ * Update, src/DE/mf2d.cpp:150-181) into private copies held in a device pool
+ * of pool_bytes.  Continuous batching: one dispatcher takes queued requests in
+ * arrival order into a batch of at most `slots` requests whose private copies
+ * fit in the pool together, refactors all their root paths with one set of
+ * level launches (their overlapping paths - every path reaches the root - are
+ * factored side by side in the same launches), solves each, and meanwhile
+ * arriving requests wait for the next batch.  An answer is bit-identical
+ * whether its request ran alone or in a batch.  A request whose private
+ * copies exceed the whole pool fails with MFGPU_ERR_OOM.
  * d_coef: the base coefficients on the device ((nx+2) x (ny+2) [x (nz+2)],
  * C order, x slowest), copied by the server; hxyz: grid spacings (null = 1). */
 typedef struct mfgpu_request_info {
   int status;               /* mfgpu_status of the request                       */
   int fronts;               /* fronts refactored for it                          */
   int iterations;           /* refinement iterations (mixed)                     */
-  int pad;
-  double queued_seconds;    /* submit -> start of its device work                */
+  int batch;                /* requests served in its batch (itself included)    */
+  double queued_seconds;    /* submit -> start of its batch                      */
   double latency_seconds;   /* submit -> result written                          */
   double residual;          /* relative residual reached (mixed)                 */
   int64_t pool_bytes;       /* private memory it held                            */

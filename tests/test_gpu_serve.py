@@ -2,8 +2,9 @@
 
 Every request's answer must equal (to 1e-12 in FP64, 1e-10 residual in mixed)
 the solve of a fresh factorization of the base matrix under that request's
-change alone, be bit-identical whether the request runs alone or among others
-in flight, and leave the base factorization untouched.
+change alone, be bit-identical whether the request runs alone or batched with
+others in flight (their root paths factored by the same launches), and leave
+the base factorization untouched.
 """
 import numpy as np
 import pytest
@@ -52,6 +53,9 @@ def test_serving_alone_equals_mixed_and_fresh_factorization(N, precision):
         alone.append(S.wait(S.submit(lo, hi, f, b))[0])
     tickets = [S.submit(lo, hi, f, b) for lo, hi, f, b in reqs]   # all in flight
     mixed = [S.wait(t) for t in tickets]
+    # requests in flight together were served in shared batches (one set of
+    # level launches for all their root paths)
+    assert max(info["batch"] for _, info in mixed) >= 2
     for (lo, hi, f, b), xa, (xm, info) in zip(reqs, alone, mixed):
         assert info["status"] == 0 and info["fronts"] > 0
         assert np.array_equal(xa, xm)       # the same alone and in the mix

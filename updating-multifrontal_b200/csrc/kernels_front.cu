@@ -81,6 +81,9 @@ __global__ void __launch_bounds__(32 * kTaskWarps) k_tasks(const Task* __restric
     return;
   }
   if (Tk.kind == TK_SPARSE) {
+    // values of this task's matrix: src_off is the element offset of its CSR
+    // values (0 but for the serving loop's batches of several matrices)
+    va += Tk.src_off;
     // A(r, c) for the tile (Sparse::operator(), src/LinAlg/sparse.cpp:80-92):
     // lane j holds column DOF c_j; every row's CSR entries are read once (all
     // lanes load the same addresses) and matched against the lanes' columns

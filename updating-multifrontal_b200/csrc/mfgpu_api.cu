@@ -14,6 +14,7 @@
 #include <map>
 #include <tuple>
 #include <deque>
+#include <functional>
 #include <condition_variable>
 #include <thread>
 #include <new>
@@ -89,9 +90,17 @@ struct Plan {
     int64_t cpref0 = 0;   // offset of the cooperative kernel's phase prefixes in cpref
     int coopItems = 0;    // largest work-item count of any cooperative phase
     int coopOuter = 0;    // outer panel width the phase prefixes were built with (0: default)
+    // A batch plan (several problems' fronts in one plan, the serving loop's)
+    // factors a level's fronts in consecutive partitions, each with the kernel
+    // its problems would get alone: `subs` holds them (f0, nf, maxN, maxn,
+    // cpref0, coopItems, coopOuter of a partition, its kernel in `kind`).
+    // Empty: one partition, the level itself, kernel by the size rules.
+    struct Sub;
+    std::vector<Sub> subs;
   };
   size_t tcPackBytes = 0;   // largest tensor-core panel pack any level of the plan needs
   std::vector<Level> lv;
+  std::vector<int> real;    // batch plans: the schedule's front id of each entry of `ids`
   std::vector<Task> tasks;
   std::vector<int64_t> pref;
   std::vector<int> ids;
@@ -117,13 +126,19 @@ struct Plan {
     cap_tasks = cap_pref = cap_ids = cap_cpref = 0;
   }
 
-  Group addGroup(const std::vector<Task>& src, const std::vector<int64_t>& ptr,
-                 const std::vector<int>& owners, int pick /* -1 all, 0/1 add task k */) {
+  // A group is built by beginGroup, appendGroup (the tasks of some owners,
+  // optionally rewritten by fx), endGroup.
+  Group beginGroup() {
     Group g;
     g.task0 = (int64_t)tasks.size();
     g.pref0 = (int64_t)pref.size();
-    int64_t acc = 0;
     pref.push_back(0);
+    return g;
+  }
+  void appendGroup(Group& g, const std::vector<Task>& src, const std::vector<int64_t>& ptr,
+                   const std::vector<int>& owners, int pick /* -1 all, 0/1 add task k */,
+                   const std::function<void(Task&)>& fx = nullptr) {
+    int64_t acc = pref.back();
     for (int o : owners) {
       int64_t a, b;
       if (pick < 0) {
@@ -135,13 +150,23 @@ struct Plan {
       }
       for (int64_t t = a; t < b; t++) {
         tasks.push_back(src[t]);
+        if (fx) fx(tasks.back());
         acc += tilesOf(src[t]);
         pref.push_back(acc);
       }
     }
+    (void)g;
+  }
+  void endGroup(Group& g) {
     g.ntasks = (int64_t)tasks.size() - g.task0;
-    g.ntiles = acc;
+    g.ntiles = pref.back();
     if (g.ntasks == 0) pref.pop_back();
+  }
+  Group addGroup(const std::vector<Task>& src, const std::vector<int64_t>& ptr,
+                 const std::vector<int>& owners, int pick) {
+    Group g = beginGroup();
+    appendGroup(g, src, ptr, owners, pick);
+    endGroup(g);
     return g;
   }
 
@@ -175,6 +200,14 @@ struct Plan {
     // host vectors must outlive the async copies
     ck(cudaStreamSynchronize(st), "plan upload");
   }
+};
+
+struct Plan::Level::Sub {
+  int64_t f0 = 0, nf = 0;
+  int maxN = 0, maxn = 0;
+  int64_t cpref0 = 0;
+  int coopItems = 0, coopOuter = 0;
+  int kind = -1;
 };
 
 // Optional per-kernel-class device timing: an event pair around each launch
@@ -288,6 +321,7 @@ struct mfgpu_handle {
   int maxFlags = 0;
   void* d_Dinv = nullptr;      // inverses of the cooperative-sweep levels' 64 x 64 pivot blocks
   int64_t* d_dinv_off = nullptr;   // per front: element offset in d_Dinv, -1 outside those levels
+  std::vector<int64_t> h_dinv_off; // host copy
   int64_t dinvElems = 0;
   // solve workspaces (d_Wd / d_Td hold elements of the factor's precision)
   double* d_Wd = nullptr;
@@ -397,6 +431,10 @@ struct mfgpu_handle {
     if (own) cudaStreamDestroy(own);
   }
 
+  // The schedule's front id of entry i of a plan's id list (batch plans list
+  // per-problem front copies under their own ids).
+  static int realId(const Plan& P, int64_t i) { return P.real.empty() ? P.ids[i] : P.real[i]; }
+
   // Build a plan for the given dirty fronts (global ids); separators adjacent
   // to a dirty front at their level are recomputed.
   void buildPlan(Plan& P, const std::vector<char>& dirtyFront) {
@@ -405,6 +443,7 @@ struct mfgpu_handle {
     P.tasks.clear();
     P.pref.clear();
     P.ids.clear();
+    P.real.clear();
     P.cpref.clear();
     P.nfronts = 0;
     P.flops = 0;
@@ -466,6 +505,127 @@ struct mfgpu_handle {
                     mfgpu::tc_pack_bytes((int)fl.size(), mfgpu::tc_pack_cap(nn, NN, K, ww)));
         }
       }
+    }
+  }
+
+  // One problem of a batch plan: its dirty fronts, the id base of its front
+  // copies (front f is vbase + f in the plan), the rewrite of its tasks into
+  // its private copies, and the element offset of its CSR values.
+  struct BatchMember {
+    const std::vector<char>* dirty;
+    int vbase;
+    std::function<void(Task&)> move;
+    int64_t valoff;
+  };
+
+  // A plan over several problems that share this schedule and differ in their
+  // values (the serving loop's requests): every level's assembly, kernel and
+  // separator launches cover all of them; each level's fronts are grouped by
+  // the kernel the size rules give each problem alone, so every front is
+  // factored exactly as in a plan of its problem alone.
+  void buildPlanBatch(Plan& P, const std::vector<BatchMember>& M) {
+    const Schedule& s = *S;
+    P.lv.assign(s.levels, Plan::Level());
+    P.tasks.clear();
+    P.pref.clear();
+    P.ids.clear();
+    P.real.clear();
+    P.cpref.clear();
+    P.nfronts = 0;
+    P.flops = 0;
+    P.tcPackBytes = 0;
+    const int W = mfgpu::tc_outer();
+    for (int ell = s.levels - 1; ell >= 0; ell--) {
+      Plan::Level& L = P.lv[ell];
+      const size_t nm = M.size();
+      std::vector<std::vector<int>> fl(nm), sl(nm);
+      std::vector<int> kind(nm, LK_NONE), kinds;
+      for (size_t m = 0; m < nm; m++) {
+        const std::vector<char>& dirty = *M[m].dirty;
+        Plan::Level one;
+        for (int b = 0; b < s.lv[ell].nbox; b++) {
+          const int f = s.lv[ell].front0 + b;
+          if (!dirty[f]) continue;
+          fl[m].push_back(f);
+          one.maxN = std::max(one.maxN, s.fronts[f].N);
+          one.maxn = std::max(one.maxn, s.fronts[f].n);
+        }
+        for (int e = 0; e < s.lv[ell].nsep; e++) {
+          const int k = s.lv[ell].sep0 + e;
+          if (dirty[s.seps[k].box[0]] || dirty[s.seps[k].box[1]]) sl[m].push_back(k);
+        }
+        one.nf = (int64_t)fl[m].size();
+        kind[m] = ruleKernel(one);
+        if (kind[m] != LK_NONE && std::find(kinds.begin(), kinds.end(), kind[m]) == kinds.end())
+          kinds.push_back(kind[m]);
+      }
+      L.f0 = (int64_t)P.ids.size();
+      for (int kd : kinds) {
+        Plan::Level::Sub u;
+        u.kind = kd;
+        u.f0 = (int64_t)P.ids.size();
+        std::vector<int> nn, NN;
+        for (size_t m = 0; m < nm; m++) {
+          if (kind[m] != kd) continue;
+          for (int f : fl[m]) {
+            P.ids.push_back(M[m].vbase + f);
+            P.real.push_back(f);
+            u.maxN = std::max(u.maxN, s.fronts[f].N);
+            u.maxn = std::max(u.maxn, s.fronts[f].n);
+            nn.push_back(s.fronts[f].n);
+            NN.push_back(s.fronts[f].N);
+            P.flops += s.front_flops(s.fronts[f]);
+          }
+        }
+        u.nf = (int64_t)P.ids.size() - u.f0;
+        if (kd == LK_COOP || kd == LK_TC) {
+          u.coopOuter = kd == LK_TC && tcSub > 0 && tcSub < W ? tcSub : 0;
+          u.cpref0 = (int64_t)P.cpref.size();
+          std::vector<int> pp = mfgpu::coop_phase_prefix(nn, NN, u.maxn, u.coopOuter);
+          P.cpref.insert(P.cpref.end(), pp.begin(), pp.end());
+          const size_t stride = nn.size() + 1;
+          for (size_t q = 0; q + stride <= pp.size(); q += stride)
+            u.coopItems = std::max(u.coopItems, pp[q + nn.size()]);
+          if (kd == LK_TC) {
+            const int w = u.coopOuter > 0 ? u.coopOuter : W;
+            for (int K = 0; K < u.maxn; K += w)
+              for (int ww : {w, W})
+                if (K % ww == 0)
+                  P.tcPackBytes = std::max(
+                      P.tcPackBytes,
+                      mfgpu::tc_pack_bytes((int)nn.size(), mfgpu::tc_pack_cap(nn, NN, K, ww)));
+          }
+        }
+        L.maxN = std::max(L.maxN, u.maxN);
+        L.maxn = std::max(L.maxn, u.maxn);
+        L.subs.push_back(u);
+      }
+      L.nf = (int64_t)P.ids.size() - L.f0;
+      P.nfronts += (int)L.nf;
+      L.s0 = (int64_t)P.ids.size();
+      for (size_t m = 0; m < nm; m++)
+        for (int k : sl[m]) {
+          P.ids.push_back(k);
+          P.real.push_back(k);
+        }
+      L.ns = (int64_t)P.ids.size() - L.s0;
+      auto group = [&](const std::vector<Task>& src, const std::vector<int64_t>& ptr,
+                       const std::vector<std::vector<int>>& own, int pick) {
+        Group g = P.beginGroup();
+        for (size_t m = 0; m < nm; m++) {
+          const BatchMember& bm = M[m];
+          P.appendGroup(g, src, ptr, own[m], pick, [&bm](Task& t) {
+            bm.move(t);
+            if (t.kind == mfgpu::TK_SPARSE) t.src_off = bm.valoff;
+          });
+        }
+        P.endGroup(g);
+        return g;
+      };
+      L.ftask = group(s.front_tasks, s.front_task_ptr, fl, -1);
+      L.sbase = group(s.sep_tasks, s.sep_task_ptr, sl, -1);
+      L.sadd0 = group(s.sep_add_tasks, s.sep_task_ptr, sl, 0);
+      L.sadd1 = group(s.sep_add_tasks, s.sep_task_ptr, sl, 1);
     }
   }
 
@@ -532,8 +692,8 @@ struct mfgpu_handle {
   size_t levelPackBytes(const Plan& P, const Plan::Level& L) const {
     std::vector<int> nn, NN;
     for (int64_t i = L.f0; i < L.f0 + L.nf; i++) {
-      nn.push_back(S->fronts[P.ids[i]].n);
-      NN.push_back(S->fronts[P.ids[i]].N);
+      nn.push_back(S->fronts[realId(P, i)].n);
+      NN.push_back(S->fronts[realId(P, i)].N);
     }
     size_t b = 0;
     const int W = mfgpu::tc_outer(), w = L.coopOuter > 0 ? L.coopOuter : W;
@@ -617,7 +777,7 @@ struct mfgpu_handle {
     T* F = (T*)d_F;
     double fl = 0;
     if (prof.on && kind != LK_STEPPED)
-      for (int64_t i = L.f0; i < L.f0 + L.nf; i++) fl += s.front_flops(s.fronts[P.ids[i]]);
+      for (int64_t i = L.f0; i < L.f0 + L.nf; i++) fl += s.front_flops(s.fronts[realId(P, i)]);
     if (kind == LK_FUSED) {
       prof.flops[MFGPU_KC_FRONT] += fl;
       prof.begin(MFGPU_KC_FRONT, stream);
@@ -656,7 +816,7 @@ struct mfgpu_handle {
     for (int k = 0; k < L.maxn; k += mfgpu::kPanel) {
       if (prof.on) {
         for (int64_t i = L.f0; i < L.f0 + L.nf; i++) {
-          const mfgpu::Front& f = s.fronts[P.ids[i]];
+          const mfgpu::Front& f = s.fronts[realId(P, i)];
           if (k >= f.n) continue;
           const double kb = std::min(mfgpu::kPanel, f.n - k), M = f.N - k - kb;
           prof.flops[MFGPU_KC_POTRF] += kb * kb * kb / 3.0 + M * kb * kb;
@@ -706,7 +866,21 @@ struct mfgpu_handle {
       prof.level = ell;
       runGroup<T>(P, L.sbase, groupBytes(P, L.sbase));
       runGroup<T>(P, L.ftask, groupBytes(P, L.ftask));
-      runLevelKernel<T>(P, L, ell, levelKernel(P, L, ell));
+      if (L.subs.empty()) {
+        runLevelKernel<T>(P, L, ell, levelKernel(P, L, ell));
+      } else {
+        for (const Plan::Level::Sub& u : L.subs) {
+          Plan::Level Ls = L;
+          Ls.f0 = u.f0;
+          Ls.nf = u.nf;
+          Ls.maxN = u.maxN;
+          Ls.maxn = u.maxn;
+          Ls.cpref0 = u.cpref0;
+          Ls.coopItems = u.coopItems;
+          Ls.coopOuter = u.coopOuter;
+          runLevelKernel<T>(P, Ls, ell, u.kind);
+        }
+      }
       finishLevel<T>(P, L, ell);
     }
     ck(cudaGetLastError(), "factor launch");
@@ -815,8 +989,8 @@ struct mfgpu_handle {
     const int split = tcSplit3Levels >= 0 && ell >= tcSplit3Levels ? tcSplitLow : tcSplit;
     std::vector<int> nn(L.nf), NN(L.nf);
     for (int64_t i = 0; i < L.nf; i++) {
-      nn[i] = s.fronts[P.ids[L.f0 + i]].n;
-      NN[i] = s.fronts[P.ids[L.f0 + i]].N;
+      nn[i] = s.fronts[realId(P, L.f0 + i)].n;
+      NN[i] = s.fronts[realId(P, L.f0 + i)].N;
     }
     const int W = mfgpu::tc_outer(), w = L.coopOuter > 0 ? L.coopOuter : W;
     int phase0 = 0;
@@ -873,7 +1047,7 @@ struct mfgpu_handle {
     for (int k = 0; k < L.maxn; k += mfgpu::kPanel) {
       if (prof.on) {
         for (int64_t i = L.f0; i < L.f0 + L.nf; i++) {
-          const mfgpu::Front& f = s.fronts[P.ids[i]];
+          const mfgpu::Front& f = s.fronts[realId(P, i)];
           if (k >= f.n) continue;
           double kb = std::min(mfgpu::kPanel, f.n - k), M = f.N - k - kb;
           prof.flops[MFGPU_KC_POTRF] += kb * kb * kb / 3.0;
@@ -939,7 +1113,7 @@ struct mfgpu_handle {
                       MFGPU_ERR_TIMEOUT);
     }
     if (e.code == 4) {
-      const mfgpu::Front& f = S->fronts[e.front];
+      const mfgpu::Front& f = S->fronts[e.front % (int)S->fronts.size()];
       char buf[256];
       snprintf(buf, sizeof buf,
                "zero pivot column in front %d (level %d, box %d) at pivot column %d: the front's "
@@ -948,7 +1122,7 @@ struct mfgpu_handle {
       throw CudaError(buf, MFGPU_ERR_PIVOT);
     }
     if (e.code == 1) {
-      const mfgpu::Front& f = S->fronts[e.front];
+      const mfgpu::Front& f = S->fronts[e.front % (int)S->fronts.size()];
       char buf[256];
       snprintf(buf, sizeof buf,
                "non-positive pivot in front %d (level %d, box %d) at pivot column %d: the matrix "
@@ -1510,6 +1684,7 @@ int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const
           cur += (int64_t)((s.fronts[i].n + B - 1) / B) * 2 * B * B;
         }
       H.dinvElems = cur;
+      H.h_dinv_off = doff;
       H.d_Dinv = dalloc<unsigned char>(std::max<int64_t>(cur, 1) * H.esz, "alloc block inverses");
       // task lists of the cooperative sweeps, per level
       std::vector<int> tab;
@@ -2321,44 +2496,28 @@ struct Request {
   mfgpu_stats stats{};
   int64_t footprint = 0;     // pool elements
   int nfronts = 0;
+  int batch = 1;             // requests served together with it (itself included)
   bool done = false;
 };
 
-// First-fit allocator over the pool (offsets and sizes in elements).
-struct PoolAlloc {
-  std::map<int64_t, int64_t> free_;   // offset -> size
-  explicit PoolAlloc(int64_t size) { free_[0] = size; }
-  int64_t take(int64_t size) {
-    for (auto it = free_.begin(); it != free_.end(); ++it)
-      if (it->second >= size) {
-        const int64_t off = it->first, rest = it->second - size;
-        free_.erase(it);
-        if (rest > 0) free_[off + size] = rest;
-        return off;
-      }
-    return -1;
-  }
-  void give(int64_t off, int64_t size) {
-    auto it = free_.emplace(off, size).first;
-    auto nx = std::next(it);
-    if (nx != free_.end() && it->first + it->second == nx->first) {
-      it->second += nx->second;
-      free_.erase(nx);
-    }
-    if (it != free_.begin()) {
-      auto pv = std::prev(it);
-      if (pv->first + pv->second == it->first) {
-        pv->second += it->second;
-        free_.erase(it);
-      }
-    }
-  }
-};
 
 inline int64_t round32(int64_t v) { return (v + 31) / 32 * 32; }
 
 }  // namespace
 
+// The serving loop.  One dispatcher thread takes the queued requests in
+// arrival order into a batch, as many as the batch capacity and the private
+// pool allow, and serves the batch with one factorization plan: every
+// request's dirty root path gets private copies of its fronts and separators
+// in the pool, and each tree level's assembly, partial factorization and
+// separator accumulation run as the same launches for all requests of the
+// batch (front copy f of batch member r is front (r + 1) * nF + f of a front
+// table of (capacity + 1) * nF entries).  A level's fronts are grouped by the
+// kernel each request would get alone, and no kernel's arithmetic for a front
+// depends on the other fronts of its launch, so an answer is bit-identical
+// alone or in any batch.  Then each request is solved with its own front
+// table, values and block inverses.  Requests arriving meanwhile queue for
+// the next batch.
 struct mfgpu_server {
   mfgpu_handle* base = nullptr;
   double h[3] = {1.0, 1.0, 1.0};
@@ -2366,14 +2525,20 @@ struct mfgpu_server {
   int64_t coef_elems = 0;
   unsigned char* d_pool = nullptr;     // private fronts and separators
   int64_t pool_elems = 0;
-  std::vector<std::unique_ptr<mfgpu_handle>> views;
-  std::vector<double*> slot_coef;
-  std::vector<std::thread> workers;
+  int capacity = 1;                    // requests per batch
+  std::unique_ptr<mfgpu_handle> view;  // the dispatcher's handle (a view of the base)
+  // batch buffers: per member coefficients, CSR values, block inverses; the
+  // batch front table and block-inverse offsets
+  double* d_coefB = nullptr;
+  double* d_valB = nullptr;
+  unsigned char* d_DinvB = nullptr;
+  FrontDev* d_frB = nullptr;
+  int64_t* d_dinv_offB = nullptr;
+  std::thread worker;
   std::mutex mu;
-  std::condition_variable cv_queue, cv_pool, cv_done;
+  std::condition_variable cv_queue, cv_done;
   std::deque<std::shared_ptr<Request>> queue;
   std::map<int64_t, std::shared_ptr<Request>> all;
-  std::unique_ptr<PoolAlloc> pool;
   int64_t next_id = 1;
   bool stop = false;
   std::vector<FrontDev> base_table;
@@ -2385,11 +2550,13 @@ struct mfgpu_server {
       stop = true;
     }
     cv_queue.notify_all();
-    cv_pool.notify_all();
-    for (auto& t : workers)
-      if (t.joinable()) t.join();
-    views.clear();
-    for (double* c : slot_coef) cudaFree(c);
+    if (worker.joinable()) worker.join();
+    view.reset();
+    cudaFree(d_coefB);
+    cudaFree(d_valB);
+    cudaFree(d_DinvB);
+    cudaFree(d_frB);
+    cudaFree(d_dinv_offB);
     cudaFree(d_coef);
     cudaFree(d_pool);
   }
@@ -2422,150 +2589,223 @@ struct mfgpu_server {
       }
   }
 
-  void run(int slot) {
-    mfgpu_handle& V = *views[slot];
-    cudaSetDevice(V.device);
+  struct Member {
+    std::shared_ptr<Request> r;
+    std::vector<char> dirty, dsep;
+    int64_t elems = 0, region = 0;
+  };
+
+  void run() {
+    cudaSetDevice(base->device);
     while (true) {
-      std::shared_ptr<Request> r;
+      std::vector<Member> batch;
       {
         std::unique_lock<std::mutex> lk(mu);
         cv_queue.wait(lk, [&] { return stop || !queue.empty(); });
         if (stop) return;
-        r = queue.front();
-        queue.pop_front();
-      }
-      std::vector<char> dirty, dsep;
-      int64_t elems = 0;
-      dirtyOf(*r, dirty, dsep, elems);
-      int64_t region = -1;
-      {
-        std::unique_lock<std::mutex> lk(mu);
-        if (elems > pool_elems) {
-          r->status = MFGPU_ERR_OOM;
-          r->error = "request needs more private memory than the whole pool";
-        } else {
-          cv_pool.wait(lk, [&] { return stop || (region = pool->take(elems)) >= 0; });
-          if (stop) return;
+        // admission in arrival order: while the batch has room and the pool
+        // holds every admitted request's private copies
+        int64_t used = 0;
+        while (!queue.empty() && (int)batch.size() < capacity) {
+          Member m;
+          m.r = queue.front();
+          dirtyOf(*m.r, m.dirty, m.dsep, m.elems);
+          if (m.elems > pool_elems) {           // can never fit: refuse it alone
+            if (!batch.empty()) break;
+            queue.pop_front();
+            m.r->status = MFGPU_ERR_OOM;
+            m.r->error = "request needs more private memory than the whole pool";
+            m.r->t_start = m.r->t_done = Clock::now();
+            m.r->done = true;
+            cv_done.notify_all();
+            continue;
+          }
+          if (used + m.elems > pool_elems) break;
+          queue.pop_front();
+          m.region = used;
+          m.r->footprint = m.elems;
+          used += m.elems;
+          batch.push_back(std::move(m));
         }
       }
-      if (region >= 0) {
-        r->t_start = Clock::now();
-        r->footprint = elems;
-        serve(V, slot, *r, dirty, dsep, region);
-        std::lock_guard<std::mutex> lk(mu);
-        pool->give(region, elems);
+      if (batch.empty()) continue;
+      const Clock::time_point t0 = Clock::now();
+      for (Member& m : batch) {
+        m.r->t_start = t0;
+        m.r->batch = (int)batch.size();
       }
+      serve(batch);
       {
         std::lock_guard<std::mutex> lk(mu);
-        r->t_done = Clock::now();
-        r->done = true;
+        const Clock::time_point t1 = Clock::now();
+        for (Member& m : batch) {
+          if (!m.r->done) m.r->t_done = t1;
+          m.r->done = true;
+        }
       }
-      cv_pool.notify_all();
       cv_done.notify_all();
     }
   }
 
-  void serve(mfgpu_handle& V, int slot, Request& r, const std::vector<char>& dirty,
-             const std::vector<char>& dsep, int64_t region) {
+  void serve(std::vector<Member>& batch) {
+    mfgpu_handle& V = *view;
     const Schedule& s = *V.S;
+    const int nF = (int)s.fronts.size();
+    const int64_t nnz = V.nnz;
+    FrontDev* own_fr = V.d_fr;
+    double* own_val = V.d_val;
+    void* own_Dinv = V.d_Dinv;
+    int64_t* own_doff = V.d_dinv_off;
+    auto restore = [&]() {
+      V.d_fr = own_fr;
+      V.d_val = own_val;
+      V.d_Dinv = own_Dinv;
+      V.d_dinv_off = own_doff;
+    };
     const int st = guarded(&V, [&]() {
-      // the request's coefficients and matrix values
-      ck(cudaMemcpyAsync(slot_coef[slot], d_coef, coef_elems * sizeof(double),
-                         cudaMemcpyDeviceToDevice, V.stream), "copy coefficients");
-      ck(mfgpu::launch_scale_box(s.dim, s.N[1], s.N[2], r.lo, r.hi, r.factor, slot_coef[slot],
-                                 V.stream), "launch coefficient change (k_scale_box)");
-      ck(cudaMemcpyAsync(V.d_val, base->d_val, V.nnz * sizeof(double), cudaMemcpyDeviceToDevice,
-                         V.stream), "copy values");
-      int nmod = 0;
-      const int rc = mfgpu_stencil_update_device(&V, slot_coef[slot], h, r.lo, r.hi, V.d_val,
-                                                 nullptr, 0, &nmod);
-      if (rc != MFGPU_OK) throw CudaError(V.err, rc);
-      // private layout: dirty fronts then dirty separators, from `region` on
-      const int64_t poolF = ((int64_t)(d_pool - (unsigned char*)V.d_F)) / (int64_t)V.esz + region;
-      const int64_t poolS = ((int64_t)(d_pool - (unsigned char*)V.d_Sep)) / (int64_t)V.esz + region;
-      std::vector<int64_t> fnew(s.fronts.size(), -1), snew(s.seps.size(), -1);
-      int64_t cur = 0;
-      for (size_t f = 0; f < s.fronts.size(); f++)
-        if (dirty[f]) {
-          fnew[f] = cur;
-          cur += round32((int64_t)s.fronts[f].ld * s.fronts[f].N);
+      std::vector<FrontDev> table((size_t)(batch.size() + 1) * nF);
+      std::copy(base_table.begin(), base_table.end(), table.begin());
+      std::vector<int64_t> doffB((size_t)(batch.size() + 1) * nF, -1);
+      std::vector<BatchM> keep;
+      std::vector<mfgpu_handle::BatchMember> members;
+      keep.reserve(batch.size());
+      for (size_t r = 0; r < batch.size(); r++) {
+        Member& m = batch[r];
+        Request& q = *m.r;
+        double* coef = d_coefB + (int64_t)r * coef_elems;
+        double* val = d_valB + (int64_t)r * nnz;
+        // the request's coefficients and matrix values
+        ck(cudaMemcpyAsync(coef, d_coef, coef_elems * sizeof(double), cudaMemcpyDeviceToDevice,
+                           V.stream), "copy coefficients");
+        ck(mfgpu::launch_scale_box(s.dim, s.N[1], s.N[2], q.lo, q.hi, q.factor, coef, V.stream),
+           "launch coefficient change (k_scale_box)");
+        ck(cudaMemcpyAsync(val, base->d_val, nnz * sizeof(double), cudaMemcpyDeviceToDevice,
+                           V.stream), "copy values");
+        int nmod = 0;
+        const int rc = mfgpu_stencil_update_device(&V, coef, h, q.lo, q.hi, val, nullptr, 0, &nmod);
+        if (rc != MFGPU_OK) throw CudaError(V.err, rc);
+        // block inverses: the base's (the dirty fronts' are recomputed)
+        if (V.dinvElems > 0)
+          ck(cudaMemcpyAsync(d_DinvB + (int64_t)r * V.dinvElems * V.esz, base->d_Dinv,
+                             V.dinvElems * V.esz, cudaMemcpyDeviceToDevice, V.stream),
+             "copy block inverses");
+        // private layout: dirty fronts then dirty separators, from the region on
+        keep.emplace_back();
+        BatchM& b = keep.back();
+        b.poolF = ((int64_t)(d_pool - (unsigned char*)V.d_F)) / (int64_t)V.esz + m.region;
+        b.poolS = ((int64_t)(d_pool - (unsigned char*)V.d_Sep)) / (int64_t)V.esz + m.region;
+        b.fnew.assign(nF, -1);
+        b.snew.assign(s.seps.size(), -1);
+        int64_t cur = 0;
+        for (int f = 0; f < nF; f++)
+          if (m.dirty[f]) {
+            b.fnew[f] = cur;
+            cur += round32((int64_t)s.fronts[f].ld * s.fronts[f].N);
+          }
+        for (size_t k = 0; k < s.seps.size(); k++)
+          if (m.dsep[k]) {
+            b.snew[k] = cur;
+            cur += round32((int64_t)s.seps[k].ld * s.seps[k].s);
+          }
+        FrontDev* tb = table.data() + (size_t)(r + 1) * nF;
+        std::copy(base_table.begin(), base_table.end(), tb);
+        int nd = 0;
+        for (int f = 0; f < nF; f++) {
+          if (m.dirty[f]) {
+            tb[f].off = b.poolF + b.fnew[f];
+            nd++;
+          }
+          if (V.h_dinv_off[f] >= 0)
+            doffB[(size_t)(r + 1) * nF + f] = (int64_t)r * V.dinvElems + V.h_dinv_off[f];
         }
-      for (size_t k = 0; k < s.seps.size(); k++)
-        if (dsep[k]) {
-          snew[k] = cur;
-          cur += round32((int64_t)s.seps[k].ld * s.seps[k].s);
-        }
-      // the view's front table: dirty fronts in the private region
-      std::vector<FrontDev> table = base_table;
-      int nd = 0;
-      for (size_t f = 0; f < s.fronts.size(); f++)
-        if (dirty[f]) {
-          table[f].off = poolF + fnew[f];
-          nd++;
-        }
-      ck(cudaMemcpyAsync(V.d_fr, table.data(), table.size() * sizeof(FrontDev),
-                         cudaMemcpyHostToDevice, V.stream), "upload front table");
-      // the update plan with task offsets moved to the private copies
-      V.buildPlan(V.upd, dirty);
-      auto ownerF = [&](int64_t off) {   // front whose storage holds element off
-        int lo = 0, hi = (int)s.fronts.size() - 1;
+        q.nfronts = nd;
+      }
+      for (size_t r = 0; r < batch.size(); r++) {
+        const BatchM* b = &keep[r];
+        const Member* m = &batch[r];
+        members.push_back(mfgpu_handle::BatchMember{
+            &m->dirty, (int)(r + 1) * nF,
+            [this, b, m, &s](Task& t) {
+              t.dst_off = b->move(s, m->dirty, m->dsep, t.dst_arena, t.dst_off);
+              if (t.kind == mfgpu::TK_COPY || t.kind == mfgpu::TK_ADD)
+                t.src_off = b->move(s, m->dirty, m->dsep, t.src_arena, t.src_off);
+            },
+            (int64_t)r * nnz});
+      }
+      ck(cudaMemcpyAsync(d_frB, table.data(), table.size() * sizeof(FrontDev),
+                         cudaMemcpyHostToDevice, V.stream), "upload batch front table");
+      ck(cudaMemcpyAsync(d_dinv_offB, doffB.data(), doffB.size() * sizeof(int64_t),
+                         cudaMemcpyHostToDevice, V.stream), "upload batch block-inverse offsets");
+      V.buildPlanBatch(V.upd, members);
+      V.upd.upload(V.stream);   // synchronises: the host tables above are consumed
+      // one factorization of every member's private root path
+      V.d_fr = d_frB;
+      V.d_val = d_valB;
+      V.d_Dinv = d_DinvB;
+      V.d_dinv_off = d_dinv_offB;
+      V.factorWith(nullptr, true, V.upd, false);
+      V.checkDevError();
+      restore();
+    });
+    restore();
+    if (st != MFGPU_OK) {
+      for (Member& m : batch) {
+        m.r->status = st;
+        m.r->error = V.err;
+      }
+      return;
+    }
+    // each member solved with its own factorization
+    V.factored = true;
+    for (size_t r = 0; r < batch.size(); r++) {
+      Request& q = *batch[r].r;
+      V.d_fr = d_frB + (size_t)(r + 1) * nF;
+      V.d_val = d_valB + (int64_t)r * nnz;
+      V.d_Dinv = d_DinvB + (int64_t)r * V.dinvElems * V.esz;
+      std::vector<double> xs((size_t)V.n * q.nrhs);
+      const int rc = solveOrApply(&V, q.b.data(), xs.data(), q.nrhs, V.n, false, false);
+      restore();
+      q.status = rc;
+      if (rc != MFGPU_OK) {
+        q.error = V.err;
+      } else {
+        for (int c = 0; c < q.nrhs; c++)
+          std::copy(xs.begin() + (int64_t)c * V.n, xs.begin() + (int64_t)(c + 1) * V.n,
+                    q.x + (int64_t)c * q.ldx);
+        q.stats = V.stats;
+      }
+      std::lock_guard<std::mutex> lk(mu);
+      q.t_done = Clock::now();
+      q.done = true;
+      cv_done.notify_all();
+    }
+  }
+
+  // A batch member's private layout: element offsets of its front and
+  // separator copies, and the map of an arena offset into them.
+  struct BatchM {
+    int64_t poolF = 0, poolS = 0;
+    std::vector<int64_t> fnew, snew;
+    int64_t move(const Schedule& s, const std::vector<char>& dirty, const std::vector<char>& dsep,
+                 int16_t arena, int64_t off) const {
+      if (arena == mfgpu::AR_FRONT) {
+        int lo = 0, hi = (int)s.fronts.size() - 1;   // front whose storage holds off
         while (lo < hi) {
           const int mid = (lo + hi + 1) >> 1;
           if (s.fronts[mid].off <= off) lo = mid;
           else hi = mid - 1;
         }
-        return lo;
-      };
-      auto ownerS = [&](int64_t off) {
-        int lo = 0, hi = (int)s.seps.size() - 1;
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (s.seps[mid].off <= off) lo = mid;
-          else hi = mid - 1;
-        }
-        return lo;
-      };
-      auto move = [&](int16_t arena, int64_t off) {
-        if (arena == mfgpu::AR_FRONT) {
-          const int f = ownerF(off);
-          return dirty[f] ? poolF + fnew[f] + (off - s.fronts[f].off) : off;
-        }
-        const int k = ownerS(off);
-        return dsep[k] ? poolS + snew[k] + (off - s.seps[k].off) : off;
-      };
-      for (Task& t : V.upd.tasks) {
-        t.dst_off = move(t.dst_arena, t.dst_off);
-        if (t.kind == mfgpu::TK_COPY || t.kind == mfgpu::TK_ADD)
-          t.src_off = move(t.src_arena, t.src_off);
+        return dirty[lo] ? poolF + fnew[lo] + (off - s.fronts[lo].off) : off;
       }
-      V.upd.upload(V.stream);
-      // block inverses: the base's, then the dirty fronts' own
-      if (V.dinvElems > 0)
-        ck(cudaMemcpyAsync(V.d_Dinv, base->d_Dinv, V.dinvElems * V.esz, cudaMemcpyDeviceToDevice,
-                           V.stream), "copy block inverses");
-      // refactor the private root paths, then solve
-      V.factorWith(nullptr, true, V.upd, false);
-      V.checkDevError();
-      r.nfronts = nd;
-    });
-    if (st != MFGPU_OK) {
-      r.status = st;
-      r.error = V.err;
-      return;
+      int lo = 0, hi = (int)s.seps.size() - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s.seps[mid].off <= off) lo = mid;
+        else hi = mid - 1;
+      }
+      return dsep[lo] ? poolS + snew[lo] + (off - s.seps[lo].off) : off;
     }
-    V.factored = true;
-    std::vector<double> xs((size_t)V.n * r.nrhs);
-    const int rc = solveOrApply(&V, r.b.data(), xs.data(), r.nrhs, V.n, false, false);
-    r.status = rc;
-    if (rc != MFGPU_OK) {
-      r.error = V.err;
-      return;
-    }
-    for (int c = 0; c < r.nrhs; c++)
-      std::copy(xs.begin() + (int64_t)c * V.n, xs.begin() + (int64_t)(c + 1) * V.n,
-                r.x + (int64_t)c * r.ldx);
-    r.stats = V.stats;
-  }
+  };
 };
 
 namespace {
@@ -2620,6 +2860,7 @@ std::unique_ptr<mfgpu_handle> makeView(mfgpu_handle& B) {
   H.d_gbar = dalloc<unsigned>(1, "alloc grid barrier");
   H.dinvElems = B.dinvElems;
   H.d_dinv_off = B.d_dinv_off;
+  H.h_dinv_off = B.h_dinv_off;
   H.flow = B.flow;
   H.d_flow = B.d_flow;
   H.maxFlags = B.maxFlags;
@@ -2647,6 +2888,7 @@ int mfgpu_server_create(mfgpu_handle* base, const double* d_coef, const double* 
     return fail(base, MFGPU_ERR_ARG, "the serving loop takes one problem of width 1");
   std::unique_ptr<mfgpu_server> S(new mfgpu_server());
   S->base = base;
+  S->capacity = slots;
   if (hxyz)
     for (int a = 0; a < 3; a++) S->h[a] = hxyz[a];
   const int st = guarded(base, [&]() {
@@ -2657,19 +2899,25 @@ int mfgpu_server_create(mfgpu_handle* base, const double* d_coef, const double* 
        "copy coefficients");
     S->pool_elems = pool_bytes / (int64_t)base->esz;
     S->d_pool = dalloc<unsigned char>((size_t)S->pool_elems * base->esz, "alloc server pool");
-    S->pool.reset(new PoolAlloc(S->pool_elems));
-    S->base_table.resize(s.fronts.size());
-    for (size_t i = 0; i < s.fronts.size(); i++) {
+    const size_t nF = s.fronts.size();
+    S->base_table.resize(nF);
+    for (size_t i = 0; i < nF; i++) {
       const mfgpu::Front& f = s.fronts[i];
       S->base_table[i] = FrontDev{f.off, f.dof_off, f.n, f.m, f.N, f.ld};
     }
-    for (int k = 0; k < slots; k++) {
-      S->views.push_back(makeView(*base));
-      S->slot_coef.push_back(dalloc<double>(S->coef_elems, "alloc slot coefficients"));
-    }
+    S->view = makeView(*base);
+    // the view's kernels read a different front table, values and block
+    // inverses for every batch member, so nothing may be replayed from a graph
+    S->view->graphs = false;
+    S->d_coefB = dalloc<double>((size_t)slots * S->coef_elems, "alloc batch coefficients");
+    S->d_valB = dalloc<double>((size_t)slots * base->nnz, "alloc batch values");
+    S->d_DinvB = dalloc<unsigned char>(
+        (size_t)slots * std::max<int64_t>(base->dinvElems, 1) * base->esz, "alloc batch inverses");
+    S->d_frB = dalloc<FrontDev>((size_t)(slots + 1) * nF, "alloc batch front table");
+    S->d_dinv_offB = dalloc<int64_t>((size_t)(slots + 1) * nF, "alloc batch inverse offsets");
   });
   if (st != MFGPU_OK) return st;
-  for (int k = 0; k < slots; k++) S->workers.emplace_back([srv = S.get(), k]() { srv->run(k); });
+  S->worker = std::thread([srv = S.get()]() { srv->run(); });
   *out = S.release();
   return MFGPU_OK;
 }
@@ -2725,6 +2973,7 @@ int mfgpu_server_wait(mfgpu_server* srv, int64_t ticket, mfgpu_request_info* inf
     info->queued_seconds = us(r->t_start - r->t_submit);
     info->latency_seconds = us(r->t_done - r->t_submit);
     info->fronts = r->nfronts;
+    info->batch = r->batch;
     info->pool_bytes = r->footprint * (int64_t)srv->base->esz;
     info->iterations = r->stats.iterations;
     info->residual = r->stats.residual;

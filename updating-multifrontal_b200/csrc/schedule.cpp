@@ -778,7 +778,7 @@ Schedule::Schedule(std::vector<Schedule>&& batch) {
   };
   auto remap = [&](Task t, int p, bool front_owner) {
     t.dst_off += t.dst_arena == AR_FRONT ? fbase[p] : sbase[p];
-    t.src_off += t.src_arena == AR_FRONT ? fbase[p] : sbase[p];
+    if (t.kind != TK_SPARSE) t.src_off += t.src_arena == AR_FRONT ? fbase[p] : sbase[p];
     if (t.kind == TK_SPARSE) {
       t.row_dof = t.rows > 0 ? tpos(p, t.row_dof) : 0;
       t.col_dof = t.cols > 0 ? tpos(p, t.col_dof) : 0;

@@ -30,7 +30,9 @@ enum Arena : int32_t { AR_FRONT = 0, AR_SEP = 1 };
 // One rectangular block operation.  Element (i, j), 0 <= i < rows, 0 <= j < cols:
 //   dst[dst_off + i + j*dst_ld]  (op)  src[src_off + (trans ? j + i*src_ld : i + j*src_ld)]
 // lower != 0 restricts the block to i >= j (diagonal blocks of symmetric storage).
-// For TK_SPARSE the DOFs are dofs[row_dof + i] and dofs[col_dof + j].
+// For TK_SPARSE the DOFs are dofs[row_dof + i] and dofs[col_dof + j], and
+// src_off is the element offset of the matrix's CSR values (0 here; the
+// serving loop sets it when one plan covers several matrices).
 struct Task {
   int64_t dst_off;
   int64_t src_off;

@@ -313,7 +313,10 @@ class Server:
     submit(lo, hi, factor, b) queues a request (coefficients of the cell box
     [lo, hi) times `factor`, right-hand sides b of shape (n,) or (n, k)) and
     returns a ticket; wait(ticket) returns (x, info).  Requests are independent:
-    each answer is that of the base matrix under its own change.
+    each answer is that of the base matrix under its own change.  Queued
+    requests are served in batches of at most `slots` whose private root-path
+    copies fit in the pool together; a batch's root paths are refactored by
+    one set of level launches (info["batch"]: the batch size).
     """
 
     def __init__(self, F, coef, slots=4, pool_gb=8.0, h=(1.0, 1.0, 1.0)):

@@ -54,7 +54,7 @@ class Info(C.Structure):
 
 
 class RequestInfo(C.Structure):
-    _fields_ = [("status", C.c_int), ("fronts", C.c_int), ("iterations", C.c_int), ("pad", C.c_int),
+    _fields_ = [("status", C.c_int), ("fronts", C.c_int), ("iterations", C.c_int), ("batch", C.c_int),
                 ("queued_seconds", C.c_double), ("latency_seconds", C.c_double),
                 ("residual", C.c_double), ("pool_bytes", C.c_int64), ("reserved", C.c_int64 * 4)]
 
