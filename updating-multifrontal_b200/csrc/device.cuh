@@ -144,6 +144,12 @@ int tc_pack_cap(const std::vector<int>& n, const std::vector<int>& N, int K, int
 size_t tc_pack_bytes(int nf, int cap);
 cudaError_t launch_tc_pack(const int* flist, int nf, int cap, const FrontDev* fr, const float* F,
                            int K, int w, int split, void* pack, cudaStream_t st);
+// Sub-panel [Ks, Ks + w) (w <= subpanel_max()) of every front in flist turned
+// into L (diagonal-block Cholesky and the solve of the rows below) by one
+// launch without grid barriers; mixed path, after every earlier update.
+int subpanel_max();
+cudaError_t launch_subpanel(const int* flist, int nf, const FrontDev* fr, float* F, int Ks, int w,
+                            DevError* err, cudaStream_t st);
 cudaError_t launch_trail_tc(const int* flist, int nf, int64_t ntiles, const FrontDev* fr, float* F,
                             int K, int w, int cend, int split, int cap, const void* pack,
                             DevError* err, cudaStream_t st);

@@ -316,14 +316,17 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_bwd(const int* __restrict__ 
 }
 
 // Persistent grid: every CTA the SMs hold at once (a cooperative launch checks
-// that they are all resident, which the flag waits rely on).
+// that they are all resident, which the flag waits rely on).  As many CTAs as
+// fit, so that the row blocks of a long chain (a root front has hundreds) each
+// get their own CTA from the start and accumulate the solved blocks as they
+// come, instead of queueing behind other tasks of the same CTA.
 template <class K>
 int flowGrid(K kern) {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, SCT, 0);
-  return sms * std::max(1, std::min(per, 2));
+  return sms * std::max(1, per);
 }
 
 template <class T, int NR>

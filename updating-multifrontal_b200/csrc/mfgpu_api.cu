@@ -339,6 +339,8 @@ struct mfgpu_handle {
   int tcSub = 128;                 // mixed: sub-panel width inside each 512-column outer panel of a
                                    // tensor-core level (0 or 512: no sub-panels)
   int fusedMinFronts = 148;        // fewest fronts for the one-CTA-per-front kernel
+  bool subpanel = true;            // tensor-core levels: sub-panels by k_subpanel (MFGPU_SUBPANEL=0:
+                                   // by the cooperative kernel)
   size_t esz = sizeof(double);     // bytes per factor element
   double* d_scale = nullptr;       // s = 1/sqrt(diag(A)) of the last full factorization
   double* d_iscale = nullptr;      // 1/s
@@ -1025,10 +1027,16 @@ struct mfgpu_handle {
     for (int K = 0; K < L.maxn; K += W) {
       for (int Ks = K; Ks < K + W && Ks < L.maxn; Ks += w) {
         prof.begin(MFGPU_KC_COOP, stream);
-        ck(mfgpu::launch_level_coop<float>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, (float*)d_F,
-                                           d_err, (float*)d_slots, P.d_cpref + L.cpref0, d_gbar,
-                                           stream, Ks, Ks + w, phase0, 0, L.coopItems, w),
-           "launch cooperative panel factorization (k_level_coop)");
+        if (subpanel && w <= mfgpu::subpanel_max()) {
+          ck(mfgpu::launch_subpanel(P.d_ids + L.f0, (int)L.nf, d_fr, (float*)d_F, Ks, w, d_err,
+                                    stream),
+             "launch sub-panel factorization (k_subpanel)");
+        } else {
+          ck(mfgpu::launch_level_coop<float>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, (float*)d_F,
+                                             d_err, (float*)d_slots, P.d_cpref + L.cpref0, d_gbar,
+                                             stream, Ks, Ks + w, phase0, 0, L.coopItems, w),
+             "launch cooperative panel factorization (k_level_coop)");
+        }
         prof.end(stream);
         phase0 += mfgpu::coop_phases(Ks, L.maxn, w);
         if (Ks + w < K + W) update(Ks, w, K + W);   // the outer panel's remaining columns
@@ -1623,6 +1631,7 @@ int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const
   if (const char* e = getenv("MFGPU_TC_SPLIT3_LEVELS")) h->tcSplit3Levels = atoi(e);
   if (const char* e = getenv("MFGPU_TC_SUB")) h->tcSub = atoi(e);
   if (const char* e = getenv("MFGPU_GRAPHS")) h->graphs = e[0] != '0';
+  if (const char* e = getenv("MFGPU_SUBPANEL")) h->subpanel = e[0] != '0';
   if (h->lu) h->solveCoopMinN = 0;   // LU fronts use the per-front sweeps
   h->h_rowptr.assign(row_ptr, row_ptr + n + 1);
   h->h_colind.assign(col_ind, col_ind + h->nnz);
@@ -2833,6 +2842,7 @@ std::unique_ptr<mfgpu_handle> makeView(mfgpu_handle& B) {
   H.tcSplit = B.tcSplit;
   H.tcSplit3Levels = B.tcSplit3Levels;
   H.tcSplitLow = B.tcSplitLow;
+  H.subpanel = B.subpanel;
   H.tcSub = B.tcSub;
   H.fusedMinFronts = B.fusedMinFronts;
   H.d_scale = B.d_scale;
