@@ -654,8 +654,8 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subpanel(const int* __restri
           const int q = j + 1 + idx % m, c = j + 1 + idx / m;
           if (c <= q) Ds[q * kSubS + c] -= Ds[q * kSubS + j] * Ds[c * kSubS + j];
         }
+        __syncthreads();                    // the next pivot is final
       }
-      __syncthreads();
     }
     const int local = item - pre[i];
     if (local == 0) {   // the factored diagonal block back into the front
