@@ -273,7 +273,8 @@ int mfgpu_load(mfgpu_handle* h, const char* path);
 /* Autotuner (no counterpart in the reference): a full factorization, like
  * mfgpu_factor, that also picks each tree level's kernel by timing.  For every
  * level with more than one eligible kernel - one CTA per front
- * (MFGPU_LEVEL_FUSED), the cooperative level kernel (MFGPU_LEVEL_COOP), the
+ * (MFGPU_LEVEL_FUSED), the cooperative level kernel (MFGPU_LEVEL_COOP),
+ * panel-by-panel launches without grid barriers (MFGPU_LEVEL_PANEL), the
  * tensor-core update (MFGPU_LEVEL_TC, mixed precision) - each candidate runs
  * `reps` times on freshly assembled fronts and the fastest is kept; later
  * full factorizations (mfgpu_factor / mfgpu_refactor*) use the table, localized
@@ -281,7 +282,7 @@ int mfgpu_load(mfgpu_handle* h, const char* path);
  * `choices` (may be NULL) receives the kernel of each level, root = 0,
  * mfgpu_get_info().levels entries. */
 enum { MFGPU_LEVEL_NONE = -1, MFGPU_LEVEL_FUSED = 0, MFGPU_LEVEL_COOP = 1, MFGPU_LEVEL_TC = 2,
-       MFGPU_LEVEL_STEPPED = 3 };
+       MFGPU_LEVEL_STEPPED = 3, MFGPU_LEVEL_LU = 4, MFGPU_LEVEL_PANEL = 5 };
 int mfgpu_autotune(mfgpu_handle* h, int reps, int* choices);
 
 /* Per-kernel-class device timing (no reference counterpart; the reference's

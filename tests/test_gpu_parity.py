@@ -164,3 +164,32 @@ def test_cooperative_sweeps_vs_oracle(dim, N, ms, nrhs, env_var):
     Xg = G.Solve(b.T)
     assert rel(X, Xg) < 1e-13
     assert np.array_equal(F.Solve(b.T), X)      # deterministic
+
+
+@pytest.mark.parametrize("dim,N,ms", [(2, (255, 255), 4), (2, (130, 70), 4), (3, (31, 31, 31), 4),
+                                      (3, (13, 17, 11), 3)])
+@pytest.mark.parametrize("kernel", ["panel", "coop"])
+def test_level_kernels_vs_oracle(dim, N, ms, kernel, env_var):
+    """Levels of moderate fronts factored panel by panel (k_subpanel +
+    k_trail_syrk, the default up to 4096 unknowns) or by the cooperative
+    kernel (MFGPU_PANEL_MAX_N=0): both within 1e-12 of the oracle, before and
+    after a localized update."""
+    env_var("MFGPU_PANEL_MAX_N", 4096 if kernel == "panel" else 0)
+    a, A, b = problem(dim, N, seed=17, nrhs=2)
+    F = make(dim, N, A, ms)
+    F.profile(True)
+    F.Factor()
+    X = F.Solve(b.T)
+    O = mf_oracle.MFOracle(A.to_scipy(), N, 1, ms)
+    O.factor()
+    for r in range(2):
+        assert rel(X[:, r], O.solve(b[r])) < 1e-12
+    side = 9 if dim == 2 else 4
+    a2, _ = patch_update(a, N, side, 10.0, seed=5)
+    A2 = stencil.build_laplacian(a2)
+    mod = stencil.modified_dofs(A, A2)
+    F.Update(A2, mod)
+    O.update(A2.to_scipy(), mod)
+    X2 = F.Solve(b.T)
+    for r in range(2):
+        assert rel(X2[:, r], O.solve(b[r])) < 1e-12

@@ -144,12 +144,19 @@ int tc_pack_cap(const std::vector<int>& n, const std::vector<int>& N, int K, int
 size_t tc_pack_bytes(int nf, int cap);
 cudaError_t launch_tc_pack(const int* flist, int nf, int cap, const FrontDev* fr, const float* F,
                            int K, int w, int split, void* pack, cudaStream_t st);
-// Sub-panel [Ks, Ks + w) (w <= subpanel_max()) of every front in flist turned
-// into L (diagonal-block Cholesky and the solve of the rows below) by one
-// launch without grid barriers; mixed path, after every earlier update.
-int subpanel_max();
-cudaError_t launch_subpanel(const int* flist, int nf, const FrontDev* fr, float* F, int Ks, int w,
+// Panel-by-panel partial Cholesky without grid barriers (kernels_panel.cu):
+// launch_subpanel turns the panel [Ks, Ks + w) of every front in flist into L
+// (w = panel_width(sizeof(T)): 64 FP64, 128 FP32; every earlier update
+// applied), launch_trail_syrk applies it to the trailing lower triangle.  At
+// most kMaxPanelFronts fronts per launch.
+constexpr int kPanelW64 = 64, kPanelW32 = 128, kMaxPanelFronts = 1024;
+int panel_width(int elem_bytes);
+template <class T>
+cudaError_t launch_subpanel(const int* flist, int nf, const FrontDev* fr, T* F, int Ks, int w,
                             DevError* err, cudaStream_t st);
+template <class T>
+cudaError_t launch_trail_syrk(const int* flist, int nf, const FrontDev* fr, T* F, int Ks, int w,
+                              cudaStream_t st);
 cudaError_t launch_trail_tc(const int* flist, int nf, int64_t ntiles, const FrontDev* fr, float* F,
                             int K, int w, int cend, int split, int cap, const void* pack,
                             DevError* err, cudaStream_t st);

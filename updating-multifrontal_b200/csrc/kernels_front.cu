@@ -777,6 +777,45 @@ __global__ void __launch_bounds__(kCT) k_level_coop(const int* __restrict__ flis
   }
 }
 
+// Trailing update of the panel-by-panel factorization (kernels_panel.cu):
+// C(k1:N, k1:N) -= P P^T, P = L(k1:N, Ks:k1), k1 = min(Ks + w, n), lower
+// 64 x 64 tiles of every front over a persistent grid.
+template <class T>
+__global__ void __launch_bounds__(kCT) k_trail_syrk(const int* __restrict__ flist, int nf,
+                                                    const FrontDev* __restrict__ fr,
+                                                    T* __restrict__ F, int Ks, int w) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* Xa = reinterpret_cast<T*>(smraw);
+  T* Xb = Xa + 64 * kPS;
+  __shared__ int pre[kMaxPanelFronts + 1];
+  const int tid = threadIdx.x;
+  for (int i = tid; i < nf; i += kCT) {
+    const FrontDev d = fr[flist[i]];
+    const int k1 = min(Ks + w, d.n), t = (d.N - k1 + 63) / 64;
+    pre[i + 1] = Ks < d.n && d.N > k1 ? t * (t + 1) / 2 : 0;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    pre[0] = 0;
+    for (int i = 0; i < nf; i++) pre[i + 1] += pre[i];
+  }
+  __syncthreads();
+  const int total = pre[nf];
+  for (int item = blockIdx.x; item < total; item += gridDim.x) {
+    int lo = 0, hi = nf - 1;   // largest i with pre[i] <= item
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (pre[mid] <= item) lo = mid;
+      else hi = mid - 1;
+    }
+    const FrontDev d = fr[flist[lo]];
+    const int k1 = min(Ks + w, d.n);
+    int I, J;
+    tri_index(item - pre[lo], I, J);
+    coop_tile_update(F + d.off, d.ld, d.N, d.N, k1 + I * 64, k1 + J * 64, Ks, k1, Xa, Xb);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Solve / apply sweeps.  One CTA per front; W is the front's workspace (N x nrhs,
 // ld N) inside a shared buffer.
@@ -1661,6 +1700,25 @@ void launch_lu_apply_up(const int* flist, int nf, const FrontDev* fr, const doub
   g_launches++;
 }
 
+template <class T>
+cudaError_t launch_trail_syrk(const int* flist, int nf, const FrontDev* fr, T* F, int Ks, int w,
+                              cudaStream_t st) {
+  if (nf <= 0) return cudaSuccess;
+  if (nf > kMaxPanelFronts || w <= 0) return cudaErrorInvalidValue;
+  const size_t sm = 2 * 64 * kPS * sizeof(T);
+  static const int grid = [sm]() {   // thread-safe one-time set-up: every resident CTA
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaFuncSetAttribute(k_trail_syrk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trail_syrk<T>, kCT, sm);
+    return sms * std::max(1, per);
+  }();
+  k_trail_syrk<T><<<grid, kCT, sm, st>>>(flist, nf, fr, F, Ks, w);
+  g_launches++;
+  return cudaGetLastError();
+}
+
 #define MFGPU_INSTANTIATE(T)                                                                      \
   template void launch_tasks<T>(const Task*, const int64_t*, int, int64_t, T*, T*, const int*,     \
                                 const int*, const double*, const int*, const double*, cudaStream_t); \
@@ -1682,7 +1740,9 @@ void launch_lu_apply_up(const int* flist, int nf, const FrontDev* fr, const doub
   template void launch_root_apply<T>(int, const FrontDev*, const T*, const int*, T*, int64_t, int, \
                                      T*, const int64_t*, cudaStream_t);                             \
   template void launch_sep_gather<T>(const int*, int, const SepDev*, const int*, T*, int64_t, int, \
-                                     const T*, const int64_t*, const FrontDev*, cudaStream_t);
+                                     const T*, const int64_t*, const FrontDev*, cudaStream_t);      \
+  template cudaError_t launch_trail_syrk<T>(const int*, int, const FrontDev*, T*, int, int,       \
+                                            cudaStream_t);
 
 MFGPU_INSTANTIATE(double)
 MFGPU_INSTANTIATE(float)

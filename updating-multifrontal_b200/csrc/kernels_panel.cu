@@ -1,0 +1,199 @@
+// Panel-by-panel partial Cholesky without grid barriers (both precisions).
+//
+// The reference factors a front's pivot block and forms its Schur complement
+// in one dense LU call sequence (src/DE/mf2d.cpp:558-576).  Here, for the
+// fronts of one tree level, every W-column panel [Ks, Ks + kb) (kb = min(W,
+// n - Ks)) takes two launches:
+//   k_subpanel     every CTA loads the kb x kb diagonal block into shared memory
+//                  and factors it itself (right-looking Cholesky; the same
+//                  arithmetic in every CTA), then takes 128-row blocks of the
+//                  rows below, solves them against it (X <- X L^{-T}, each
+//                  row by two threads) and writes them back; the first item
+//                  of a front writes the factored block back;
+//   k_trail_syrk   the trailing lower triangle, C(k1:N, k1:N) -= P P^T with
+//                  P = L(k1:N, Ks:k1), in 64 x 64 tiles (FP64: DMMA m8n8k4;
+//                  FP32: FFMA), all fronts' tiles over all SMs.
+// Every element of a panel is read and written once by k_subpanel and no CTA
+// waits for another, so a level of a few small fronts (the top of a 2D tree)
+// costs two short launches per panel instead of two grid barriers per 32
+// columns.  The tensor-core levels of the mixed path use k_subpanel alone for
+// their 128-column sub-panels (their updates run on the tensor cores).
+// A non-positive pivot records error code 1.
+#include <algorithm>
+#include <atomic>
+#include <cstdint>
+
+#include "device.cuh"
+
+namespace mfgpu {
+
+extern std::atomic<long long> g_launches;
+
+namespace {
+
+constexpr int kSubRows = 128;             // rows per solve item
+constexpr int kSubThreads = 256;
+
+template <class T>
+__device__ __forceinline__ T rsq(T x);
+template <>
+__device__ __forceinline__ float rsq<float>(float x) { return rsqrtf(x); }
+template <>
+__device__ __forceinline__ double rsq<double>(double x) { return rsqrt(x); }
+
+template <int W>
+constexpr int sub_stride() { return W + 1; }
+
+template <class T, int W>
+constexpr size_t sub_smem() {
+  return (size_t)(W + kSubRows) * sub_stride<W>() * sizeof(T) + W * sizeof(T);
+}
+
+template <class T, int W>
+__global__ void __launch_bounds__(kSubThreads) k_subpanel(const int* __restrict__ flist, int nf,
+                                                          const FrontDev* __restrict__ fr,
+                                                          T* __restrict__ F, int Ks,
+                                                          DevError* err) {
+  constexpr int S = sub_stride<W>();
+  extern __shared__ __align__(16) unsigned char sub_raw[];
+  T* Ds = reinterpret_cast<T*>(sub_raw);   // diagonal block, lower, row-major stride S
+  T* Xs = Ds + W * S;                      // a 128-row block of the panel
+  T* Dinv = Xs + kSubRows * S;             // 1 / L(c, c)
+  __shared__ int pre[kMaxPanelFronts + 1];
+  const int tid = threadIdx.x;
+  // items per front (in parallel), then their prefix (thread 0, shared memory)
+  for (int i = tid; i < nf; i += kSubThreads) {
+    const FrontDev d = fr[flist[i]];
+    pre[i + 1] = Ks < d.n ? 1 + (d.N - Ks - min(W, d.n - Ks) + kSubRows - 1) / kSubRows : 0;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    pre[0] = 0;
+    for (int i = 0; i < nf; i++) pre[i + 1] += pre[i];
+  }
+  __syncthreads();
+  const int total = pre[nf];
+  int cur = -1;
+  for (int item = blockIdx.x; item < total; item += gridDim.x) {
+    int lo = 0, hi = nf - 1;   // largest i with pre[i] <= item
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (pre[mid] <= item) lo = mid;
+      else hi = mid - 1;
+    }
+    const int i = lo, f = flist[i];
+    const FrontDev d = fr[f];
+    T* A = F + d.off;
+    const int64_t ld = d.ld;
+    const int kb = min(W, d.n - Ks);
+    if (i != cur) {
+      // load and factor the diagonal block
+      cur = i;
+      __syncthreads();
+      for (int idx = tid; idx < kb * kb; idx += kSubThreads) {
+        const int r = idx % kb, c = idx / kb;
+        Ds[r * S + c] = r >= c ? A[(Ks + r) + (int64_t)(Ks + c) * ld] : T(0);
+      }
+      __syncthreads();
+      for (int j = 0; j < kb; j++) {
+        T dj = Ds[j * S + j];
+        if (!(dj > T(0))) {                 // non-positive or NaN pivot: not SPD
+          if (tid == 0 && atomicCAS(&err->code, 0, 1) == 0) {
+            err->front = f;
+            err->col = Ks + j;
+          }
+          dj = T(1);
+        }
+        const T r = rsq<T>(dj);
+        __syncthreads();                    // every thread has read L(j, j)
+        if (tid == 0) {
+          Ds[j * S + j] = dj * r;
+          Dinv[j] = r;
+        }
+        for (int q = j + 1 + tid; q < kb; q += kSubThreads) Ds[q * S + j] *= r;
+        __syncthreads();
+        const int m = kb - j - 1;
+        for (int idx = tid; idx < m * m; idx += kSubThreads) {
+          const int q = j + 1 + idx % m, c = j + 1 + idx / m;
+          if (c <= q) Ds[q * S + c] -= Ds[q * S + j] * Ds[c * S + j];
+        }
+        __syncthreads();                    // the next pivot is final
+      }
+    }
+    const int local = item - pre[i];
+    if (local == 0) {   // the factored diagonal block back into the front
+      for (int idx = tid; idx < kb * kb; idx += kSubThreads) {
+        const int r = idx % kb, c = idx / kb;
+        if (r >= c) A[(Ks + r) + (int64_t)(Ks + c) * ld] = Ds[r * S + c];
+      }
+      continue;
+    }
+    const int r0 = Ks + kb + (local - 1) * kSubRows, rows = min(kSubRows, d.N - r0);
+    __syncthreads();
+    for (int idx = tid; idx < kSubRows * kb; idx += kSubThreads) {
+      const int r = idx % kSubRows, c = idx / kSubRows;
+      Xs[r * S + c] = r < rows ? A[(r0 + r) + (int64_t)(Ks + c) * ld] : T(0);
+    }
+    __syncthreads();
+    {
+      // row r by the thread pair (2r, 2r + 1), adjacent lanes: each sums every
+      // other earlier column, the pair combines, both keep the solved value
+      const int r = tid >> 1, h = tid & 1;
+      T* x = Xs + r * S;
+      for (int c = 0; c < kb; c++) {
+        const T* lc = Ds + c * S;
+        T p = T(0);
+        for (int t = h; t < c; t += 2) p = fma(x[t], lc[t], p);
+        p += __shfl_xor_sync(0xffffffffu, p, 1);
+        const T v = (x[c] - p) * Dinv[c];
+        __syncwarp();
+        if (h == 0) x[c] = v;
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < kSubRows * kb; idx += kSubThreads) {
+      const int r = idx % kSubRows, c = idx / kSubRows;
+      if (r < rows) A[(r0 + r) + (int64_t)(Ks + c) * ld] = Xs[r * S + c];
+    }
+  }
+}
+
+template <class T, int W>
+cudaError_t launchSub(const int* flist, int nf, const FrontDev* fr, T* F, int Ks, DevError* err,
+                      cudaStream_t st) {
+  static const int grid = []() {   // thread-safe one-time set-up: every resident CTA
+    int dev = 0, n = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    cudaFuncSetAttribute(k_subpanel<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sub_smem<T, W>());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_subpanel<T, W>, kSubThreads,
+                                                  sub_smem<T, W>());
+    return n * std::max(1, per);
+  }();
+  k_subpanel<T, W><<<grid, kSubThreads, sub_smem<T, W>(), st>>>(flist, nf, fr, F, Ks, err);
+  g_launches++;
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+int panel_width(int elem_bytes) { return elem_bytes == 8 ? kPanelW64 : kPanelW32; }
+
+template <>
+cudaError_t launch_subpanel<float>(const int* flist, int nf, const FrontDev* fr, float* F, int Ks,
+                                   int w, DevError* err, cudaStream_t st) {
+  if (nf <= 0) return cudaSuccess;
+  if (nf > kMaxPanelFronts || w != kPanelW32) return cudaErrorInvalidValue;
+  return launchSub<float, kPanelW32>(flist, nf, fr, F, Ks, err, st);
+}
+template <>
+cudaError_t launch_subpanel<double>(const int* flist, int nf, const FrontDev* fr, double* F, int Ks,
+                                    int w, DevError* err, cudaStream_t st) {
+  if (nf <= 0) return cudaSuccess;
+  if (nf > kMaxPanelFronts || w != kPanelW64) return cudaErrorInvalidValue;
+  return launchSub<double, kPanelW64>(flist, nf, fr, F, Ks, err, st);
+}
+
+}  // namespace mfgpu

@@ -572,134 +572,9 @@ __global__ void __launch_bounds__(TCT, 1) k_trail_tc(const int* __restrict__ fli
                  "r"(NACC * TN));
 }
 
-// ---------------------------------------------------------------------------
-// Sub-panel factorization of the tensor-core levels, without grid barriers.
-// Columns [Ks, Ks + kb) (kb = min(w, n - Ks) <= 128) of every front, already
-// updated by every earlier panel, become L: every CTA loads the kb x kb
-// diagonal block into shared memory and factors it itself (right-looking
-// Cholesky; the same arithmetic in every CTA), then takes 128-row blocks of
-// the rows below and solves them against it, X <- X L^{-T}, each row by two
-// threads; the first item of a front writes the factored block back.  So each
-// element of the sub-panel is read and written once and no CTA waits for
-// another.  A non-positive pivot records error code 1 (one CTA reports it).
-constexpr int kSubW = 128;                // widest sub-panel
-constexpr int kSubS = kSubW + 1;          // shared-memory row stride
-constexpr int kSubThreads = 256;
-constexpr size_t kSubSmem = (size_t)2 * kSubW * kSubS * sizeof(float) + kSubW * sizeof(float);
-
-__global__ void __launch_bounds__(kSubThreads, 1) k_subpanel(const int* __restrict__ flist, int nf,
-                                                             const FrontDev* __restrict__ fr,
-                                                             float* __restrict__ F, int Ks, int w,
-                                                             DevError* err) {
-  extern __shared__ __align__(16) float sub_sm[];
-  float* Ds = sub_sm;                      // diagonal block, lower, row-major stride kSubS
-  float* Xs = Ds + kSubW * kSubS;          // a 128-row block of the panel
-  float* Dinv = Xs + kSubW * kSubS;        // 1 / L(c, c)
-  __shared__ int pre[kMaxTcFronts + 1];
-  const int tid = threadIdx.x;
-  // items per front (in parallel), then their prefix (thread 0, shared memory)
-  for (int i = tid; i < nf; i += kSubThreads) {
-    const FrontDev d = fr[flist[i]];
-    pre[i + 1] = Ks < d.n ? 1 + (d.N - Ks - min(w, d.n - Ks) + kSubW - 1) / kSubW : 0;
-  }
-  __syncthreads();
-  if (tid == 0) {
-    pre[0] = 0;
-    for (int i = 0; i < nf; i++) pre[i + 1] += pre[i];
-  }
-  __syncthreads();
-  const int total = pre[nf];
-  int cur = -1;
-  for (int item = blockIdx.x; item < total; item += gridDim.x) {
-    int lo = 0, hi = nf - 1;   // largest i with pre[i] <= item
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (pre[mid] <= item) lo = mid;
-      else hi = mid - 1;
-    }
-    const int i = lo, f = flist[i];
-    const FrontDev d = fr[f];
-    float* A = F + d.off;
-    const int64_t ld = d.ld;
-    const int kb = min(w, d.n - Ks);
-    if (i != cur) {
-      // load and factor the diagonal block
-      cur = i;
-      __syncthreads();
-      for (int idx = tid; idx < kb * kb; idx += kSubThreads) {
-        const int r = idx % kb, c = idx / kb;
-        Ds[r * kSubS + c] = r >= c ? A[(Ks + r) + (int64_t)(Ks + c) * ld] : 0.0f;
-      }
-      __syncthreads();
-      for (int j = 0; j < kb; j++) {
-        float dj = Ds[j * kSubS + j];
-        if (!(dj > 0.0f)) {                 // non-positive or NaN pivot: not SPD
-          if (tid == 0 && blockIdx.x == (unsigned)(pre[i] % gridDim.x) &&
-              atomicCAS(&err->code, 0, 1) == 0) {
-            err->front = f;
-            err->col = Ks + j;
-          }
-          dj = 1.0f;
-        }
-        const float r = rsqrtf(dj);
-        __syncthreads();                    // every thread has read L(j, j)
-        if (tid == 0) {
-          Ds[j * kSubS + j] = dj * r;
-          Dinv[j] = r;
-        }
-        for (int q = j + 1 + tid; q < kb; q += kSubThreads) Ds[q * kSubS + j] *= r;
-        __syncthreads();
-        const int m = kb - j - 1;
-        for (int idx = tid; idx < m * m; idx += kSubThreads) {
-          const int q = j + 1 + idx % m, c = j + 1 + idx / m;
-          if (c <= q) Ds[q * kSubS + c] -= Ds[q * kSubS + j] * Ds[c * kSubS + j];
-        }
-        __syncthreads();                    // the next pivot is final
-      }
-    }
-    const int local = item - pre[i];
-    if (local == 0) {   // the factored diagonal block back into the front
-      for (int idx = tid; idx < kb * kb; idx += kSubThreads) {
-        const int r = idx % kb, c = idx / kb;
-        if (r >= c) A[(Ks + r) + (int64_t)(Ks + c) * ld] = Ds[r * kSubS + c];
-      }
-      continue;
-    }
-    const int r0 = Ks + kb + (local - 1) * kSubW, rows = min(kSubW, d.N - r0);
-    __syncthreads();
-    for (int idx = tid; idx < kSubW * kb; idx += kSubThreads) {
-      const int r = idx % kSubW, c = idx / kSubW;
-      Xs[r * kSubS + c] = r < rows ? A[(r0 + r) + (int64_t)(Ks + c) * ld] : 0.0f;
-    }
-    __syncthreads();
-    {
-      // row r by the thread pair (2r, 2r + 1), adjacent lanes: each sums every
-      // other earlier column, the pair combines, both keep the solved value
-      const int r = tid >> 1, h = tid & 1;
-      float* x = Xs + r * kSubS;
-      for (int c = 0; c < kb; c++) {
-        const float* lc = Ds + c * kSubS;
-        float p = 0.0f;
-        for (int t = h; t < c; t += 2) p = fmaf(x[t], lc[t], p);
-        p += __shfl_xor_sync(0xffffffffu, p, 1);
-        const float v = (x[c] - p) * Dinv[c];
-        __syncwarp();
-        if (h == 0) x[c] = v;
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-    for (int idx = tid; idx < kSubW * kb; idx += kSubThreads) {
-      const int r = idx % kSubW, c = idx / kSubW;
-      if (r < rows) A[(r0 + r) + (int64_t)(Ks + c) * ld] = Xs[r * kSubS + c];
-    }
-  }
-}
-
 }  // namespace
 
 int tc_outer() { return kTcOuter; }
-int subpanel_max() { return kSubW; }
 int tc_max_fronts() { return kMaxTcFronts; }
 
 int64_t tc_tiles(const std::vector<int>& n, const std::vector<int>& N, int K, int w, int cend) {
@@ -746,22 +621,6 @@ cudaError_t launch_tc_pack(const int* flist, int nf, int cap, const FrontDev* fr
     k_tc_pack<2><<<grid, 128, 0, st>>>(flist, fr, F, K, w, cap, (unsigned char*)pack);
   else
     k_tc_pack<1><<<grid, 128, 0, st>>>(flist, fr, F, K, w, cap, (unsigned char*)pack);
-  g_launches++;
-  return cudaGetLastError();
-}
-
-cudaError_t launch_subpanel(const int* flist, int nf, const FrontDev* fr, float* F, int Ks, int w,
-                            DevError* err, cudaStream_t st) {
-  if (nf <= 0) return cudaSuccess;
-  if (nf > kMaxTcFronts || w <= 0 || w > kSubW) return cudaErrorInvalidValue;
-  static const int sms = []() {   // thread-safe one-time set-up
-    int dev = 0, n = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    cudaFuncSetAttribute(k_subpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSubSmem);
-    return n;
-  }();
-  k_subpanel<<<sms, kSubThreads, kSubSmem, st>>>(flist, nf, fr, F, Ks, w, err);
   g_launches++;
   return cudaGetLastError();
 }

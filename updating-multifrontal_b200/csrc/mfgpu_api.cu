@@ -341,6 +341,7 @@ struct mfgpu_handle {
   int fusedMinFronts = 148;        // fewest fronts for the one-CTA-per-front kernel
   bool subpanel = true;            // tensor-core levels: sub-panels by k_subpanel (MFGPU_SUBPANEL=0:
                                    // by the cooperative kernel)
+  int panelMaxN = 4096;            // largest front of a level factored panel by panel (0: never)
   size_t esz = sizeof(double);     // bytes per factor element
   double* d_scale = nullptr;       // s = 1/sqrt(diag(A)) of the last full factorization
   double* d_iscale = nullptr;      // 1/s
@@ -659,7 +660,8 @@ struct mfgpu_handle {
 
   // Level kernels.  The size rules choose one per level; mfgpu_autotune can
   // replace the choice for the levels of the full factorization by timing.
-  enum LevelKernel { LK_NONE = -1, LK_FUSED = 0, LK_COOP = 1, LK_TC = 2, LK_STEPPED = 3, LK_LU = 4 };
+  enum LevelKernel { LK_NONE = -1, LK_FUSED = 0, LK_COOP = 1, LK_TC = 2, LK_STEPPED = 3, LK_LU = 4,
+                     LK_PANEL = 5 };
 
   int ruleKernel(const Plan::Level& L) const {
     if (L.nf <= 0) return LK_NONE;
@@ -667,6 +669,7 @@ struct mfgpu_handle {
     if (useFused((int)L.nf, L.maxN)) return LK_FUSED;
     if (!mfgpu::coop_fits((int)L.nf) || (stepped && !mixed)) return LK_STEPPED;
     if (mixed && tcLevel(L)) return LK_TC;
+    if (panelFits(L)) return LK_PANEL;
     return LK_COOP;
   }
 
@@ -676,6 +679,14 @@ struct mfgpu_handle {
     return ruleKernel(L);
   }
 
+  // Levels of moderate fronts (up to panelMaxN) go panel by panel
+  // (k_subpanel + k_trail_syrk, no grid barriers); the cooperative kernel's
+  // 512-column outer panels keep the trailing updates of very large fronts
+  // denser.
+  bool panelFits(const Plan::Level& L) const {
+    return panelMaxN > 0 && L.maxN <= panelMaxN && L.nf <= mfgpu::kMaxPanelFronts;
+  }
+
   // Kernels that can factor level L (autotuning candidates).
   std::vector<int> levelCandidates(const Plan::Level& L) const {
     std::vector<int> c;
@@ -683,6 +694,7 @@ struct mfgpu_handle {
     if (mfgpu::small_front_fits(L.maxN, (int)esz)) c.push_back(LK_FUSED);
     if (mfgpu::coop_fits((int)L.nf) && !(stepped && !mixed)) {
       c.push_back(LK_COOP);
+      if (L.nf <= mfgpu::kMaxPanelFronts) c.push_back(LK_PANEL);
       if (mixed && L.nf <= mfgpu::tc_max_fronts() && L.maxN >= 1024) c.push_back(LK_TC);
     }
     if (c.empty()) c.push_back(ruleKernel(L));
@@ -804,6 +816,24 @@ struct mfgpu_handle {
     } else if (kind == LK_LU) {
       if (sizeof(T) != sizeof(double)) throw CudaError("LU fronts are FP64 only", MFGPU_ERR_ARG);
       runLU(P, L);
+    } else if (kind == LK_PANEL) {
+      prof.flops[MFGPU_KC_COOP] += fl;
+      runPanel<T>(P, L);
+    }
+  }
+
+  // Panel by panel (kernels_panel.cu): per W-column panel the barrier-free
+  // panel factorization, then the trailing update of every front of the level.
+  template <class T>
+  void runPanel(const Plan& P, const Plan::Level& L) {
+    const int W = mfgpu::panel_width((int)sizeof(T));
+    for (int k = 0; k < L.maxn; k += W) {
+      prof.begin(MFGPU_KC_COOP, stream);
+      ck(mfgpu::launch_subpanel<T>(P.d_ids + L.f0, (int)L.nf, d_fr, (T*)d_F, k, W, d_err, stream),
+         "launch panel factorization (k_subpanel)");
+      ck(mfgpu::launch_trail_syrk<T>(P.d_ids + L.f0, (int)L.nf, d_fr, (T*)d_F, k, W, stream),
+         "launch panel trailing update (k_trail_syrk)");
+      prof.end(stream);
     }
   }
 
@@ -1027,9 +1057,9 @@ struct mfgpu_handle {
     for (int K = 0; K < L.maxn; K += W) {
       for (int Ks = K; Ks < K + W && Ks < L.maxn; Ks += w) {
         prof.begin(MFGPU_KC_COOP, stream);
-        if (subpanel && w <= mfgpu::subpanel_max()) {
-          ck(mfgpu::launch_subpanel(P.d_ids + L.f0, (int)L.nf, d_fr, (float*)d_F, Ks, w, d_err,
-                                    stream),
+        if (subpanel && w == mfgpu::panel_width(sizeof(float)) && L.nf <= mfgpu::kMaxPanelFronts) {
+          ck(mfgpu::launch_subpanel<float>(P.d_ids + L.f0, (int)L.nf, d_fr, (float*)d_F, Ks, w,
+                                           d_err, stream),
              "launch sub-panel factorization (k_subpanel)");
         } else {
           ck(mfgpu::launch_level_coop<float>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, (float*)d_F,
@@ -1632,6 +1662,7 @@ int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const
   if (const char* e = getenv("MFGPU_TC_SUB")) h->tcSub = atoi(e);
   if (const char* e = getenv("MFGPU_GRAPHS")) h->graphs = e[0] != '0';
   if (const char* e = getenv("MFGPU_SUBPANEL")) h->subpanel = e[0] != '0';
+  if (const char* e = getenv("MFGPU_PANEL_MAX_N")) h->panelMaxN = atoi(e);
   if (h->lu) h->solveCoopMinN = 0;   // LU fronts use the per-front sweeps
   h->h_rowptr.assign(row_ptr, row_ptr + n + 1);
   h->h_colind.assign(col_ind, col_ind + h->nnz);
@@ -2843,6 +2874,7 @@ std::unique_ptr<mfgpu_handle> makeView(mfgpu_handle& B) {
   H.tcSplit3Levels = B.tcSplit3Levels;
   H.tcSplitLow = B.tcSplitLow;
   H.subpanel = B.subpanel;
+  H.panelMaxN = B.panelMaxN;
   H.tcSub = B.tcSub;
   H.fusedMinFronts = B.fusedMinFronts;
   H.d_scale = B.d_scale;

@@ -206,7 +206,7 @@ class _MFBase:
         """Restore a factorization written by save() (mfgpu_load)."""
         self._check(self._lib.mfgpu_load(self._h, os.fsencode(path)))
 
-    LEVEL_KERNELS = {-1: "none", 0: "fused", 1: "coop", 2: "tc", 3: "stepped"}
+    LEVEL_KERNELS = {-1: "none", 0: "fused", 1: "coop", 2: "tc", 3: "stepped", 4: "lu", 5: "panel"}
 
     def autotune(self, reps=2):
         """Full factorization that times each level's eligible kernels and keeps
