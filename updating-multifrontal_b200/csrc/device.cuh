@@ -148,12 +148,14 @@ cudaError_t launch_tc_pack(const int* flist, int nf, int cap, const FrontDev* fr
 // launch_subpanel turns the panel [Ks, Ks + w) of every front in flist into L
 // (w = panel_width(sizeof(T)): 64 FP64, 128 FP32; every earlier update
 // applied), launch_trail_syrk applies it to the trailing lower triangle.  At
-// most kMaxPanelFronts fronts per launch.
+// most kMaxPanelFronts fronts per launch; dslot: panel_slot_bytes(nf, sizeof(T))
+// of scratch for the factored diagonal blocks.
 constexpr int kPanelW64 = 64, kPanelW32 = 128, kMaxPanelFronts = 1024;
 int panel_width(int elem_bytes);
+size_t panel_slot_bytes(int nf, int elem_bytes);
 template <class T>
 cudaError_t launch_subpanel(const int* flist, int nf, const FrontDev* fr, T* F, int Ks, int w,
-                            DevError* err, cudaStream_t st);
+                            T* dslot, DevError* err, cudaStream_t st);
 template <class T>
 cudaError_t launch_trail_syrk(const int* flist, int nf, const FrontDev* fr, T* F, int Ks, int w,
                               cudaStream_t st);

@@ -9,7 +9,9 @@
 //                  arithmetic in every CTA), then takes 128-row blocks of the
 //                  rows below, solves them against it (X <- X L^{-T}, each
 //                  row by two threads) and writes them back; the first item
-//                  of a front writes the factored block back;
+//                  of a front leaves the factored block in a scratch slot
+//                  (the front's own copy is still being read by other CTAs),
+//                  and k_panel_diag, the next launch, puts it in place;
 //   k_trail_syrk   the trailing lower triangle, C(k1:N, k1:N) -= P P^T with
 //                  P = L(k1:N, Ks:k1), in 64 x 64 tiles (FP64: DMMA m8n8k4;
 //                  FP32: FFMA), all fronts' tiles over all SMs.
@@ -53,7 +55,7 @@ template <class T, int W>
 __global__ void __launch_bounds__(kSubThreads) k_subpanel(const int* __restrict__ flist, int nf,
                                                           const FrontDev* __restrict__ fr,
                                                           T* __restrict__ F, int Ks,
-                                                          DevError* err) {
+                                                          T* __restrict__ dslot, DevError* err) {
   constexpr int S = sub_stride<W>();
   extern __shared__ __align__(16) unsigned char sub_raw[];
   T* Ds = reinterpret_cast<T*>(sub_raw);   // diagonal block, lower, row-major stride S
@@ -121,10 +123,11 @@ __global__ void __launch_bounds__(kSubThreads) k_subpanel(const int* __restrict_
       }
     }
     const int local = item - pre[i];
-    if (local == 0) {   // the factored diagonal block back into the front
+    if (local == 0) {   // the factored diagonal block to the front's slot
+      T* slot = dslot + (int64_t)i * W * W;
       for (int idx = tid; idx < kb * kb; idx += kSubThreads) {
         const int r = idx % kb, c = idx / kb;
-        if (r >= c) A[(Ks + r) + (int64_t)(Ks + c) * ld] = Ds[r * S + c];
+        if (r >= c) slot[r + c * W] = Ds[r * S + c];
       }
       continue;
     }
@@ -159,9 +162,26 @@ __global__ void __launch_bounds__(kSubThreads) k_subpanel(const int* __restrict_
   }
 }
 
+// The factored diagonal blocks from their slots into the fronts, a CTA per front.
 template <class T, int W>
-cudaError_t launchSub(const int* flist, int nf, const FrontDev* fr, T* F, int Ks, DevError* err,
-                      cudaStream_t st) {
+__global__ void __launch_bounds__(kSubThreads) k_panel_diag(const int* __restrict__ flist,
+                                                            const FrontDev* __restrict__ fr,
+                                                            T* __restrict__ F, int Ks,
+                                                            const T* __restrict__ dslot) {
+  const FrontDev d = fr[flist[blockIdx.x]];
+  if (Ks >= d.n) return;
+  const int kb = min(W, d.n - Ks);
+  const T* slot = dslot + (int64_t)blockIdx.x * W * W;
+  T* A = F + d.off;
+  for (int idx = threadIdx.x; idx < kb * kb; idx += kSubThreads) {
+    const int r = idx % kb, c = idx / kb;
+    if (r >= c) A[(Ks + r) + (int64_t)(Ks + c) * d.ld] = slot[r + c * W];
+  }
+}
+
+template <class T, int W>
+cudaError_t launchSub(const int* flist, int nf, const FrontDev* fr, T* F, int Ks, T* dslot,
+                      DevError* err, cudaStream_t st) {
   static const int grid = []() {   // thread-safe one-time set-up: every resident CTA
     int dev = 0, n = 0, per = 0;
     cudaGetDevice(&dev);
@@ -172,8 +192,9 @@ cudaError_t launchSub(const int* flist, int nf, const FrontDev* fr, T* F, int Ks
                                                   sub_smem<T, W>());
     return n * std::max(1, per);
   }();
-  k_subpanel<T, W><<<grid, kSubThreads, sub_smem<T, W>(), st>>>(flist, nf, fr, F, Ks, err);
-  g_launches++;
+  k_subpanel<T, W><<<grid, kSubThreads, sub_smem<T, W>(), st>>>(flist, nf, fr, F, Ks, dslot, err);
+  k_panel_diag<T, W><<<nf, kSubThreads, 0, st>>>(flist, fr, F, Ks, dslot);
+  g_launches += 2;
   return cudaGetLastError();
 }
 
@@ -181,19 +202,24 @@ cudaError_t launchSub(const int* flist, int nf, const FrontDev* fr, T* F, int Ks
 
 int panel_width(int elem_bytes) { return elem_bytes == 8 ? kPanelW64 : kPanelW32; }
 
+size_t panel_slot_bytes(int nf, int elem_bytes) {
+  const size_t w = (size_t)panel_width(elem_bytes);
+  return (size_t)std::min(nf, kMaxPanelFronts) * w * w * (size_t)elem_bytes;
+}
+
 template <>
 cudaError_t launch_subpanel<float>(const int* flist, int nf, const FrontDev* fr, float* F, int Ks,
-                                   int w, DevError* err, cudaStream_t st) {
+                                   int w, float* dslot, DevError* err, cudaStream_t st) {
   if (nf <= 0) return cudaSuccess;
-  if (nf > kMaxPanelFronts || w != kPanelW32) return cudaErrorInvalidValue;
-  return launchSub<float, kPanelW32>(flist, nf, fr, F, Ks, err, st);
+  if (nf > kMaxPanelFronts || w != kPanelW32 || !dslot) return cudaErrorInvalidValue;
+  return launchSub<float, kPanelW32>(flist, nf, fr, F, Ks, dslot, err, st);
 }
 template <>
 cudaError_t launch_subpanel<double>(const int* flist, int nf, const FrontDev* fr, double* F, int Ks,
-                                    int w, DevError* err, cudaStream_t st) {
+                                    int w, double* dslot, DevError* err, cudaStream_t st) {
   if (nf <= 0) return cudaSuccess;
-  if (nf > kMaxPanelFronts || w != kPanelW64) return cudaErrorInvalidValue;
-  return launchSub<double, kPanelW64>(flist, nf, fr, F, Ks, err, st);
+  if (nf > kMaxPanelFronts || w != kPanelW64 || !dslot) return cudaErrorInvalidValue;
+  return launchSub<double, kPanelW64>(flist, nf, fr, F, Ks, dslot, err, st);
 }
 
 }  // namespace mfgpu

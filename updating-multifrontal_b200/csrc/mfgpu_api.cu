@@ -307,6 +307,7 @@ struct mfgpu_handle {
   std::map<std::tuple<const void*, const void*, int>, int> sweepSeen;
   void* d_slots = nullptr;     // diagonal-block hand-off slots of the cooperative kernel
   void* d_tcpack = nullptr;    // tensor-core panel images (mixed path)
+  void* d_pslot = nullptr;     // factored diagonal blocks of the panel-by-panel kernels
   size_t tcPackCap = 0;
   unsigned* d_gbar = nullptr;  // grid-barrier arrival counter of the cooperative kernels
   // Cooperative (flag-ordered) sweeps: per level, its forward / backward task
@@ -413,6 +414,7 @@ struct mfgpu_handle {
     cudaFree(d_err);
     cudaFree(d_slots);
     cudaFree(d_tcpack);
+    cudaFree(d_pslot);
     cudaFree(d_gbar);
     cudaFree(d_Wd);
     cudaFree(d_X);
@@ -829,7 +831,8 @@ struct mfgpu_handle {
     const int W = mfgpu::panel_width((int)sizeof(T));
     for (int k = 0; k < L.maxn; k += W) {
       prof.begin(MFGPU_KC_COOP, stream);
-      ck(mfgpu::launch_subpanel<T>(P.d_ids + L.f0, (int)L.nf, d_fr, (T*)d_F, k, W, d_err, stream),
+      ck(mfgpu::launch_subpanel<T>(P.d_ids + L.f0, (int)L.nf, d_fr, (T*)d_F, k, W, (T*)d_pslot,
+                                   d_err, stream),
          "launch panel factorization (k_subpanel)");
       ck(mfgpu::launch_trail_syrk<T>(P.d_ids + L.f0, (int)L.nf, d_fr, (T*)d_F, k, W, stream),
          "launch panel trailing update (k_trail_syrk)");
@@ -1059,7 +1062,7 @@ struct mfgpu_handle {
         prof.begin(MFGPU_KC_COOP, stream);
         if (subpanel && w == mfgpu::panel_width(sizeof(float)) && L.nf <= mfgpu::kMaxPanelFronts) {
           ck(mfgpu::launch_subpanel<float>(P.d_ids + L.f0, (int)L.nf, d_fr, (float*)d_F, Ks, w,
-                                           d_err, stream),
+                                           (float*)d_pslot, d_err, stream),
              "launch sub-panel factorization (k_subpanel)");
         } else {
           ck(mfgpu::launch_level_coop<float>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, (float*)d_F,
@@ -1773,6 +1776,12 @@ int createFrom(std::unique_ptr<Schedule> sched, int n, const int* row_ptr, const
     H.d_err = dalloc<DevError>(1, "alloc error word");
     ck(cudaMemset(H.d_err, 0, sizeof(DevError)), "clear error word");
     H.d_slots = dalloc<unsigned char>(mfgpu::coop_slot_elems() * H.esz, "alloc diagonal slots");
+    {
+      int most = 1;   // fronts of the largest level (panel launches take up to kMaxPanelFronts)
+      for (int ell = 0; ell < s.levels; ell++) most = std::max(most, s.lv[ell].nbox);
+      H.d_pslot = dalloc<unsigned char>(mfgpu::panel_slot_bytes(most, (int)H.esz),
+                                        "alloc panel diagonal slots");
+    }
     H.d_gbar = dalloc<unsigned>(1, "alloc grid barrier");
     H.d_all = dalloc<int>(all.size(), "alloc id list");
     if (H.lu) H.d_ipiv = dalloc<int>(s.dofs.size(), "alloc LU pivots");
@@ -2899,6 +2908,8 @@ std::unique_ptr<mfgpu_handle> makeView(mfgpu_handle& B) {
   ck(cudaMemsetAsync(H.d_err, 0, sizeof(DevError), H.stream), "clear error word");
   H.setLimit(B.waitLimit);   // the base's poll limit
   H.d_slots = dalloc<unsigned char>(mfgpu::coop_slot_elems() * H.esz, "alloc diagonal slots");
+  H.d_pslot = dalloc<unsigned char>(mfgpu::panel_slot_bytes(mfgpu::kMaxPanelFronts, (int)H.esz),
+                                    "alloc panel diagonal slots");
   H.d_gbar = dalloc<unsigned>(1, "alloc grid barrier");
   H.dinvElems = B.dinvElems;
   H.d_dinv_off = B.d_dinv_off;
