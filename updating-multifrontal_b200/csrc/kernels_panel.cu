@@ -48,7 +48,83 @@ constexpr int sub_stride() { return W + 1; }
 
 template <class T, int W>
 constexpr size_t sub_smem() {
-  return (size_t)(W + kSubRows) * sub_stride<W>() * sizeof(T) + W * sizeof(T);
+  return ((size_t)(W + kSubRows) * sub_stride<W>() + (size_t)(W / 32) * 32 * 33) * sizeof(T);
+}
+
+// One warp factors the 32 x 32 (jb x jb) diagonal block at (j0, j0) of Ds in
+// place (lane i holds row i in registers; Cholesky by shuffles) and writes the
+// inverse of the factor to Li (row-major, stride 33).  Returns the first
+// non-positive pivot column of the block or -1.
+template <class T, int S>
+__device__ int warp_chol_inv(T* Ds, int j0, int jb, T* Li) {
+  const int lane = threadIdx.x & 31;
+  T row[32];
+#pragma unroll
+  for (int t = 0; t < 32; t++)
+    row[t] = (lane < jb && t <= lane) ? Ds[(j0 + lane) * S + j0 + t] : T(0);
+  int bad = -1;
+#pragma unroll
+  for (int j = 0; j < 32; j++) {
+    if (j < jb) {
+      T djj = __shfl_sync(0xffffffffu, row[j], j);
+      if (!(djj > T(0))) {                 // non-positive or NaN pivot: not SPD
+        if (bad < 0) bad = j;
+        djj = T(1);
+      }
+      const T r = rsq<T>(djj);
+      if (lane == j) row[j] = djj * r;
+      else if (lane > j) row[j] = row[j] * r;
+#pragma unroll
+      for (int l = j + 1; l < 32; l++) {
+        const T llj = __shfl_sync(0xffffffffu, row[j], l);
+        if (lane >= l && l < jb) row[l] -= row[j] * llj;
+      }
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 32; t++)
+    if (lane < jb && t <= lane) Ds[(j0 + lane) * S + j0 + t] = row[t];
+  __syncwarp();
+  // lane c: column c of the inverse, x_i = (delta_ic - sum_{c<=t<i} L(i,t) x_t) / L(i,i)
+  T x[32];
+#pragma unroll
+  for (int i = 0; i < 32; i++) {
+    T v = T(0);
+    if (i < jb && i >= lane) {
+      T acc = i == lane ? T(1) : T(0);
+#pragma unroll
+      for (int t = 0; t < i; t++)
+        if (t >= lane) acc -= Ds[(j0 + i) * S + j0 + t] * x[t];
+      v = acc / Ds[(j0 + i) * S + j0 + i];
+    }
+    x[i] = v;
+    Li[i * 33 + lane] = v;
+  }
+  __syncwarp();
+  return bad;
+}
+
+// Row `r` of block b of a panel held row-major in P (stride S), by one warp
+// (lane c = column 32 b + c): left-looking against the factored columns
+// before the block (Lc: the factor, row-major stride S), then the block
+// solve with the block inverse Li.  Rows of several warps run independently.
+template <class T, int S>
+__device__ __forceinline__ void warp_row_block(T* P, int r, int b, int jb, const T* Lc,
+                                               const T* Li) {
+  const int lane = threadIdx.x & 31, c0 = 32 * b;
+  T* pr = P + r * S;
+  T acc = lane < jb ? pr[c0 + lane] : T(0);
+  const T* lrow = Lc + (c0 + lane) * S;
+  if (lane < jb)
+    for (int t = 0; t < c0; t++) acc -= pr[t] * lrow[t];
+  T y = T(0);
+#pragma unroll
+  for (int t = 0; t < 32; t++) {
+    const T at = __shfl_sync(0xffffffffu, acc, t);
+    if (t <= lane && t < jb) y += at * Li[lane * 33 + t];
+  }
+  __syncwarp();
+  if (lane < jb) pr[c0 + lane] = y;
 }
 
 template <class T, int W>
@@ -58,11 +134,12 @@ __global__ void __launch_bounds__(kSubThreads) k_subpanel(const int* __restrict_
                                                           T* __restrict__ dslot, DevError* err) {
   constexpr int S = sub_stride<W>();
   extern __shared__ __align__(16) unsigned char sub_raw[];
-  T* Ds = reinterpret_cast<T*>(sub_raw);   // diagonal block, lower, row-major stride S
+  T* Ds = reinterpret_cast<T*>(sub_raw);   // diagonal block -> its factor, row-major stride S
   T* Xs = Ds + W * S;                      // a 128-row block of the panel
-  T* Dinv = Xs + kSubRows * S;             // 1 / L(c, c)
+  T* Lib = Xs + kSubRows * S;              // inverses of the 32 x 32 diagonal blocks, 32 x 33 each
   __shared__ int pre[kMaxPanelFronts + 1];
-  const int tid = threadIdx.x;
+  __shared__ int badcol;
+  const int tid = threadIdx.x, warp = tid >> 5, nwarp = kSubThreads / 32;
   // items per front (in parallel), then their prefix (thread 0, shared memory)
   for (int i = tid; i < nf; i += kSubThreads) {
     const FrontDev d = fr[flist[i]];
@@ -87,39 +164,45 @@ __global__ void __launch_bounds__(kSubThreads) k_subpanel(const int* __restrict_
     const FrontDev d = fr[f];
     T* A = F + d.off;
     const int64_t ld = d.ld;
-    const int kb = min(W, d.n - Ks);
+    const int kb = min(W, d.n - Ks), nb = (kb + 31) / 32;
     if (i != cur) {
-      // load and factor the diagonal block
+      // load the diagonal block and factor it, 32 columns at a time, left-looking
       cur = i;
       __syncthreads();
       for (int idx = tid; idx < kb * kb; idx += kSubThreads) {
         const int r = idx % kb, c = idx / kb;
         Ds[r * S + c] = r >= c ? A[(Ks + r) + (int64_t)(Ks + c) * ld] : T(0);
       }
+      if (tid == 0) badcol = -1;
       __syncthreads();
-      for (int j = 0; j < kb; j++) {
-        T dj = Ds[j * S + j];
-        if (!(dj > T(0))) {                 // non-positive or NaN pivot: not SPD
-          if (tid == 0 && atomicCAS(&err->code, 0, 1) == 0) {
-            err->front = f;
-            err->col = Ks + j;
+      for (int b = 0; b < nb; b++) {
+        const int c0 = 32 * b, jb = min(32, kb - c0);
+        // block b's diagonal block less the earlier columns' contributions
+        if (b > 0)
+          for (int r = c0 + warp; r < c0 + jb; r += nwarp) {
+            const int lane = tid & 31;
+            if (lane < jb && lane <= r - c0) {
+              T acc = Ds[r * S + c0 + lane];
+              const T* lr = Ds + r * S;
+              const T* lc = Ds + (c0 + lane) * S;
+              for (int t = 0; t < c0; t++) acc -= lr[t] * lc[t];
+              Ds[r * S + c0 + lane] = acc;
+            }
           }
-          dj = T(1);
-        }
-        const T r = rsq<T>(dj);
-        __syncthreads();                    // every thread has read L(j, j)
-        if (tid == 0) {
-          Ds[j * S + j] = dj * r;
-          Dinv[j] = r;
-        }
-        for (int q = j + 1 + tid; q < kb; q += kSubThreads) Ds[q * S + j] *= r;
         __syncthreads();
-        const int m = kb - j - 1;
-        for (int idx = tid; idx < m * m; idx += kSubThreads) {
-          const int q = j + 1 + idx % m, c = j + 1 + idx / m;
-          if (c <= q) Ds[q * S + c] -= Ds[q * S + j] * Ds[c * S + j];
+        if (warp == 0) {
+          const int bad = warp_chol_inv<T, S>(Ds, c0, jb, Lib + b * 32 * 33);
+          if ((tid & 31) == 0 && bad >= 0 && badcol < 0) badcol = Ks + c0 + bad;
         }
-        __syncthreads();                    // the next pivot is final
+        __syncthreads();
+        // the rows of the diagonal block below block b
+        for (int r = c0 + jb + warp; r < kb; r += nwarp)
+          warp_row_block<T, S>(Ds, r, b, jb, Ds, Lib + b * 32 * 33);
+        __syncthreads();
+      }
+      if (tid == 0 && badcol >= 0 && atomicCAS(&err->code, 0, 1) == 0) {
+        err->front = f;
+        err->col = badcol;
       }
     }
     const int local = item - pre[i];
@@ -138,22 +221,10 @@ __global__ void __launch_bounds__(kSubThreads) k_subpanel(const int* __restrict_
       Xs[r * S + c] = r < rows ? A[(r0 + r) + (int64_t)(Ks + c) * ld] : T(0);
     }
     __syncthreads();
-    {
-      // row r by the thread pair (2r, 2r + 1), adjacent lanes: each sums every
-      // other earlier column, the pair combines, both keep the solved value
-      const int r = tid >> 1, h = tid & 1;
-      T* x = Xs + r * S;
-      for (int c = 0; c < kb; c++) {
-        const T* lc = Ds + c * S;
-        T p = T(0);
-        for (int t = h; t < c; t += 2) p = fma(x[t], lc[t], p);
-        p += __shfl_xor_sync(0xffffffffu, p, 1);
-        const T v = (x[c] - p) * Dinv[c];
-        __syncwarp();
-        if (h == 0) x[c] = v;
-        __syncwarp();
-      }
-    }
+    // X <- X L^{-T}: each row by one warp, block by block, no block barrier
+    for (int r = warp; r < rows; r += nwarp)
+      for (int b = 0; b < nb; b++)
+        warp_row_block<T, S>(Xs, r, b, min(32, kb - 32 * b), Ds, Lib + b * 32 * 33);
     __syncthreads();
     for (int idx = tid; idx < kSubRows * kb; idx += kSubThreads) {
       const int r = idx % kSubRows, c = idx / kSubRows;
