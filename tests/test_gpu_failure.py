@@ -31,8 +31,9 @@ def prob():
     return A, b, x
 
 
-def test_barrier_timeout_in_factor_then_recovers(prob):
+def test_barrier_timeout_in_factor_then_recovers(prob, monkeypatch):
     A, b, x = prob
+    monkeypatch.setenv("MFGPU_PANEL_MAX_N", "0")   # levels on the cooperative (grid-barrier) kernel
     F = MF2D(A, N[0], N[1], 1, 4)
     F.set_wait_limit(1)
     with pytest.raises(MFError) as e:

@@ -126,8 +126,14 @@ __device__ __forceinline__ T ldcg(const T* p) {
 // column blocks j before it as their ready flags come up, then a pivot block
 // forms y_R = Dinv_R (b_R - acc), writes it to X and to the front's second
 // workspace half (Y) and raises its flag; a boundary block leaves -acc in W
-// for the separator gather.  A task waits only on tasks listed before it, and
-// a cooperative launch keeps every CTA resident, so the sweep cannot stall.
+// for the separator gather.  Everything the last dependency does not change -
+// its L block, the block's row of the inverse, the right-hand side - is in
+// registers before the task waits for it, so a step of the chain of dependent
+// blocks costs one small load, a product and two four-lane reductions.  The
+// four lanes of a row (tid & 3) split its 64 columns; a warp's loads of one
+// column offset still cover whole 32-byte sectors.  A task waits only on
+// tasks listed before it, and a cooperative launch keeps every CTA resident,
+// so the sweep cannot stall.
 template <class T, int NR>
 __global__ void __launch_bounds__(SCT) k_solve_flow_fwd(const int* __restrict__ flist,
                                                         const FrontDev* __restrict__ fr,
@@ -141,9 +147,9 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_fwd(const int* __restrict__ 
                                                         const int* __restrict__ flagoff, int* flags,
                                                         DevError* err) {
   constexpr int CH = 4;                       // column blocks per shared-memory round
-  __shared__ T ys[CH * SB][NR + 1];           // solved blocks; reused for the reduction
-  __shared__ T ws[SB][NR + 1];
-  const int tid = threadIdx.x, rl = tid & (SB - 1), g = tid >> 6;   // row, column group
+  __shared__ T ys[CH * SB][NR + 1];           // solved blocks
+  __shared__ T ws[SB][NR + 1];                // b_R - acc of the block
+  const int tid = threadIdx.x, rl = tid >> 2, g = tid & 3;   // row, column quarter
   for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
     const int2 tk = tasks[t];
     const int i = tk.x, R = tk.y, f = flist[i];
@@ -157,12 +163,15 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_fwd(const int* __restrict__ 
     const bool piv = R < nb;
     const int row0 = piv ? R * SB : d.n + (R - nb) * SB;
     const int rows = min(SB, (piv ? d.n : d.N) - row0);
+    const bool live = rl < rows;
     const int jmax = piv ? R : nb;
+    const T* Ar = A + row0 + rl;
     T acc[NR];
 #pragma unroll
     for (int c = 0; c < NR; c++) acc[c] = T(0);
-    for (int j0 = 0; j0 < jmax; j0 += CH) {
-      const int jc = min(CH, jmax - j0);
+    // every block but the last, CH at a time as their flags come up
+    for (int j0 = 0; j0 < jmax - 1; j0 += CH) {
+      const int jc = min(CH, jmax - 1 - j0);
       __syncthreads();                        // ys of the previous round is consumed
       if (tid == 0)
         for (int jj = 0; jj < jc; jj++) flow_wait(fl + j0 + jj, err);
@@ -173,8 +182,7 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_fwd(const int* __restrict__ 
         ys[r][c] = col < d.n ? ldcg(Y + col + (int64_t)c * d.N) : T(0);
       }
       __syncthreads();
-      if (rl < rows) {
-        const T* Ar = A + row0 + rl;
+      if (live) {
         for (int jj = 0; jj < jc; jj++) {
           const int cb = (j0 + jj) * SB + 16 * g;
           T l[16];
@@ -187,33 +195,73 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_fwd(const int* __restrict__ 
         }
       }
     }
-    // sum the four column groups' partials
-    __syncthreads();
+    // before the last wait: that block's L values, this row's quarter of
+    // Dinv_R (lower triangular, column-major) and the right-hand side
+    T ll[16], dv[16], w[NR];
+    const int cl = (jmax - 1) * SB + 16 * g;
 #pragma unroll
-    for (int c = 0; c < NR; c++) ys[g * SB + rl][c] = acc[c];
-    __syncthreads();
-    for (int idx = tid; idx < SB * nrhs; idx += SCT) {
-      const int r = idx % SB, c = idx / SB;
-      const T s = (ys[r][c] + ys[SB + r][c]) + (ys[2 * SB + r][c] + ys[3 * SB + r][c]);
-      if (r < rows) {
-        if (piv) ws[r][c] = X[dl[row0 + r] + (int64_t)c * ldx] - s;
-        else W[row0 + r + (int64_t)c * d.N] = -s;
-      } else if (piv) {
-        ws[r][c] = T(0);
+    for (int q = 0; q < 16; q++)
+      ll[q] = (jmax > 0 && live && cl + q < d.n) ? Ar[(int64_t)(cl + q) * d.ld] : T(0);
+    if (piv) {
+      const T* D = Dv + dinv_off[f] + (int64_t)R * 2 * SB * SB;
+#pragma unroll
+      for (int q = 0; q < 16; q++) dv[q] = 16 * g + q <= rl ? D[rl + (16 * g + q) * SB] : T(0);
+#pragma unroll
+      for (int c = 0; c < NR; c++)
+        w[c] = (live && g == 0 && c < nrhs) ? X[dl[row0 + rl] + (int64_t)c * ldx] : T(0);
+    }
+    if (jmax > 0) {
+      __syncthreads();                        // ys of the previous round is consumed
+      if (tid == 0) flow_wait(fl + jmax - 1, err);
+      __syncthreads();
+      for (int idx = tid; idx < SB * nrhs; idx += SCT) {
+        const int r = idx % SB, c = idx / SB;
+        const int col = (jmax - 1) * SB + r;
+        ys[r][c] = col < d.n ? ldcg(Y + col + (int64_t)c * d.N) : T(0);
       }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < 16; q++)
+#pragma unroll
+        for (int c = 0; c < NR; c++) acc[c] = fma(ll[q], ys[16 * g + q][c], acc[c]);
     }
-    if (!piv) continue;
+    // sum the four quarters of the row
+#pragma unroll
+    for (int c = 0; c < NR; c++) {
+      acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 1);
+      acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 2);
+    }
+    if (!piv) {
+      if (live && g == 0)
+#pragma unroll
+        for (int c = 0; c < NR; c++)
+          if (c < nrhs) W[row0 + rl + (int64_t)c * d.N] = -acc[c];
+      continue;
+    }
+    if (g == 0)
+#pragma unroll
+      for (int c = 0; c < NR; c++) ws[rl][c] = live ? w[c] - acc[c] : T(0);
     __syncthreads();
-    // y_R = Dinv_R w_R (lower 64 x 64, column-major)
-    const T* D = Dv + dinv_off[f] + (int64_t)R * 2 * SB * SB;
-    for (int idx = tid; idx < SB * nrhs; idx += SCT) {
-      const int r = idx % SB, c = idx / SB;
-      if (r >= rows) continue;
-      T y = T(0);
-      for (int q = 0; q <= r; q++) y = fma(D[r + q * SB], ws[q][c], y);
-      Y[row0 + r + (int64_t)c * d.N] = y;
-      X[dl[row0 + r] + (int64_t)c * ldx] = y;
+    // y_R = Dinv_R w_R: each lane its quarter, then the four-lane sum
+    T y[NR];
+#pragma unroll
+    for (int c = 0; c < NR; c++) y[c] = T(0);
+#pragma unroll
+    for (int q = 0; q < 16; q++)
+#pragma unroll
+      for (int c = 0; c < NR; c++) y[c] = fma(dv[q], ws[16 * g + q][c], y[c]);
+#pragma unroll
+    for (int c = 0; c < NR; c++) {
+      y[c] += __shfl_xor_sync(0xffffffffu, y[c], 1);
+      y[c] += __shfl_xor_sync(0xffffffffu, y[c], 2);
     }
+    if (live && g == 0)
+#pragma unroll
+      for (int c = 0; c < NR; c++)
+        if (c < nrhs) {
+          Y[row0 + rl + (int64_t)c * d.N] = y[c];
+          X[dl[row0 + rl] + (int64_t)c * ldx] = y[c];
+        }
     __syncthreads();
     if (tid == 0) flow_publish(flags + flagoff[i] + R);
   }
@@ -223,8 +271,11 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_fwd(const int* __restrict__ 
 // (y - L21^T x_bd).  Task (i, j), pivot column block j of front i, listed by
 // distance from the front's last block: r = sum over the rows below block j of
 // L(r, block j)^T x_r, the boundary rows first (x_bd is final on entry), then
-// the solved pivot blocks from the last one down as their flags come up; then
-// x_j = Dinv_j^T (y_j - r) to X and Y and the flag.
+// the solved pivot blocks from the last one down as their flags come up (the
+// nearest block, the last dependency, with its L values, this column's
+// quarter of Dinv_j^T and y_j in registers before the wait); then
+// x_j = Dinv_j^T (y_j - r) to X and Y and the flag.  The four lanes of a
+// column (tid & 3) split the rows.
 template <class T, int NR>
 __global__ void __launch_bounds__(SCT) k_solve_flow_bwd(const int* __restrict__ flist,
                                                         const FrontDev* __restrict__ fr,
@@ -238,7 +289,7 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_bwd(const int* __restrict__ 
                                                         const int* __restrict__ flagoff, int* flags,
                                                         DevError* err) {
   __shared__ T xs[SB][NR + 1];
-  __shared__ T vj[SB][NR + 1];
+  __shared__ T vs[SB][NR + 1];
   const int tid = threadIdx.x, cl = tid >> 2, q = tid & 3;   // column of the block, row quarter
   for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
     const int2 tk = tasks[t];
@@ -250,13 +301,14 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_bwd(const int* __restrict__ 
     const int* dl = dofs + d.dof_off;
     const int* fl = flags + flagoff[i];
     const int nb = cdiv(d.n, SB), col0 = j * SB, kbj = min(SB, d.n - col0);
+    const bool live = cl < kbj;
     const T* Lc = A + (int64_t)(col0 + cl) * d.ld;
     T acc[NR];
 #pragma unroll
     for (int c = 0; c < NR; c++) acc[c] = T(0);
     // rows [r0, r0 + nr) against xs: lanes (cl, q) take rows 16 q .. 16 q + 15
     auto chunk = [&](int r0, int nr) {
-      if (cl >= kbj) return;
+      if (!live) return;
 #pragma unroll 4
       for (int rr = 0; rr < 16; rr++) {
         const int r = 16 * q + rr;
@@ -277,7 +329,7 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_bwd(const int* __restrict__ 
       __syncthreads();
       chunk(r0, nr);
     }
-    for (int R = nb - 1; R > j; R--) {                  // solved pivot blocks below
+    for (int R = nb - 1; R > j + 1; R--) {              // solved pivot blocks below but the nearest
       const int r0 = R * SB, nr = min(SB, d.n - r0);
       __syncthreads();
       if (tid == 0) flow_wait(fl + R, err);
@@ -289,27 +341,65 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_bwd(const int* __restrict__ 
       __syncthreads();
       chunk(r0, nr);
     }
+    // before the last wait: block j + 1's L values, this column's quarter of
+    // Dinv_j^T (upper triangular, column-major) and y_j
+    const int rn = (j + 1) * SB, nn = j + 1 < nb ? min(SB, d.n - rn) : 0;
+    T ln[16], dt[16], v[NR];
+#pragma unroll
+    for (int rr = 0; rr < 16; rr++)
+      ln[rr] = (live && 16 * q + rr < nn) ? Lc[rn + 16 * q + rr] : T(0);
+    {
+      const T* D = Dv + dinv_off[f] + (int64_t)j * 2 * SB * SB + SB * SB;
+#pragma unroll
+      for (int p = 0; p < 16; p++) dt[p] = 16 * q + p >= cl ? D[cl + (16 * q + p) * SB] : T(0);
+#pragma unroll
+      for (int c = 0; c < NR; c++)
+        v[c] = (live && q == 0 && c < nrhs) ? X[dl[col0 + cl] + (int64_t)c * ldx] : T(0);
+    }
+    if (nn > 0) {
+      __syncthreads();                        // xs of the previous round is consumed
+      if (tid == 0) flow_wait(fl + j + 1, err);
+      __syncthreads();
+      for (int idx = tid; idx < SB * nrhs; idx += SCT) {
+        const int r = idx % SB, c = idx / SB;
+        xs[r][c] = r < nn ? ldcg(Y + rn + r + (int64_t)c * d.N) : T(0);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int rr = 0; rr < 16; rr++)
+#pragma unroll
+        for (int c = 0; c < NR; c++) acc[c] = fma(ln[rr], xs[16 * q + rr][c], acc[c]);
+    }
 #pragma unroll
     for (int c = 0; c < NR; c++) {
       acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 1);
       acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 2);
     }
-    __syncthreads();
+    __syncthreads();                          // vs of the previous task is consumed
     if (q == 0)
 #pragma unroll
-      for (int c = 0; c < NR; c++)
-        if (c < nrhs) vj[cl][c] = cl < kbj ? X[dl[col0 + cl] + (int64_t)c * ldx] - acc[c] : T(0);
+      for (int c = 0; c < NR; c++) vs[cl][c] = live ? v[c] - acc[c] : T(0);
     __syncthreads();
-    // x_j = Dinv_j^T v (upper 64 x 64, column-major, right after Dinv_j)
-    const T* DT = Dv + dinv_off[f] + (int64_t)j * 2 * SB * SB + SB * SB;
-    for (int idx = tid; idx < SB * nrhs; idx += SCT) {
-      const int r = idx % SB, c = idx / SB;
-      if (r >= kbj) continue;
-      T x = T(0);
-      for (int p = r; p < kbj; p++) x = fma(DT[r + p * SB], vj[p][c], x);
-      Y[col0 + r + (int64_t)c * d.N] = x;
-      X[dl[col0 + r] + (int64_t)c * ldx] = x;
+    // x_j = Dinv_j^T v: each lane its quarter, then the four-lane sum
+    T x[NR];
+#pragma unroll
+    for (int c = 0; c < NR; c++) x[c] = T(0);
+#pragma unroll
+    for (int p = 0; p < 16; p++)
+#pragma unroll
+      for (int c = 0; c < NR; c++) x[c] = fma(dt[p], vs[16 * q + p][c], x[c]);
+#pragma unroll
+    for (int c = 0; c < NR; c++) {
+      x[c] += __shfl_xor_sync(0xffffffffu, x[c], 1);
+      x[c] += __shfl_xor_sync(0xffffffffu, x[c], 2);
     }
+    if (live && q == 0)
+#pragma unroll
+      for (int c = 0; c < NR; c++)
+        if (c < nrhs) {
+          Y[col0 + cl + (int64_t)c * d.N] = x[c];
+          X[dl[col0 + cl] + (int64_t)c * ldx] = x[c];
+        }
     __syncthreads();
     if (tid == 0) flow_publish(flags + flagoff[i] + j);
   }

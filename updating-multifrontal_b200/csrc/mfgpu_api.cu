@@ -340,9 +340,10 @@ struct mfgpu_handle {
   int tcSub = 128;                 // mixed: sub-panel width inside each 512-column outer panel of a
                                    // tensor-core level (0 or 512: no sub-panels)
   int fusedMinFronts = 148;        // fewest fronts for the one-CTA-per-front kernel
-  bool subpanel = true;            // tensor-core levels: sub-panels by k_subpanel (MFGPU_SUBPANEL=0:
-                                   // by the cooperative kernel)
-  int panelMaxN = 4096;            // largest front of a level factored panel by panel (0: never)
+  bool subpanel = false;           // tensor-core levels: sub-panels by k_subpanel (MFGPU_SUBPANEL=1)
+                                   // instead of the cooperative kernel, which measures faster
+  int panelMaxN = 0;               // largest front of a level factored panel by panel (0: never;
+                                   // MFGPU_PANEL_MAX_N; the autotuner may still pick the kernel)
   size_t esz = sizeof(double);     // bytes per factor element
   double* d_scale = nullptr;       // s = 1/sqrt(diag(A)) of the last full factorization
   double* d_iscale = nullptr;      // 1/s
