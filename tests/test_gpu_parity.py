@@ -170,10 +170,10 @@ def test_cooperative_sweeps_vs_oracle(dim, N, ms, nrhs, env_var):
                                       (3, (13, 17, 11), 3)])
 @pytest.mark.parametrize("kernel", ["panel", "coop"])
 def test_level_kernels_vs_oracle(dim, N, ms, kernel, env_var):
-    """Levels of moderate fronts factored panel by panel (k_subpanel +
-    k_trail_syrk, the default up to 4096 unknowns) or by the cooperative
-    kernel (MFGPU_PANEL_MAX_N=0): both within 1e-12 of the oracle, before and
-    after a localized update."""
+    """Levels of moderate fronts factored panel by panel (k_diag_factor +
+    k_panel_trsm + k_trail_syrk, MFGPU_PANEL_MAX_N=4096) or by the cooperative
+    kernel (the default): both within 1e-12 of the oracle, before and after a
+    localized update."""
     env_var("MFGPU_PANEL_MAX_N", 4096 if kernel == "panel" else 0)
     a, A, b = problem(dim, N, seed=17, nrhs=2)
     F = make(dim, N, A, ms)

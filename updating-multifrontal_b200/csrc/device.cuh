@@ -149,7 +149,7 @@ cudaError_t launch_tc_pack(const int* flist, int nf, int cap, const FrontDev* fr
 // (w = panel_width(sizeof(T)): 64 FP64, 128 FP32; every earlier update
 // applied), launch_trail_syrk applies it to the trailing lower triangle.  At
 // most kMaxPanelFronts fronts per launch; dslot: panel_slot_bytes(nf, sizeof(T))
-// of scratch for the factored diagonal blocks.
+// of scratch for the inverses of the factored diagonal blocks.
 constexpr int kPanelW64 = 64, kPanelW32 = 128, kMaxPanelFronts = 1024;
 int panel_width(int elem_bytes);
 size_t panel_slot_bytes(int nf, int elem_bytes);

@@ -340,7 +340,7 @@ struct mfgpu_handle {
   int tcSub = 128;                 // mixed: sub-panel width inside each 512-column outer panel of a
                                    // tensor-core level (0 or 512: no sub-panels)
   int fusedMinFronts = 148;        // fewest fronts for the one-CTA-per-front kernel
-  bool subpanel = false;           // tensor-core levels: sub-panels by k_subpanel (MFGPU_SUBPANEL=1)
+  bool subpanel = false;           // tensor-core levels: sub-panels by k_diag_factor + k_panel_trsm (MFGPU_SUBPANEL=1)
                                    // instead of the cooperative kernel, which measures faster
   int panelMaxN = 0;               // largest front of a level factored panel by panel (0: never;
                                    // MFGPU_PANEL_MAX_N; the autotuner may still pick the kernel)
@@ -683,7 +683,7 @@ struct mfgpu_handle {
   }
 
   // Levels of moderate fronts (up to panelMaxN) go panel by panel
-  // (k_subpanel + k_trail_syrk, no grid barriers); the cooperative kernel's
+  // (k_diag_factor + k_panel_trsm + k_trail_syrk, no grid barriers); the cooperative kernel's
   // 512-column outer panels keep the trailing updates of very large fronts
   // denser.
   bool panelFits(const Plan::Level& L) const {
@@ -834,7 +834,7 @@ struct mfgpu_handle {
       prof.begin(MFGPU_KC_COOP, stream);
       ck(mfgpu::launch_subpanel<T>(P.d_ids + L.f0, (int)L.nf, d_fr, (T*)d_F, k, W, (T*)d_pslot,
                                    d_err, stream),
-         "launch panel factorization (k_subpanel)");
+         "launch panel factorization (k_diag_factor, k_panel_trsm)");
       ck(mfgpu::launch_trail_syrk<T>(P.d_ids + L.f0, (int)L.nf, d_fr, (T*)d_F, k, W, stream),
          "launch panel trailing update (k_trail_syrk)");
       prof.end(stream);
@@ -1064,7 +1064,7 @@ struct mfgpu_handle {
         if (subpanel && w == mfgpu::panel_width(sizeof(float)) && L.nf <= mfgpu::kMaxPanelFronts) {
           ck(mfgpu::launch_subpanel<float>(P.d_ids + L.f0, (int)L.nf, d_fr, (float*)d_F, Ks, w,
                                            (float*)d_pslot, d_err, stream),
-             "launch sub-panel factorization (k_subpanel)");
+             "launch sub-panel factorization (k_diag_factor, k_panel_trsm)");
         } else {
           ck(mfgpu::launch_level_coop<float>(P.d_ids + L.f0, (int)L.nf, L.maxn, d_fr, (float*)d_F,
                                              d_err, (float*)d_slots, P.d_cpref + L.cpref0, d_gbar,
