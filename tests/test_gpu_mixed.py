@@ -39,15 +39,15 @@ def relres(A, x, b):
 @pytest.fixture(params=["default", "tensor-core levels", "tensor-core sub-panels", "panel levels"])
 def tc_mode(request, monkeypatch):
     """'tensor-core levels' sends every level with a front of 512 or more onto
-    the tcgen05 trailing update (three-term TF32); 'tensor-core sub-panels'
-    also factors their 128-column sub-panels with k_diag_factor +
-    k_panel_trsm instead of the cooperative kernel; 'panel levels' factors
-    every level of fronts up to 4096 panel by panel (k_diag_factor +
-    k_panel_trsm + k_trail_syrk)."""
+    the tcgen05 trailing update (three-term TF32) with their 128-column
+    sub-panels factored by the cooperative kernel; 'tensor-core sub-panels'
+    the same with the sub-panels by k_diag_factor + k_panel_trsm (the
+    default); 'panel levels' factors every level of fronts up to 4096 panel
+    by panel (k_diag_factor + k_panel_trsm + k_trail_syrk)."""
     if request.param.startswith("tensor-core"):
         monkeypatch.setenv("MFGPU_TC_MIN_N", "512")
-    if request.param == "tensor-core sub-panels":
-        monkeypatch.setenv("MFGPU_SUBPANEL", "1")
+    if request.param == "tensor-core levels":
+        monkeypatch.setenv("MFGPU_SUBPANEL", "0")
     if request.param == "panel levels":
         monkeypatch.setenv("MFGPU_PANEL_MAX_N", "4096")
     return request.param

@@ -7,15 +7,16 @@
 // already applied) becomes L in two launches:
 //   k_diag_factor  one CTA per front factors the kb x kb diagonal block in
 //                  shared memory, 32 columns at a time (a warp's register
-//                  Cholesky of the 32 x 32 block with its inverse, the rows
-//                  below it by that inverse, the rest of the block by 4 x 4
-//                  register tiles), writes L11 back and leaves the inverse of
-//                  L11 in the front's scratch slot, K-major;
-//   k_panel_trsm   the rows below the block, L21 = A21 L11^{-T}, as one
-//                  product with that inverse: 128-row items over a persistent
-//                  grid, each CTA a 128 x W tile of A21 and the inverse in
-//                  shared memory (K-major, 16-byte vector loads), 8 x (W/16)
-//                  outputs per thread in registers.
+//                  Cholesky of the 32 x 32 block, the rows below it by
+//                  substitution, the rest of the block by 4 x 4 register
+//                  tiles, the block inverses off the critical path), writes
+//                  L11 back and leaves the inverses of its 32 x 32 diagonal
+//                  blocks in the front's scratch slot;
+//   k_panel_trsm   the rows below the block, L21 = A21 L11^{-T}, by blocked
+//                  substitution with L11 and those inverses: 128-row items
+//                  over a persistent grid, 16 outputs per thread in
+//                  registers, the next tile already on its way (cp.async
+//                  into a second buffer).
 // The trailing update then follows (k_trail_syrk here, the tensor-core update
 // on the mixed path's large levels).  The diagonal block is the only serial
 // part and it is factored once, by one CTA; the panel below is plain
@@ -34,6 +35,11 @@ namespace {
 
 constexpr int kPanThreads = 256;
 constexpr int kTrsmRows = 128;            // rows per k_panel_trsm item
+
+// Scratch of warp_chol_inv in shared memory (16-byte aligned): the factor
+// transposed, LT[t * 36 + i] = L(i, t), then the current column.
+constexpr int kLT = 36;
+constexpr int kCholScratch = 32 * kLT + 32;
 
 template <class T>
 __device__ __forceinline__ T rsq(T x);
@@ -56,11 +62,12 @@ constexpr int ls_stride() { return W + vpad<T>(); }
 
 template <class T, int W>
 constexpr size_t diag_smem() {
-  return (size_t)2 * W * diag_stride<W>() * sizeof(T);
+  return ((size_t)2 * W * diag_stride<W>() + kCholScratch) * sizeof(T);
 }
 template <class T, int W>
 constexpr size_t trsm_smem() {
-  return ((size_t)W * xs_stride<T>() + (size_t)W * ls_stride<T, W>()) * sizeof(T);
+  return ((size_t)2 * W * xs_stride<T>() + (size_t)W * ls_stride<T, W>() + (size_t)W * 32) *
+         sizeof(T);
 }
 
 // Four consecutive values from 16-byte aligned shared memory.
@@ -74,14 +81,36 @@ __device__ __forceinline__ void ld4(const double* p, double v[4]) {
   v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 
+// One element global -> shared without a register round trip (cp.async, so
+// that a thread has dozens of loads in flight); zero-filled when !take.
+__device__ __forceinline__ void cp_elem(float* dst, const float* src, bool take) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(take ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_elem(double* dst, const double* src, bool take) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(take ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // One warp factors the jb x jb (jb <= 32) diagonal block at (j0, j0) of Ds
-// (row-major, stride S) in place - lane i holds row i in registers, the
-// columns are eliminated by shuffles - and writes the inverse of the factor
-// to Li (row-major, stride LS; zero above the diagonal and outside jb).
+// (row-major, stride S) in place: lane i holds row i in registers; each
+// scaled column goes through shared memory once and comes back four values
+// per load.  Leaves the factor transposed in Wk (LT[t * 36 + i] = L(i, t)).
 // Returns the first non-positive pivot column of the block, or -1.
-template <class T, int S, int LS>
-__device__ int warp_chol_inv(T* Ds, int j0, int jb, T* Li) {
+template <class T, int S>
+__device__ int warp_chol(T* Ds, int j0, int jb, T* Wk) {
   const int lane = threadIdx.x & 31;
+  T* LT = Wk;
+  T* cb = Wk + 32 * kLT;
   T row[32];
 #pragma unroll
   for (int t = 0; t < 32; t++)
@@ -98,53 +127,123 @@ __device__ int warp_chol_inv(T* Ds, int j0, int jb, T* Li) {
       const T r = rsq<T>(djj);
       if (lane == j) row[j] = djj * r;
       else if (lane > j) row[j] = row[j] * r;
+      cb[lane] = row[j];                   // L(lane, j)
+      __syncwarp();
 #pragma unroll
-      for (int l = j + 1; l < 32; l++) {
-        const T llj = __shfl_sync(0xffffffffu, row[j], l);
-        if (lane >= l && l < jb) row[l] -= row[j] * llj;
+      for (int l4 = 0; l4 < 32; l4 += 4) {
+        if (l4 + 3 > j) {
+          T v[4];
+          ld4(cb + l4, v);
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const int l = l4 + u;
+            if (l > j && lane >= l && l < jb) row[l] -= row[j] * v[u];
+          }
+        }
       }
+      __syncwarp();                        // cb is rewritten by the next column
     }
   }
 #pragma unroll
-  for (int t = 0; t < 32; t++)
+  for (int t = 0; t < 32; t++) {
     if (lane < jb && t <= lane) Ds[(j0 + lane) * S + j0 + t] = row[t];
-  __syncwarp();
-  // lane c: column c of the inverse, x_i = (delta_ic - sum_{c<=t<i} L(i,t) x_t) / L(i,i)
-  T x[32];
-#pragma unroll
-  for (int i = 0; i < 32; i++) {
-    T v = T(0);
-    if (i < jb && i >= lane) {
-      T acc = i == lane ? T(1) : T(0);
-#pragma unroll
-      for (int t = 0; t < i; t++)
-        if (t >= lane) acc -= Ds[(j0 + i) * S + j0 + t] * x[t];
-      v = acc / Ds[(j0 + i) * S + j0 + i];
-    }
-    x[i] = v;
-    Li[i * LS + lane] = v;
+    LT[t * kLT + lane] = row[t];
   }
   __syncwarp();
   return bad;
 }
 
-// The kb x kb diagonal block of every front's panel, a CTA per front:
-// right-looking over 32-column blocks (warp register Cholesky and inverse of
-// the block, the rows below it times that inverse by a warp per row, the rest
-// of the block by 4 x 4 register tiles), then the inverse of L11 block row by
-// block row, V(r, c) = -Li_r sum_{k=c}^{r-1} L(r, k) V(k, c).  Writes L11 into
-// the front (lower triangle) and the inverse, K-major (slot[t W + c] =
-// Linv(c, t), zero outside the lower kb x kb triangle), into the front's slot.
+// One warp: the inverse of the jb x jb factor left in Wk by warp_chol, to Li
+// (row-major, stride LS; zero above the diagonal and outside jb).  Lane c
+// holds column c and eliminates right-looking, so the dependent chain is one
+// multiply-add per column.
+template <class T, int LS>
+__device__ void warp_inv(const T* Wk, int jb, T* Li) {
+  const int lane = threadIdx.x & 31;
+  const T* LT = Wk;
+  const T rd = lane < jb ? T(1) / LT[lane * kLT + lane] : T(1);
+  T x[32];
+#pragma unroll
+  for (int i = 0; i < 32; i++) x[i] = i == lane ? T(1) : T(0);
+#pragma unroll
+  for (int t = 0; t < 32; t++) {
+    if (t < jb) {
+      x[t] *= __shfl_sync(0xffffffffu, rd, t);
+#pragma unroll
+      for (int i4 = 0; i4 < 32; i4 += 4) {
+        if (i4 + 3 > t) {
+          T v[4];
+          ld4(LT + t * kLT + i4, v);
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const int i = i4 + u;
+            if (i > t && i < jb) x[i] -= v[u] * x[t];
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 32; i++) Li[i * LS + lane] = (i < jb && lane < jb && i >= lane) ? x[i] : T(0);
+}
+
+// 4 x 4 tiles of the lower triangle of the trailing block rows/columns
+// [c1, kb): A(r, c) -= sum_t L(r, c0 + t) L(c, c0 + t), c <= r, for the tiles
+// tI = first, first + step, ... below last (lower-triangle tile index).
+template <class T, int S>
+__device__ __forceinline__ void trail_tiles(T* As, int c0, int c1, int kb, int first, int last,
+                                            int step) {
+  for (int tI = first; tI < last; tI += step) {
+    int ti = (int)((sqrtf(8.f * (float)tI + 1.f) - 1.f) * 0.5f);   // tile row of lower index tI
+    while (ti * (ti + 1) / 2 > tI) ti--;
+    while ((ti + 1) * (ti + 2) / 2 <= tI) ti++;
+    const int ra = c1 + 4 * ti, ca = c1 + 4 * (tI - ti * (ti + 1) / 2);
+    T acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) acc[i][j] = T(0);
+#pragma unroll 4
+    for (int t = 0; t < 32; t++) {
+      T a[4], bb[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        a[i] = ra + i < kb ? As[(ra + i) * S + c0 + t] : T(0);
+        bb[i] = ca + i < kb ? As[(ca + i) * S + c0 + t] : T(0);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (ra + i < kb && ca + j <= ra + i) As[(ra + i) * S + ca + j] -= acc[i][j];
+  }
+}
+
+// The kb x kb diagonal block of every front's panel, a CTA per front,
+// right-looking over 32-column blocks with the serial part overlapped: while
+// warp 0 inverts block b, warps 1-7 solve the rows below it against its
+// factor (forward substitution, lane = column, fourteen rows interleaved);
+// then block b+1's diagonal region takes its update, and while warp 0 factors
+// it the other warps update the rest of the trailing block.  Writes L11 into
+// the front (lower triangle) and the inverses of its 32 x 32 diagonal blocks
+// into the front's slot, K-major: slot[b 1024 + t 32 + c] = Li_b(c, t), zero
+// outside the block's jb x jb lower triangle.
 template <class T, int W>
 __global__ void __launch_bounds__(kPanThreads) k_diag_factor(const int* __restrict__ flist,
                                                              const FrontDev* __restrict__ fr,
                                                              T* __restrict__ F, int Ks,
                                                              T* __restrict__ slot, DevError* err) {
-  constexpr int S = diag_stride<W>(), NB = W / 32;
-  constexpr int ME = NB > 1 ? (NB - 1) * 1024 / kPanThreads : 1;   // inverse entries per thread
+  constexpr int S = diag_stride<W>(), NW = kPanThreads / 32;
+  constexpr int MQ = (W - 32 + NW - 2) / (NW - 1);   // rows below a block per solving warp
   extern __shared__ __align__(16) unsigned char diag_raw[];
   T* As = reinterpret_cast<T*>(diag_raw);   // the block, then L11 (row-major, stride S)
-  T* Vs = As + W * S;                       // the inverse of L11 (row-major, stride S)
+  T* Vs = As + W * S;                       // inverses of the diagonal blocks (row-major, S)
+  T* Wk = Vs + W * S;                       // warp_chol / warp_inv scratch
   __shared__ int badcol;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const FrontDev d = fr[flist[blockIdx.x]];
@@ -154,94 +253,60 @@ __global__ void __launch_bounds__(kPanThreads) k_diag_factor(const int* __restri
   const int kb = min(W, d.n - Ks), nb = (kb + 31) / 32;
   for (int idx = tid; idx < W * W; idx += kPanThreads) {
     const int r = idx % W, c = idx / W;
-    As[r * S + c] = (r < kb && c <= r) ? A[(Ks + r) + (int64_t)(Ks + c) * ld] : T(0);
-    Vs[r * S + c] = T(0);
+    const bool take = r < kb && c <= r;
+    cp_elem(As + r * S + c, take ? A + (Ks + r) + (int64_t)(Ks + c) * ld : A, take);
   }
+  cp_commit();
   if (tid == 0) badcol = -1;
+  cp_wait<0>();
+  __syncthreads();
+  if (warp == 0) {
+    const int bad = warp_chol<T, S>(As, 0, min(32, kb), Wk);
+    if (lane == 0 && bad >= 0) badcol = Ks + bad;
+  }
   __syncthreads();
   for (int b = 0; b < nb; b++) {
     const int c0 = 32 * b, jb = min(32, kb - c0), c1 = c0 + jb;
     if (warp == 0) {
-      const int bad = warp_chol_inv<T, S, S>(As, c0, jb, Vs + c0 * S + c0);
-      if (lane == 0 && bad >= 0 && badcol < 0) badcol = Ks + c0 + bad;
-    }
-    __syncthreads();
-    // rows below block b (jb = 32 whenever there are any): L(r, c0 + c) =
-    // sum_t A(r, c0 + t) Linv_b(c, t), a warp per row, lane c
-    for (int r = c1 + warp; r < kb; r += kPanThreads / 32) {
-      T acc = T(0);
-#pragma unroll 8
-      for (int t = 0; t < 32; t++) acc += As[r * S + c0 + t] * Vs[(c0 + lane) * S + c0 + t];
-      __syncwarp();
-      As[r * S + c0 + lane] = acc;
-    }
-    __syncthreads();
-    // the rest of the block: A(r, c) -= sum_t L(r, c0 + t) L(c, c0 + t), c <= r
-    const int m4 = (kb - c1 + 3) / 4, ntile = m4 * (m4 + 1) / 2;
-    for (int tI = tid; tI < ntile; tI += kPanThreads) {
-      int ti = (int)((sqrtf(8.f * (float)tI + 1.f) - 1.f) * 0.5f);   // tile row of lower index tI
-      while (ti * (ti + 1) / 2 > tI) ti--;
-      while ((ti + 1) * (ti + 2) / 2 <= tI) ti++;
-      const int ra = c1 + 4 * ti, ca = c1 + 4 * (tI - ti * (ti + 1) / 2);
-      T acc[4][4];
+      warp_inv<T, S>(Wk, jb, Vs + c0 * S + c0);
+    } else if (c1 < kb) {
+      // rows below block b (jb = 32): x L_bb^T = a, lane c solves column c
+      T lr[32];
 #pragma unroll
-      for (int i = 0; i < 4; i++)
+      for (int t = 0; t < 32; t++) lr[t] = t <= lane ? As[(c0 + lane) * S + c0 + t] : T(0);
+      const T rd = T(1) / As[(c0 + lane) * S + c0 + lane];
+      T a[MQ];
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = T(0);
-#pragma unroll 4
+      for (int q = 0; q < MQ; q++) {
+        const int r = c1 + (warp - 1) + (NW - 1) * q;
+        a[q] = r < kb ? As[r * S + c0 + lane] : T(0);
+      }
+#pragma unroll
       for (int t = 0; t < 32; t++) {
-        T a[4], bb[4];
+        const T rdt = __shfl_sync(0xffffffffu, rd, t);
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-          a[i] = ra + i < kb ? As[(ra + i) * S + c0 + t] : T(0);
-          bb[i] = ca + i < kb ? As[(ca + i) * S + c0 + t] : T(0);
+        for (int q = 0; q < MQ; q++) {
+          const T xt = __shfl_sync(0xffffffffu, a[q], t) * rdt;
+          a[q] = lane == t ? xt : (lane > t ? fma(-xt, lr[t], a[q]) : a[q]);
         }
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-          for (int j = 0; j < 4; j++) acc[i][j] += a[i] * bb[j];
       }
 #pragma unroll
-      for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-          if (ra + i < kb && ca + j <= ra + i) As[(ra + i) * S + ca + j] -= acc[i][j];
-    }
-    __syncthreads();
-  }
-  // the inverse below its diagonal blocks, block row rb at a time
-  for (int rb = 1; rb < nb; rb++) {
-    const int R0 = 32 * rb, ne = rb * 1024;
-    // sum_{k} L(rb, k) V(k, c) into block (rb, c) of Vs: nothing reads that block row yet
-#pragma unroll
-    for (int q = 0; q < ME; q++) {
-      const int e = tid + q * kPanThreads;
-      if (e < ne) {
-        const int cb = e >> 10, i = (e >> 5) & 31, j = e & 31;
-        T acc = T(0);
-        for (int k = 32 * cb; k < R0; k++) acc += As[(R0 + i) * S + k] * Vs[k * S + 32 * cb + j];
-        Vs[(R0 + i) * S + 32 * cb + j] = acc;
+      for (int q = 0; q < MQ; q++) {
+        const int r = c1 + (warp - 1) + (NW - 1) * q;
+        if (r < kb) As[r * S + c0 + lane] = a[q];
       }
     }
     __syncthreads();
-    T v[ME];
-#pragma unroll
-    for (int q = 0; q < ME; q++) {
-      const int e = tid + q * kPanThreads;
-      v[q] = T(0);
-      if (e < ne) {
-        const int cb = e >> 10, i = (e >> 5) & 31, j = e & 31;
-        T acc = T(0);
-        for (int t = 0; t <= i; t++)
-          acc += Vs[(R0 + i) * S + R0 + t] * Vs[(R0 + t) * S + 32 * cb + j];
-        v[q] = -acc;
-      }
-    }
+    if (c1 >= kb) break;                    // the last block: nothing below it
+    const int m4 = (kb - c1 + 3) / 4, ntile = m4 * (m4 + 1) / 2;
+    const int ndiag = min(8, m4) * (min(8, m4) + 1) / 2;   // tiles of block b+1's diagonal region
+    trail_tiles<T, S>(As, c0, c1, kb, tid, ndiag, kPanThreads);
     __syncthreads();
-#pragma unroll
-    for (int q = 0; q < ME; q++) {
-      const int e = tid + q * kPanThreads;
-      if (e < ne) Vs[(R0 + ((e >> 5) & 31)) * S + 32 * (e >> 10) + (e & 31)] = v[q];
+    if (warp == 0) {
+      const int bad = warp_chol<T, S>(As, c1, min(32, kb - c1), Wk);
+      if (lane == 0 && bad >= 0 && badcol < 0) badcol = Ks + c1 + bad;
+    } else {
+      trail_tiles<T, S>(As, c0, c1, kb, ndiag + tid - 32, ntile, kPanThreads - 32);
     }
     __syncthreads();
   }
@@ -253,28 +318,34 @@ __global__ void __launch_bounds__(kPanThreads) k_diag_factor(const int* __restri
     const int r = idx % kb, c = idx / kb;
     if (c <= r) A[(Ks + r) + (int64_t)(Ks + c) * ld] = As[r * S + c];
   }
-  T* Lt = slot + (int64_t)blockIdx.x * W * W;
-  for (int idx = tid; idx < W * W; idx += kPanThreads) Lt[idx] = Vs[(idx % W) * S + idx / W];
+  T* Li = slot + (int64_t)blockIdx.x * W * W;
+  for (int idx = tid; idx < W * 32; idx += kPanThreads) {
+    const int bq = idx >> 10, t = (idx >> 5) & 31, c = idx & 31;
+    Li[idx] = bq < nb ? Vs[(32 * bq + c) * S + 32 * bq + t] : T(0);
+  }
 }
 
-// The rows below the diagonal block, L21 = A21 L11^{-T} = A21 Linv^T, over a
-// persistent grid.  Items are 128-row blocks of every front's rows [Ks + kb,
-// N), listed front by front.  A CTA holds the tile K-major (Xs[t][r]) and the
-// front's inverse K-major (Ls[t][c] = Linv(c, t), loaded once per front it
-// visits); thread (tx, ty) accumulates rows 4 ty .. 4 ty + 3 and 64 + the
-// same, columns tx + 16 j (+ 64 h) in registers.  Linv(c, t) = 0 for t > c, so
-// past t = 64 h only the column groups from h on take part.  The result goes
-// through shared memory (row-major, stride W + 1) for coalesced stores.
+// The rows below the diagonal block, L21 = A21 L11^{-T}, over a persistent
+// grid.  Items are 128-row blocks of every front's rows [Ks + kb, N), listed
+// front by front; a CTA takes items blockIdx.x, + gridDim.x, ... and fetches
+// the next item's tile (cp.async, 64 KB in flight per CTA) into its second
+// buffer while it works on the current one.  The tile is K-major (X[c][r]);
+// L11 (from the front, K-major: Ls[t][c] = L(c, t)) and the inverses of its
+// 32 x 32 diagonal blocks (from the slot) are fetched once per front the CTA
+// visits.  Blocked substitution, 32 columns at a time: Y_b = X_b - sum_{k<b}
+// Z_k L_bk^T, then Z_b = Y_b Li_b^T, written over X_b.  Thread (tx, ty) owns
+// rows 4 ty .. 4 ty + 3 and 64 + the same, and in block b the columns
+// 32 b + tx and 32 b + tx + 16, in registers.
 template <class T, int W>
 __global__ void __launch_bounds__(kPanThreads) k_panel_trsm(const int* __restrict__ flist, int nf,
                                                             const FrontDev* __restrict__ fr,
                                                             T* __restrict__ F, int Ks,
                                                             const T* __restrict__ slot) {
-  constexpr int XS = xs_stride<T>(), LS = ls_stride<T, W>(), CG = W / 64, RS = W + 1;
-  static_assert(kTrsmRows * RS <= W * XS, "result tile must fit the input tile");
+  constexpr int XS = xs_stride<T>(), LS = ls_stride<T, W>(), NB = W / 32;
   extern __shared__ __align__(16) unsigned char trsm_raw[];
-  T* Xs = reinterpret_cast<T*>(trsm_raw);   // the tile (K-major), then the result (row-major)
-  T* Ls = Xs + W * XS;                       // the inverse, K-major
+  T* Xb = reinterpret_cast<T*>(trsm_raw);   // two tile buffers, K-major
+  T* Ls = Xb + 2 * W * XS;                   // L11, K-major
+  T* Lis = Ls + W * LS;                      // inverses of its diagonal blocks, K-major
   __shared__ int pre[kMaxPanelFronts + 1];
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   for (int i = tid; i < nf; i += kPanThreads) {
@@ -288,68 +359,131 @@ __global__ void __launch_bounds__(kPanThreads) k_panel_trsm(const int* __restric
   }
   __syncthreads();
   const int total = pre[nf];
-  int cur = -1;
-  for (int item = blockIdx.x; item < total; item += gridDim.x) {
+  if ((int)blockIdx.x >= total) return;
+  // item -> front index, first row, rows, panel width
+  auto locate = [&](int item, int& i, int& r0, int& rows, int& kb) {
     int lo = 0, hi = nf - 1;   // largest i with pre[i] <= item
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (pre[mid] <= item) lo = mid;
       else hi = mid - 1;
     }
-    const int i = lo;
+    i = lo;
     const FrontDev d = fr[flist[i]];
-    T* A = F + d.off;
-    const int64_t ld = d.ld;
-    const int kb = min(W, d.n - Ks);
-    const int r0 = Ks + kb + (item - pre[i]) * kTrsmRows, rows = min(kTrsmRows, d.N - r0);
-    __syncthreads();                         // the previous item's result has been stored
-    if (i != cur) {
-      cur = i;
-      const T* Lt = slot + (int64_t)i * W * W;
-      for (int idx = tid; idx < W * W; idx += kPanThreads) Ls[(idx / W) * LS + idx % W] = Lt[idx];
-    }
+    kb = min(W, d.n - Ks);
+    r0 = Ks + kb + (item - pre[i]) * kTrsmRows;
+    rows = min(kTrsmRows, d.N - r0);
+  };
+  auto fetch = [&](T* X, int i, int r0, int rows, int kb) {
+    const FrontDev d = fr[flist[i]];
+    const T* A = F + d.off;
     for (int idx = tid; idx < W * kTrsmRows; idx += kPanThreads) {
       const int r = idx % kTrsmRows, t = idx / kTrsmRows;
-      Xs[t * XS + r] = (r < rows && t < kb) ? A[(r0 + r) + (int64_t)(Ks + t) * ld] : T(0);
+      const bool take = r < rows && t < kb;
+      cp_elem(X + t * XS + r, take ? A + (r0 + r) + (int64_t)(Ks + t) * d.ld : A, take);
+    }
+  };
+  int i, r0, rows, kb, cur = -1;
+  locate(blockIdx.x, i, r0, rows, kb);
+  fetch(Xb, i, r0, rows, kb);
+  cp_commit();
+  for (int item = blockIdx.x, k = 0; item < total; item += gridDim.x, k++) {
+    T* X = Xb + (k & 1) * W * XS;
+    __syncthreads();                         // the other buffer's result has been stored
+    if (i != cur) {
+      cur = i;
+      const FrontDev d = fr[flist[i]];
+      const T* A = F + d.off;
+      for (int idx = tid; idx < W * W; idx += kPanThreads) {
+        const int c = idx % W, t = idx / W;
+        const bool take = c < kb && t < kb && t <= c;
+        cp_elem(Ls + t * LS + c, take ? A + (Ks + c) + (int64_t)(Ks + t) * d.ld : A, take);
+      }
+      const T* Lt = slot + (int64_t)i * W * W;
+      for (int idx = tid; idx < W * 32; idx += kPanThreads) cp_elem(Lis + idx, Lt + idx, true);
+      cp_commit();
+    }
+    int ni = i, nr0 = 0, nrows = 0, nkb = 0;
+    if (item + (int)gridDim.x < total) {
+      locate(item + gridDim.x, ni, nr0, nrows, nkb);
+      fetch(Xb + ((k + 1) & 1) * W * XS, ni, nr0, nrows, nkb);
+      cp_commit();
+      cp_wait<1>();                          // all but the prefetch
+    } else {
+      cp_wait<0>();
     }
     __syncthreads();
-    T acc[8][4 * CG];
+    const int nbk = (kb + 31) / 32;
+    for (int b = 0; b < nbk && b < NB; b++) {
+      const int ca = 32 * b + tx, cb = ca + 16;
+      T acc[8][2];
+      {
+        T xa[8], xb[8];                      // X_b, the thread's two columns
+        ld4(X + ca * XS + 4 * ty, xa);
+        ld4(X + ca * XS + 64 + 4 * ty, xa + 4);
+        ld4(X + cb * XS + 4 * ty, xb);
+        ld4(X + cb * XS + 64 + 4 * ty, xb + 4);
 #pragma unroll
-    for (int a = 0; a < 8; a++)
+        for (int r = 0; r < 8; r++) {
+          acc[r][0] = xa[r];
+          acc[r][1] = xb[r];
+        }
+      }
+      for (int t = 0; t < 32 * b; t++) {     // - Z_k L_bk^T over the solved columns
+        T z[8];
+        ld4(X + t * XS + 4 * ty, z);
+        ld4(X + t * XS + 64 + 4 * ty, z + 4);
+        const T la = Ls[t * LS + ca], lb = Ls[t * LS + cb];
 #pragma unroll
-      for (int c = 0; c < 4 * CG; c++) acc[a][c] = T(0);
+        for (int r = 0; r < 8; r++) {
+          acc[r][0] = fma(-z[r], la, acc[r][0]);
+          acc[r][1] = fma(-z[r], lb, acc[r][1]);
+        }
+      }
+      // Y_b in place (only this thread reads these entries before the barrier)
 #pragma unroll
-    for (int hs = 0; hs < CG; hs++) {
-      const int tend = min(kb, 64 * hs + 64);
-      for (int t = 64 * hs; t < tend; t++) {
-        T a[8], b[4 * CG];
-        ld4(Xs + t * XS + 4 * ty, a);
-        ld4(Xs + t * XS + 64 + 4 * ty, a + 4);
+      for (int r = 0; r < 8; r++) {
+        X[ca * XS + 64 * (r >> 2) + 4 * ty + (r & 3)] = acc[r][0];
+        X[cb * XS + 64 * (r >> 2) + 4 * ty + (r & 3)] = acc[r][1];
+      }
+      __syncthreads();
+      // Z_b = Y_b Li_b^T
+      T out[8][2];
 #pragma unroll
-        for (int h = hs; h < CG; h++)
+      for (int r = 0; r < 8; r++) out[r][0] = out[r][1] = T(0);
+      const T* Li = Lis + b * 1024;
+#pragma unroll 4
+      for (int t = 0; t < 32; t++) {
+        T y[8];
+        ld4(X + (32 * b + t) * XS + 4 * ty, y);
+        ld4(X + (32 * b + t) * XS + 64 + 4 * ty, y + 4);
+        const T la = Li[t * 32 + tx], lb = Li[t * 32 + tx + 16];
 #pragma unroll
-          for (int j = 0; j < 4; j++) b[4 * h + j] = Ls[t * LS + 64 * h + tx + 16 * j];
+        for (int r = 0; r < 8; r++) {
+          out[r][0] = fma(y[r], la, out[r][0]);
+          out[r][1] = fma(y[r], lb, out[r][1]);
+        }
+      }
+      __syncthreads();                       // every read of Y_b is done
 #pragma unroll
-        for (int r = 0; r < 8; r++)
-#pragma unroll
-          for (int h = hs; h < CG; h++)
-#pragma unroll
-            for (int j = 0; j < 4; j++) acc[r][4 * h + j] = fma(a[r], b[4 * h + j], acc[r][4 * h + j]);
+      for (int r = 0; r < 8; r++) {
+        X[ca * XS + 64 * (r >> 2) + 4 * ty + (r & 3)] = out[r][0];
+        X[cb * XS + 64 * (r >> 2) + 4 * ty + (r & 3)] = out[r][1];
+      }
+      __syncthreads();
+    }
+    {
+      const FrontDev d = fr[flist[i]];
+      T* A = F + d.off;
+      for (int idx = tid; idx < kb * kTrsmRows; idx += kPanThreads) {
+        const int r = idx % kTrsmRows, c = idx / kTrsmRows;
+        if (r < rows) A[(r0 + r) + (int64_t)(Ks + c) * d.ld] = X[c * XS + r];
       }
     }
-    __syncthreads();                         // every read of the tile is done
-#pragma unroll
-    for (int r = 0; r < 8; r++)
-#pragma unroll
-      for (int h = 0; h < CG; h++)
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-          Xs[(64 * (r >> 2) + 4 * ty + (r & 3)) * RS + 64 * h + tx + 16 * j] = acc[r][4 * h + j];
-    __syncthreads();
-    for (int idx = tid; idx < kb * kTrsmRows; idx += kPanThreads) {
-      const int r = idx % kTrsmRows, c = idx / kTrsmRows;
-      if (r < rows) A[(r0 + r) + (int64_t)(Ks + c) * ld] = Xs[r * RS + c];
-    }
+    i = ni;
+    r0 = nr0;
+    rows = nrows;
+    kb = nkb;
   }
 }
 

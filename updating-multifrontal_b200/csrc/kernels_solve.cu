@@ -288,7 +288,8 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_bwd(const int* __restrict__ 
                                                         const int2* __restrict__ tasks, int ntasks,
                                                         const int* __restrict__ flagoff, int* flags,
                                                         DevError* err) {
-  __shared__ T xs[SB][NR + 1];
+  constexpr int BR = 4;                       // boundary row blocks per shared-memory round
+  __shared__ T xs[BR * SB][NR + 1];
   __shared__ T vs[SB][NR + 1];
   const int tid = threadIdx.x, cl = tid >> 2, q = tid & 3;   // column of the block, row quarter
   for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
@@ -306,28 +307,29 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_bwd(const int* __restrict__ 
     T acc[NR];
 #pragma unroll
     for (int c = 0; c < NR; c++) acc[c] = T(0);
-    // rows [r0, r0 + nr) against xs: lanes (cl, q) take rows 16 q .. 16 q + 15
-    auto chunk = [&](int r0, int nr) {
+    // rows [r0, r0 + nr) against xs rows [x0, x0 + nr): lanes (cl, q) take
+    // rows 16 q .. 16 q + 15, all 16 loads in flight before the products
+    auto chunk = [&](int r0, int nr, int x0) {
       if (!live) return;
-#pragma unroll 4
-      for (int rr = 0; rr < 16; rr++) {
-        const int r = 16 * q + rr;
-        if (r < nr) {
-          const T l = Lc[r0 + r];
+      T l[16];
 #pragma unroll
-          for (int c = 0; c < NR; c++) acc[c] = fma(l, xs[r][c], acc[c]);
-        }
-      }
+      for (int rr = 0; rr < 16; rr++) l[rr] = 16 * q + rr < nr ? Lc[r0 + 16 * q + rr] : T(0);
+#pragma unroll
+      for (int rr = 0; rr < 16; rr++)
+#pragma unroll
+        for (int c = 0; c < NR; c++) acc[c] = fma(l[rr], xs[x0 + 16 * q + rr][c], acc[c]);
     };
-    for (int r0 = d.n; r0 < d.N; r0 += SB) {           // boundary rows: x_bd from X
-      const int nr = min(SB, d.N - r0);
+    for (int r0 = d.n; r0 < d.N; r0 += BR * SB) {      // boundary rows: x_bd from X
+      const int nr = min(BR * SB, d.N - r0);
       __syncthreads();
-      for (int idx = tid; idx < SB * nrhs; idx += SCT) {
-        const int r = idx % SB, c = idx / SB;
+      for (int idx = tid; idx < BR * SB * nrhs; idx += SCT) {
+        const int r = idx % (BR * SB), c = idx / (BR * SB);
         xs[r][c] = r < nr ? X[dl[r0 + r] + (int64_t)c * ldx] : T(0);
       }
       __syncthreads();
-      chunk(r0, nr);
+#pragma unroll
+      for (int s = 0; s < BR; s++)
+        if (s * SB < nr) chunk(r0 + s * SB, min(SB, nr - s * SB), s * SB);
     }
     for (int R = nb - 1; R > j + 1; R--) {              // solved pivot blocks below but the nearest
       const int r0 = R * SB, nr = min(SB, d.n - r0);
@@ -339,7 +341,7 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_bwd(const int* __restrict__ 
         xs[r][c] = r < nr ? ldcg(Y + r0 + r + (int64_t)c * d.N) : T(0);
       }
       __syncthreads();
-      chunk(r0, nr);
+      chunk(r0, nr, 0);
     }
     // before the last wait: block j + 1's L values, this column's quarter of
     // Dinv_j^T (upper triangular, column-major) and y_j

@@ -340,8 +340,8 @@ struct mfgpu_handle {
   int tcSub = 128;                 // mixed: sub-panel width inside each 512-column outer panel of a
                                    // tensor-core level (0 or 512: no sub-panels)
   int fusedMinFronts = 148;        // fewest fronts for the one-CTA-per-front kernel
-  bool subpanel = false;           // tensor-core levels: sub-panels by k_diag_factor + k_panel_trsm (MFGPU_SUBPANEL=1)
-                                   // instead of the cooperative kernel, which measures faster
+  bool subpanel = true;            // tensor-core levels: sub-panels by k_diag_factor + k_panel_trsm
+                                   // (MFGPU_SUBPANEL=0: by the cooperative kernel)
   int panelMaxN = 0;               // largest front of a level factored panel by panel (0: never;
                                    // MFGPU_PANEL_MAX_N; the autotuner may still pick the kernel)
   size_t esz = sizeof(double);     // bytes per factor element
