@@ -33,7 +33,7 @@ def test_autotuned_factorization(N, precision):
     F = make(N, A, **kw)
     choices = F.autotune(2)
     assert len(choices) == F.info()["levels"]
-    assert set(choices) <= {"fused", "coop", "tc", "stepped", "none"}
+    assert set(choices) <= {"fused", "coop", "tc", "stepped", "panel", "none"}
     G = make(N, A, **kw)                      # size rules
     G.Factor()
     x, y = F.Solve(b[0]), G.Solve(b[0])
