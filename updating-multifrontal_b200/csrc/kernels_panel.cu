@@ -7,11 +7,11 @@
 // already applied) becomes L in two launches:
 //   k_diag_factor  one CTA per front factors the kb x kb diagonal block in
 //                  shared memory, 32 columns at a time (a warp's register
-//                  Cholesky of the 32 x 32 block, the rows below it by
-//                  substitution, the rest of the block by 4 x 4 register
-//                  tiles, the block inverses off the critical path), writes
-//                  L11 back and leaves the inverses of its 32 x 32 diagonal
-//                  blocks in the front's scratch slot;
+//                  Cholesky and inverse of the 32 x 32 block, the rows below
+//                  it by that inverse, the rest of the block by 4 x 4
+//                  register tiles),
+//                  writes L11 back and leaves the inverses of its 32 x 32
+//                  diagonal blocks in the front's scratch slot;
 //   k_panel_trsm   the rows below the block, L21 = A21 L11^{-T}, by blocked
 //                  substitution with L11 and those inverses: 128-row items
 //                  over a persistent grid, 16 outputs per thread in
@@ -225,21 +225,22 @@ __device__ __forceinline__ void trail_tiles(T* As, int c0, int c1, int kb, int f
 }
 
 // The kb x kb diagonal block of every front's panel, a CTA per front,
-// right-looking over 32-column blocks with the serial part overlapped: while
-// warp 0 inverts block b, warps 1-7 solve the rows below it against its
-// factor (forward substitution, lane = column, fourteen rows interleaved);
-// then block b+1's diagonal region takes its update, and while warp 0 factors
-// it the other warps update the rest of the trailing block.  Writes L11 into
-// the front (lower triangle) and the inverses of its 32 x 32 diagonal blocks
-// into the front's slot, K-major: slot[b 1024 + t 32 + c] = Li_b(c, t), zero
-// outside the block's jb x jb lower triangle.
+// right-looking over 32-column blocks: warp 0 factors block b and inverts it
+// (registers, shared-memory broadcasts), then all warps form the rows below it
+// as products with that inverse (a warp per eight rows, independent
+// accumulators) and update the rest of the block (4 x 4 register tiles).  The
+// phases do not overlap: the tile updates' shared-memory traffic would stretch
+// the warp's latency-bound chain (measured slower).  Writes L11 into the front
+// (lower triangle) and the inverses of its 32 x 32 diagonal blocks into the
+// front's slot, K-major: slot[b 1024 + t 32 + c] = Li_b(c, t), zero outside
+// the block's jb x jb lower triangle.
 template <class T, int W>
 __global__ void __launch_bounds__(kPanThreads) k_diag_factor(const int* __restrict__ flist,
                                                              const FrontDev* __restrict__ fr,
                                                              T* __restrict__ F, int Ks,
                                                              T* __restrict__ slot, DevError* err) {
   constexpr int S = diag_stride<W>(), NW = kPanThreads / 32;
-  constexpr int MQ = (W - 32 + NW - 2) / (NW - 1);   // rows below a block per solving warp
+  constexpr int MQ = (W - 32) / NW;         // rows below a block per warp, at most
   extern __shared__ __align__(16) unsigned char diag_raw[];
   T* As = reinterpret_cast<T*>(diag_raw);   // the block, then L11 (row-major, stride S)
   T* Vs = As + W * S;                       // inverses of the diagonal blocks (row-major, S)
@@ -260,54 +261,39 @@ __global__ void __launch_bounds__(kPanThreads) k_diag_factor(const int* __restri
   if (tid == 0) badcol = -1;
   cp_wait<0>();
   __syncthreads();
-  if (warp == 0) {
-    const int bad = warp_chol<T, S>(As, 0, min(32, kb), Wk);
-    if (lane == 0 && bad >= 0) badcol = Ks + bad;
-  }
-  __syncthreads();
   for (int b = 0; b < nb; b++) {
     const int c0 = 32 * b, jb = min(32, kb - c0), c1 = c0 + jb;
     if (warp == 0) {
+      const int bad = warp_chol<T, S>(As, c0, jb, Wk);
       warp_inv<T, S>(Wk, jb, Vs + c0 * S + c0);
-    } else if (c1 < kb) {
-      // rows below block b (jb = 32): x L_bb^T = a, lane c solves column c
-      T lr[32];
-#pragma unroll
-      for (int t = 0; t < 32; t++) lr[t] = t <= lane ? As[(c0 + lane) * S + c0 + t] : T(0);
-      const T rd = T(1) / As[(c0 + lane) * S + c0 + lane];
-      T a[MQ];
-#pragma unroll
-      for (int q = 0; q < MQ; q++) {
-        const int r = c1 + (warp - 1) + (NW - 1) * q;
-        a[q] = r < kb ? As[r * S + c0 + lane] : T(0);
-      }
-#pragma unroll
-      for (int t = 0; t < 32; t++) {
-        const T rdt = __shfl_sync(0xffffffffu, rd, t);
-#pragma unroll
-        for (int q = 0; q < MQ; q++) {
-          const T xt = __shfl_sync(0xffffffffu, a[q], t) * rdt;
-          a[q] = lane == t ? xt : (lane > t ? fma(-xt, lr[t], a[q]) : a[q]);
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < MQ; q++) {
-        const int r = c1 + (warp - 1) + (NW - 1) * q;
-        if (r < kb) As[r * S + c0 + lane] = a[q];
-      }
+      if (lane == 0 && bad >= 0 && badcol < 0) badcol = Ks + c0 + bad;
     }
     __syncthreads();
     if (c1 >= kb) break;                    // the last block: nothing below it
-    const int m4 = (kb - c1 + 3) / 4, ntile = m4 * (m4 + 1) / 2;
-    const int ndiag = min(8, m4) * (min(8, m4) + 1) / 2;   // tiles of block b+1's diagonal region
-    trail_tiles<T, S>(As, c0, c1, kb, tid, ndiag, kPanThreads);
-    __syncthreads();
-    if (warp == 0) {
-      const int bad = warp_chol<T, S>(As, c1, min(32, kb - c1), Wk);
-      if (lane == 0 && bad >= 0 && badcol < 0) badcol = Ks + c1 + bad;
-    } else {
-      trail_tiles<T, S>(As, c0, c1, kb, ndiag + tid - 32, ntile, kPanThreads - 32);
+    // rows below block b (jb = 32): L(r, c0 + c) = sum_t A(r, c0 + t) Li_b(c, t)
+    {
+      T acc[MQ];
+#pragma unroll
+      for (int q = 0; q < MQ; q++) acc[q] = T(0);
+#pragma unroll 4
+      for (int t = 0; t < 32; t++) {
+        const T l = Vs[(c0 + lane) * S + c0 + t];
+#pragma unroll
+        for (int q = 0; q < MQ; q++) {
+          const int r = c1 + warp + NW * q;
+          if (r < kb) acc[q] = fma(As[r * S + c0 + t], l, acc[q]);
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < MQ; q++) {
+        const int r = c1 + warp + NW * q;
+        if (r < kb) As[r * S + c0 + lane] = acc[q];
+      }
     }
+    __syncthreads();
+    const int m4 = (kb - c1 + 3) / 4;
+    trail_tiles<T, S>(As, c0, c1, kb, tid, m4 * (m4 + 1) / 2, kPanThreads);
     __syncthreads();
   }
   if (tid == 0 && badcol >= 0 && atomicCAS(&err->code, 0, 1) == 0) {
