@@ -715,6 +715,9 @@ def main():
     ap.add_argument("--rate", type=float, default=4.0, help="serving: arrivals per second")
     ap.add_argument("--requests", type=int, default=24, help="serving: requests in the stream")
     ap.add_argument("--slots", type=int, default=8, help="serving: requests per batch")
+    ap.add_argument("--serve-reference", action="store_true",
+                    help="serving: also time the reference's CPU Update + Solve of the first "
+                         "request on the host cores (minutes: it factors the base first)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -1022,11 +1025,27 @@ def run_serve(args, w):
                 "h2d_bytes_per_step": int(np.mean([b.nbytes for *_, b in reqs])),
                 "d2h_bytes_per_step": int(np.mean([b.nbytes for *_, b in reqs]))},
     }
+    F.close()
+    if args.serve_reference:
+        # the reference serves a request as Update + Solve on its own factored
+        # base (no batching, no serving loop); time the first request
+        lo, hi, f, b = reqs[0]
+        threads = os.cpu_count() or 1
+        res = reference_time(w["dim"], N, w["max_side"], a,
+                             stencil.scale_box(a, lo, hi[0] - lo[0], f),
+                             np.ascontiguousarray(b.T), threads, reps=1)
+        if res is not None:
+            line["reference_cpu"] = {
+                "update_s": res["update_s"][0], "solve_s": res["solve_s"][0],
+                "update_solve_s": res["update_s"][0] + res["solve_s"][0],
+                "base_factor_s": res["factor_s"][0], "cores": threads, "kind": "reference",
+                "sample": f"request 0 (box side {hi[0] - lo[0]}, factor {f:.3g}, "
+                          f"{b.shape[1]} RHS) as the reference's Update + Solve on its factored "
+                          f"base, OPENBLAS_NUM_THREADS={threads}"}
     print(json.dumps(line))
     if args.json_out:
         with open(args.json_out, "w") as fo:
             fo.write(json.dumps(line) + "\n")
-    F.close()
     return 0
 
 

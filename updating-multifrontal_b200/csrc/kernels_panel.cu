@@ -415,6 +415,7 @@ __global__ void __launch_bounds__(kPanThreads) k_panel_trsm(const int* __restric
           acc[r][1] = xb[r];
         }
       }
+#pragma unroll 4
       for (int t = 0; t < 32 * b; t++) {     // - Z_k L_bk^T over the solved columns
         T z[8];
         ld4(X + t * XS + 4 * ty, z);
