@@ -1,8 +1,9 @@
 // Host-only check of the tensor-core update's tile bookkeeping (no GPU
 // needed): for many fronts, panels [K, K + w) and column bounds, the tile
 // count per front, the decoding of a tile index into (block row, block
-// column) and the pack capacity agree with a brute-force enumeration of the
-// 128 x 256 tiles of C(k1:N, k1:cmax) that touch its lower triangle.
+// column) - a bijection onto the tile set, in the grouped order - and the pack
+// capacity agree with a brute-force enumeration of the 128 x 256 tiles of
+// C(k1:N, k1:cmax) that touch its lower triangle.
 #include <cstdio>
 #include <random>
 #include <set>
@@ -18,8 +19,10 @@ using namespace mfgpu;
 int main() {
   std::mt19937 rng(20261203);
   long long checked = 0;
-  for (int trial = 0; trial < 20000; trial++) {
-    const int n = 1 + (int)(rng() % 3000), N = n + (int)(rng() % 3000);
+  for (int trial = 0; trial < 20300; trial++) {
+    // the last 300 trials: fronts of up to 50,000 (several row groups of tiles)
+    const int span = trial < 20000 ? 3000 : 25000;
+    const int n = 1 + (int)(rng() % span), N = n + (int)(rng() % span);
     const int w = (rng() % 2) ? 512 : 128;
     const int K = (int)(rng() % ((n + w - 1) / w + 1)) * w;
     const int cend = (rng() % 3 == 0) ? -1 : K + 512 * (1 + (int)(rng() % 2));
@@ -44,7 +47,7 @@ int main() {
     std::set<std::pair<int, int>> got;
     for (int t = 0; t < T; t++) {
       int I, J;
-      tile_ij(t, g.nj, I, J);
+      tile_ij(t, g.nb, g.nj, I, J);
       got.insert({I, J});
     }
     if (got != want) {

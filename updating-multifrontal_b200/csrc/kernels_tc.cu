@@ -128,20 +128,48 @@ __host__ __device__ inline int geo_tiles(const PanelGeo& g) {
   return g.nj * (g.nj + 1) + (g.nb - 2 * g.nj) * g.nj;
 }
 
-__host__ __device__ inline void tile_ij(int t, int nj, int& I, int& J) {
-  const int tri = nj * (nj + 1);
-  if (t < tri) {
-    int p = (int)((sqrt(4.0 * t + 1.0) - 1.0) * 0.5);
-    while (p * (p + 1) > t) p--;
-    while ((p + 1) * (p + 2) <= t) p++;
-    const int o = t - p * (p + 1);
-    I = 2 * p + o / (p + 1);
-    J = o % (p + 1);
-  } else {
-    const int t2 = t - tri;
-    I = 2 * nj + t2 / nj;
-    J = t2 % nj;
+// Tile order.  The tiles of a front ({(I, J): I < nb, J < nj, 2 J <= I})
+// come in groups of kTileGroup block rows; inside group [a, b) block column J
+// runs outer and the rows max(a, 2 J) .. b - 1 inner.  The CTAs working at
+// the same time then share one or two column blocks of B and revisit the
+// group's rows of A, whose packed images (16 MB per 32 rows at K = 512) stay
+// in L2; in plain row order they sweep every column block of the panel, which
+// for the largest fronts (a 196 MB panel at 127^3) does not fit in L2.
+constexpr int kTileGroup = 64;
+
+// Columns of group [a, b) holding all its rows (2 J <= a) and holding some.
+__host__ __device__ inline void group_cols(int a, int b, int nj, int& jf, int& je) {
+  jf = a / 2 + 1 < nj ? a / 2 + 1 : nj;
+  je = (b - 1) / 2 + 1 < nj ? (b - 1) / 2 + 1 : nj;
+}
+// Tiles in the first k partial columns (column jf + i holds b - 2 (jf + i)).
+__host__ __device__ inline int partial_tiles(int b, int jf, int k) {
+  return k * (b - 2 * jf) - k * (k - 1);
+}
+
+__host__ __device__ inline void tile_ij(int t, int nb, int nj, int& I, int& J) {
+  int a = 0, b = 0, jf = 0, je = 0;
+  for (a = 0; a < nb; a += kTileGroup) {
+    b = a + kTileGroup < nb ? a + kTileGroup : nb;
+    group_cols(a, b, nj, jf, je);
+    const int T = jf * (b - a) + partial_tiles(b, jf, je - jf);
+    if (t < T) break;
+    t -= T;
   }
+  const int h = b - a;
+  if (t < jf * h) {
+    J = t / h;
+    I = a + t % h;
+    return;
+  }
+  t -= jf * h;
+  const double c1 = (double)(b - 2 * jf) + 1.0;   // partial_tiles(k) = k (c1 - k)
+  int k = (int)((c1 - sqrt(c1 * c1 - 4.0 * (double)t)) * 0.5);
+  if (k < 0) k = 0;
+  while (k > 0 && partial_tiles(b, jf, k) > t) k--;
+  while (partial_tiles(b, jf, k + 1) <= t) k++;
+  J = jf + k;
+  I = 2 * J + (t - partial_tiles(b, jf, k));
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -291,7 +319,7 @@ __device__ __forceinline__ TileInfo tile_info(const int* pre, int nf, const int*
   t.nch = g.nch;
   t.nb = g.nb;
   t.slot = lo;
-  tile_ij(tile - pre[lo], g.nj, t.I, t.J);
+  tile_ij(tile - pre[lo], g.nb, g.nj, t.I, t.J);
   t.r0 = t.k1 + t.I * TM;
   t.c0 = t.k1 + t.J * TN;
   return t;
