@@ -36,10 +36,11 @@ namespace {
 constexpr int kPanThreads = 256;
 constexpr int kTrsmRows = 128;            // rows per k_panel_trsm item
 
-// Scratch of warp_chol_inv in shared memory (16-byte aligned): the factor
-// transposed, LT[t * 36 + i] = L(i, t), then the current column.
+// Scratch of warp_chol / warp_inv in shared memory (16-byte aligned): the
+// factor transposed, LT[t * 36 + i] = L(i, t), then four columns of the
+// factor, lane-major (cb[4 i + u] = L(i, jj + u)).
 constexpr int kLT = 36;
-constexpr int kCholScratch = 32 * kLT + 32;
+constexpr int kCholScratch = 32 * kLT + 128;
 
 template <class T>
 __device__ __forceinline__ T rsq(T x);
@@ -81,6 +82,15 @@ __device__ __forceinline__ void ld4(const double* p, double v[4]) {
   v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 
+// Four consecutive values to 16-byte aligned shared memory.
+__device__ __forceinline__ void st4(float* p, float a, float b, float c, float d) {
+  *reinterpret_cast<float4*>(p) = make_float4(a, b, c, d);
+}
+__device__ __forceinline__ void st4(double* p, double a, double b, double c, double d) {
+  *reinterpret_cast<double2*>(p) = make_double2(a, b);
+  *reinterpret_cast<double2*>(p + 2) = make_double2(c, d);
+}
+
 // One element global -> shared without a register round trip (cp.async, so
 // that a thread has dozens of loads in flight); zero-filled when !take.
 __device__ __forceinline__ void cp_elem(float* dst, const float* src, bool take) {
@@ -102,10 +112,53 @@ __device__ __forceinline__ void cp_wait() {
 }
 
 // One warp factors the jb x jb (jb <= 32) diagonal block at (j0, j0) of Ds
-// (row-major, stride S) in place: lane i holds row i in registers; each
-// scaled column goes through shared memory once and comes back four values
-// per load.  Leaves the factor transposed in Wk (LT[t * 36 + i] = L(i, t)).
-// Returns the first non-positive pivot column of the block, or -1.
+// (row-major, stride S) in place: lane i holds row i in registers.  Four
+// columns at a time: their pivots and their mutual updates by shuffles, then
+// the four columns of every lane go through shared memory once and the
+// columns to the right take one rank-4 update (four values per load), so the
+// warp makes one shared-memory round trip per four columns.  Leaves the factor
+// transposed in Wk (LT[t * 36 + i] = L(i, t)).  Returns the first
+// non-positive pivot column of the block, or -1.
+template <class T, int JJ>
+__device__ __forceinline__ void chol_cols4(T (&row)[32], int lane, int jb, T* cb, int& bad) {
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int j = JJ + u;
+    if (j < jb) {
+      T djj = __shfl_sync(0xffffffffu, row[j], j);
+      if (!(djj > T(0))) {                 // non-positive or NaN pivot: not SPD
+        if (bad < 0) bad = j;
+        djj = T(1);
+      }
+      const T r = rsq<T>(djj);
+      if (lane == j) row[j] = djj * r;
+      else if (lane > j) row[j] = row[j] * r;
+#pragma unroll
+      for (int l = j + 1; l < JJ + 4; l++) {   // the rest of the four columns
+        const T llj = __shfl_sync(0xffffffffu, row[j], l);
+        if (lane >= l && l < jb) row[l] -= row[j] * llj;
+      }
+    }
+  }
+  if (JJ + 4 < 32) {
+    st4(cb + 4 * lane, row[JJ], row[JJ + 1], row[JJ + 2], row[JJ + 3]);
+    __syncwarp();
+#pragma unroll
+    for (int l = JJ + 4; l < 32; l++) {      // rank-4 update of the columns to the right
+      T v[4];
+      ld4(cb + 4 * l, v);
+      if (lane >= l && l < jb) {
+        T acc = row[l];
+        acc = fma(-row[JJ], v[0], acc);
+        acc = fma(-row[JJ + 1], v[1], acc);
+        acc = fma(-row[JJ + 2], v[2], acc);
+        row[l] = fma(-row[JJ + 3], v[3], acc);
+      }
+    }
+    __syncwarp();                          // cb is rewritten by the next four columns
+  }
+}
+
 template <class T, int S>
 __device__ int warp_chol(T* Ds, int j0, int jb, T* Wk) {
   const int lane = threadIdx.x & 31;
@@ -116,34 +169,14 @@ __device__ int warp_chol(T* Ds, int j0, int jb, T* Wk) {
   for (int t = 0; t < 32; t++)
     row[t] = (lane < jb && t <= lane) ? Ds[(j0 + lane) * S + j0 + t] : T(0);
   int bad = -1;
-#pragma unroll
-  for (int j = 0; j < 32; j++) {
-    if (j < jb) {
-      T djj = __shfl_sync(0xffffffffu, row[j], j);
-      if (!(djj > T(0))) {                 // non-positive or NaN pivot: not SPD
-        if (bad < 0) bad = j;
-        djj = T(1);
-      }
-      const T r = rsq<T>(djj);
-      if (lane == j) row[j] = djj * r;
-      else if (lane > j) row[j] = row[j] * r;
-      cb[lane] = row[j];                   // L(lane, j)
-      __syncwarp();
-#pragma unroll
-      for (int l4 = 0; l4 < 32; l4 += 4) {
-        if (l4 + 3 > j) {
-          T v[4];
-          ld4(cb + l4, v);
-#pragma unroll
-          for (int u = 0; u < 4; u++) {
-            const int l = l4 + u;
-            if (l > j && lane >= l && l < jb) row[l] -= row[j] * v[u];
-          }
-        }
-      }
-      __syncwarp();                        // cb is rewritten by the next column
-    }
-  }
+  chol_cols4<T, 0>(row, lane, jb, cb, bad);
+  chol_cols4<T, 4>(row, lane, jb, cb, bad);
+  chol_cols4<T, 8>(row, lane, jb, cb, bad);
+  chol_cols4<T, 12>(row, lane, jb, cb, bad);
+  chol_cols4<T, 16>(row, lane, jb, cb, bad);
+  chol_cols4<T, 20>(row, lane, jb, cb, bad);
+  chol_cols4<T, 24>(row, lane, jb, cb, bad);
+  chol_cols4<T, 28>(row, lane, jb, cb, bad);
 #pragma unroll
   for (int t = 0; t < 32; t++) {
     if (lane < jb && t <= lane) Ds[(j0 + lane) * S + j0 + t] = row[t];
@@ -155,8 +188,9 @@ __device__ int warp_chol(T* Ds, int j0, int jb, T* Wk) {
 
 // One warp: the inverse of the jb x jb factor left in Wk by warp_chol, to Li
 // (row-major, stride LS; zero above the diagonal and outside jb).  Lane c
-// holds column c and eliminates right-looking, so the dependent chain is one
-// multiply-add per column.
+// holds column c and eliminates right-looking four rows at a time: the 4 x 4
+// diagonal block, then a rank-4 update of the rows below it (four values per
+// load of the transposed factor).
 template <class T, int LS>
 __device__ void warp_inv(const T* Wk, int jb, T* Li) {
   const int lane = threadIdx.x & 31;
@@ -166,19 +200,32 @@ __device__ void warp_inv(const T* Wk, int jb, T* Li) {
 #pragma unroll
   for (int i = 0; i < 32; i++) x[i] = i == lane ? T(1) : T(0);
 #pragma unroll
-  for (int t = 0; t < 32; t++) {
-    if (t < jb) {
-      x[t] *= __shfl_sync(0xffffffffu, rd, t);
+  for (int tt = 0; tt < 32; tt += 4) {
 #pragma unroll
-      for (int i4 = 0; i4 < 32; i4 += 4) {
-        if (i4 + 3 > t) {
-          T v[4];
-          ld4(LT + t * kLT + i4, v);
+    for (int u = 0; u < 4; u++) {
+      const int t = tt + u;
+      if (t < jb) {
+        x[t] *= __shfl_sync(0xffffffffu, rd, t);
 #pragma unroll
-          for (int u = 0; u < 4; u++) {
-            const int i = i4 + u;
-            if (i > t && i < jb) x[i] -= v[u] * x[t];
-          }
+        for (int i = t + 1; i < tt + 4; i++)
+          if (i < jb) x[i] -= LT[t * kLT + i] * x[t];
+      }
+    }
+#pragma unroll
+    for (int i4 = tt + 4; i4 < 32; i4 += 4) {
+      T v0[4], v1[4], v2[4], v3[4];
+      ld4(LT + (tt + 0) * kLT + i4, v0);
+      ld4(LT + (tt + 1) * kLT + i4, v1);
+      ld4(LT + (tt + 2) * kLT + i4, v2);
+      ld4(LT + (tt + 3) * kLT + i4, v3);
+#pragma unroll
+      for (int w = 0; w < 4; w++) {
+        if (i4 + w < jb) {
+          T acc = x[i4 + w];
+          acc = fma(-v0[w], x[tt], acc);
+          acc = fma(-v1[w], x[tt + 1], acc);
+          acc = fma(-v2[w], x[tt + 2], acc);
+          x[i4 + w] = fma(-v3[w], x[tt + 3], acc);
         }
       }
     }
