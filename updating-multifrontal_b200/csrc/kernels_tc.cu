@@ -135,7 +135,7 @@ __host__ __device__ inline int geo_tiles(const PanelGeo& g) {
 // group's rows of A, whose packed images (16 MB per 32 rows at K = 512) stay
 // in L2; in plain row order they sweep every column block of the panel, which
 // for the largest fronts (a 196 MB panel at 127^3) does not fit in L2.
-constexpr int kTileGroup = 64;
+constexpr int kTileGroup = 32;
 
 // Columns of group [a, b) holding all its rows (2 J <= a) and holding some.
 __host__ __device__ inline void group_cols(int a, int b, int nj, int& jf, int& je) {
