@@ -289,9 +289,15 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_bwd(const int* __restrict__ 
                                                         const int* __restrict__ flagoff, int* flags,
                                                         DevError* err) {
   constexpr int BR = 4;                       // boundary row blocks per shared-memory round
+  // Up to four right-hand sides the rows below go warp by column: warp wp
+  // takes columns 8 wp .. 8 wp + 7 of the block, its lanes 32 consecutive rows
+  // per load (coalesced), and a shuffle reduction sums the lanes at the end.
+  constexpr bool CW = NR <= 4;
   __shared__ T xs[BR * SB][NR + 1];
   __shared__ T vs[SB][NR + 1];
+  __shared__ T red[CW ? SB : 1][NR + 1];
   const int tid = threadIdx.x, cl = tid >> 2, q = tid & 3;   // column of the block, row quarter
+  const int wl = tid & 31, wp = tid >> 5;
   for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
     const int2 tk = tasks[t];
     const int i = tk.x, j = tk.y, f = flist[i];
@@ -307,17 +313,39 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_bwd(const int* __restrict__ 
     T acc[NR];
 #pragma unroll
     for (int c = 0; c < NR; c++) acc[c] = T(0);
-    // rows [r0, r0 + nr) against xs rows [x0, x0 + nr): lanes (cl, q) take
-    // rows 16 q .. 16 q + 15, all 16 loads in flight before the products
+    T accw[CW ? 8 : 1][NR];
+#pragma unroll
+    for (int k = 0; k < (CW ? 8 : 1); k++)
+#pragma unroll
+      for (int c = 0; c < NR; c++) accw[k][c] = T(0);
+    // rows [r0, r0 + nr) (nr <= 64) against xs rows [x0, x0 + nr), every
+    // load in flight before the products
     auto chunk = [&](int r0, int nr, int x0) {
-      if (!live) return;
-      T l[16];
+      if constexpr (CW) {
+        T l0[8], l1[8];
 #pragma unroll
-      for (int rr = 0; rr < 16; rr++) l[rr] = 16 * q + rr < nr ? Lc[r0 + 16 * q + rr] : T(0);
+        for (int k = 0; k < 8; k++) {
+          const int c = 8 * wp + k;
+          const T* Lk = A + (int64_t)(col0 + c) * d.ld + r0;
+          l0[k] = (c < kbj && wl < nr) ? Lk[wl] : T(0);
+          l1[k] = (c < kbj && wl + 32 < nr) ? Lk[wl + 32] : T(0);
+        }
 #pragma unroll
-      for (int rr = 0; rr < 16; rr++)
+        for (int k = 0; k < 8; k++)
 #pragma unroll
-        for (int c = 0; c < NR; c++) acc[c] = fma(l[rr], xs[x0 + 16 * q + rr][c], acc[c]);
+          for (int c = 0; c < NR; c++)
+            accw[k][c] = fma(l1[k], xs[x0 + wl + 32][c], fma(l0[k], xs[x0 + wl][c], accw[k][c]));
+      } else {
+        // lanes (cl, q) take rows 16 q .. 16 q + 15
+        if (!live) return;
+        T l[16];
+#pragma unroll
+        for (int rr = 0; rr < 16; rr++) l[rr] = 16 * q + rr < nr ? Lc[r0 + 16 * q + rr] : T(0);
+#pragma unroll
+        for (int rr = 0; rr < 16; rr++)
+#pragma unroll
+          for (int c = 0; c < NR; c++) acc[c] = fma(l[rr], xs[x0 + 16 * q + rr][c], acc[c]);
+      }
     };
     for (int r0 = d.n; r0 < d.N; r0 += BR * SB) {      // boundary rows: x_bd from X
       const int nr = min(BR * SB, d.N - r0);
@@ -342,6 +370,20 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_bwd(const int* __restrict__ 
       }
       __syncthreads();
       chunk(r0, nr, 0);
+    }
+    if constexpr (CW) {                      // the warps' column sums to the (cl, q) lanes
+#pragma unroll
+      for (int k = 0; k < 8; k++)
+#pragma unroll
+        for (int c = 0; c < NR; c++) {
+          T v = accw[k][c];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if (wl == 0) red[8 * wp + k][c] = v;
+        }
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < NR; c++) acc[c] = (q == 0 && live) ? red[cl][c] : T(0);
     }
     // before the last wait: block j + 1's L values, this column's quarter of
     // Dinv_j^T (upper triangular, column-major) and y_j
