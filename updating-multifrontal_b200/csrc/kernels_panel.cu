@@ -14,9 +14,8 @@
 //                  diagonal blocks in the front's scratch slot;
 //   k_panel_trsm   the rows below the block, L21 = A21 L11^{-T}, by blocked
 //                  substitution with L11 and those inverses: 128-row items
-//                  over a persistent grid, 16 outputs per thread in
-//                  registers, the next tile already on its way (cp.async
-//                  into a second buffer).
+//                  over a persistent grid of two CTAs per SM, 16 outputs
+//                  per thread in registers.
 // The trailing update then follows (k_trail_syrk here, the tensor-core update
 // on the mixed path's large levels).  The diagonal block is the only serial
 // part and it is factored once, by one CTA; the panel below is plain
@@ -66,9 +65,9 @@ constexpr size_t diag_smem() {
   return ((size_t)2 * W * diag_stride<W>() + kCholScratch) * sizeof(T);
 }
 template <class T, int W>
-constexpr size_t trsm_smem() {
-  return ((size_t)2 * W * xs_stride<T>() + (size_t)W * ls_stride<T, W>() + (size_t)W * 32) *
-         sizeof(T);
+constexpr size_t trsm_smem() {   // tile, off-diagonal blocks of L11, block inverses
+  return ((size_t)W * xs_stride<T>() + (size_t)(W / 32) * (W / 32 - 1) / 2 * 1024 +
+          (size_t)W * 32) * sizeof(T);
 }
 
 // Four consecutive values from 16-byte aligned shared memory.
@@ -359,26 +358,28 @@ __global__ void __launch_bounds__(kPanThreads) k_diag_factor(const int* __restri
 }
 
 // The rows below the diagonal block, L21 = A21 L11^{-T}, over a persistent
-// grid.  Items are 128-row blocks of every front's rows [Ks + kb, N), listed
-// front by front; a CTA takes items blockIdx.x, + gridDim.x, ... and fetches
-// the next item's tile (cp.async, 64 KB in flight per CTA) into its second
-// buffer while it works on the current one.  The tile is K-major (X[c][r]);
-// L11 (from the front, K-major: Ls[t][c] = L(c, t)) and the inverses of its
-// 32 x 32 diagonal blocks (from the slot) are fetched once per front the CTA
-// visits.  Blocked substitution, 32 columns at a time: Y_b = X_b - sum_{k<b}
+// grid of two CTAs per SM.  Items are 128-row blocks of every front's rows
+// [Ks + kb, N), listed front by front; a CTA takes items blockIdx.x,
+// + gridDim.x, ...  The tile is K-major (X[c][r], fetched with cp.async);
+// the off-diagonal 32 x 32 blocks of L11 (K-major inside each block, read
+// from the front) and the inverses of its diagonal blocks (from the slot) are
+// fetched once per front the CTA visits - only what the substitution reads,
+// so that two CTAs fit an SM and one computes while the other waits for its
+// tile.  Blocked substitution, 32 columns at a time: Y_b = X_b - sum_{k<b}
 // Z_k L_bk^T, then Z_b = Y_b Li_b^T, written over X_b.  Thread (tx, ty) owns
 // rows 4 ty .. 4 ty + 3 and 64 + the same, and in block b the columns
 // 32 b + tx and 32 b + tx + 16, in registers.
 template <class T, int W>
-__global__ void __launch_bounds__(kPanThreads) k_panel_trsm(const int* __restrict__ flist, int nf,
-                                                            const FrontDev* __restrict__ fr,
-                                                            T* __restrict__ F, int Ks,
-                                                            const T* __restrict__ slot) {
-  constexpr int XS = xs_stride<T>(), LS = ls_stride<T, W>(), NB = W / 32;
+__global__ void __launch_bounds__(kPanThreads, 2) k_panel_trsm(const int* __restrict__ flist,
+                                                               int nf,
+                                                               const FrontDev* __restrict__ fr,
+                                                               T* __restrict__ F, int Ks,
+                                                               const T* __restrict__ slot) {
+  constexpr int XS = xs_stride<T>(), NB = W / 32;
   extern __shared__ __align__(16) unsigned char trsm_raw[];
-  T* Xb = reinterpret_cast<T*>(trsm_raw);   // two tile buffers, K-major
-  T* Ls = Xb + 2 * W * XS;                   // L11, K-major
-  T* Lis = Ls + W * LS;                      // inverses of its diagonal blocks, K-major
+  T* X = reinterpret_cast<T*>(trsm_raw);    // the tile, K-major
+  T* Lp = X + W * XS;                        // block (b, k < b) of L11 at (b (b - 1) / 2 + k) 1024
+  T* Lis = Lp + NB * (NB - 1) / 2 * 1024;    // inverses of its diagonal blocks, K-major
   __shared__ int pre[kMaxPanelFronts + 1];
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   for (int i = tid; i < nf; i += kPanThreads) {
@@ -392,59 +393,42 @@ __global__ void __launch_bounds__(kPanThreads) k_panel_trsm(const int* __restric
   }
   __syncthreads();
   const int total = pre[nf];
-  if ((int)blockIdx.x >= total) return;
-  // item -> front index, first row, rows, panel width
-  auto locate = [&](int item, int& i, int& r0, int& rows, int& kb) {
+  int cur = -1;
+  for (int item = blockIdx.x; item < total; item += gridDim.x) {
     int lo = 0, hi = nf - 1;   // largest i with pre[i] <= item
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (pre[mid] <= item) lo = mid;
       else hi = mid - 1;
     }
-    i = lo;
+    const int i = lo;
     const FrontDev d = fr[flist[i]];
-    kb = min(W, d.n - Ks);
-    r0 = Ks + kb + (item - pre[i]) * kTrsmRows;
-    rows = min(kTrsmRows, d.N - r0);
-  };
-  auto fetch = [&](T* X, int i, int r0, int rows, int kb) {
-    const FrontDev d = fr[flist[i]];
-    const T* A = F + d.off;
-    for (int idx = tid; idx < W * kTrsmRows; idx += kPanThreads) {
-      const int r = idx % kTrsmRows, t = idx / kTrsmRows;
-      const bool take = r < rows && t < kb;
-      cp_elem(X + t * XS + r, take ? A + (r0 + r) + (int64_t)(Ks + t) * d.ld : A, take);
-    }
-  };
-  int i, r0, rows, kb, cur = -1;
-  locate(blockIdx.x, i, r0, rows, kb);
-  fetch(Xb, i, r0, rows, kb);
-  cp_commit();
-  for (int item = blockIdx.x, k = 0; item < total; item += gridDim.x, k++) {
-    T* X = Xb + (k & 1) * W * XS;
-    __syncthreads();                         // the other buffer's result has been stored
+    T* A = F + d.off;
+    const int64_t ld = d.ld;
+    const int kb = min(W, d.n - Ks);
+    const int r0 = Ks + kb + (item - pre[i]) * kTrsmRows, rows = min(kTrsmRows, d.N - r0);
+    __syncthreads();                         // the previous item's result has been stored
     if (i != cur) {
       cur = i;
-      const FrontDev d = fr[flist[i]];
-      const T* A = F + d.off;
-      for (int idx = tid; idx < W * W; idx += kPanThreads) {
-        const int c = idx % W, t = idx / W;
-        const bool take = c < kb && t < kb && t <= c;
-        cp_elem(Ls + t * LS + c, take ? A + (Ks + c) + (int64_t)(Ks + t) * d.ld : A, take);
+      for (int idx = tid; idx < NB * (NB - 1) / 2 * 1024; idx += kPanThreads) {
+        const int blk = idx >> 10, tt = (idx >> 5) & 31, cc = idx & 31;
+        int b = 1;
+        while ((b + 1) * b / 2 <= blk) b++;  // block row b of packed block blk
+        const int k = blk - b * (b - 1) / 2;
+        const int c = 32 * b + cc, t = 32 * k + tt;
+        const bool take = c < kb && t < kb;
+        cp_elem(Lp + idx, take ? A + (Ks + c) + (int64_t)(Ks + t) * ld : A, take);
       }
       const T* Lt = slot + (int64_t)i * W * W;
       for (int idx = tid; idx < W * 32; idx += kPanThreads) cp_elem(Lis + idx, Lt + idx, true);
-      cp_commit();
     }
-    int ni = i, nr0 = 0, nrows = 0, nkb = 0;
-    if (item + (int)gridDim.x < total) {
-      locate(item + gridDim.x, ni, nr0, nrows, nkb);
-      fetch(Xb + ((k + 1) & 1) * W * XS, ni, nr0, nrows, nkb);
-      cp_commit();
-      cp_wait<1>();                          // all but the prefetch
-    } else {
-      cp_wait<0>();
+    for (int idx = tid; idx < W * kTrsmRows; idx += kPanThreads) {
+      const int r = idx % kTrsmRows, t = idx / kTrsmRows;
+      const bool take = r < rows && t < kb;
+      cp_elem(X + t * XS + r, take ? A + (r0 + r) + (int64_t)(Ks + t) * ld : A, take);
     }
+    cp_commit();
+    cp_wait<0>();
     __syncthreads();
     const int nbk = (kb + 31) / 32;
     for (int b = 0; b < nbk && b < NB; b++) {
@@ -462,16 +446,19 @@ __global__ void __launch_bounds__(kPanThreads) k_panel_trsm(const int* __restric
           acc[r][1] = xb[r];
         }
       }
+      for (int k = 0; k < b; k++) {          // - Z_k L_bk^T over the solved blocks
+        const T* Lb = Lp + (b * (b - 1) / 2 + k) * 1024;
 #pragma unroll 4
-      for (int t = 0; t < 32 * b; t++) {     // - Z_k L_bk^T over the solved columns
-        T z[8];
-        ld4(X + t * XS + 4 * ty, z);
-        ld4(X + t * XS + 64 + 4 * ty, z + 4);
-        const T la = Ls[t * LS + ca], lb = Ls[t * LS + cb];
+        for (int tt = 0; tt < 32; tt++) {
+          T z[8];
+          ld4(X + (32 * k + tt) * XS + 4 * ty, z);
+          ld4(X + (32 * k + tt) * XS + 64 + 4 * ty, z + 4);
+          const T la = Lb[tt * 32 + tx], lb = Lb[tt * 32 + tx + 16];
 #pragma unroll
-        for (int r = 0; r < 8; r++) {
-          acc[r][0] = fma(-z[r], la, acc[r][0]);
-          acc[r][1] = fma(-z[r], lb, acc[r][1]);
+          for (int r = 0; r < 8; r++) {
+            acc[r][0] = fma(-z[r], la, acc[r][0]);
+            acc[r][1] = fma(-z[r], lb, acc[r][1]);
+          }
         }
       }
       // Y_b in place (only this thread reads these entries before the barrier)
@@ -506,18 +493,10 @@ __global__ void __launch_bounds__(kPanThreads) k_panel_trsm(const int* __restric
       }
       __syncthreads();
     }
-    {
-      const FrontDev d = fr[flist[i]];
-      T* A = F + d.off;
-      for (int idx = tid; idx < kb * kTrsmRows; idx += kPanThreads) {
-        const int r = idx % kTrsmRows, c = idx / kTrsmRows;
-        if (r < rows) A[(r0 + r) + (int64_t)(Ks + c) * d.ld] = X[c * XS + r];
-      }
+    for (int idx = tid; idx < kb * kTrsmRows; idx += kPanThreads) {
+      const int r = idx % kTrsmRows, c = idx / kTrsmRows;
+      if (r < rows) A[(r0 + r) + (int64_t)(Ks + c) * ld] = X[c * XS + r];
     }
-    i = ni;
-    r0 = nr0;
-    rows = nrows;
-    kb = nkb;
   }
 }
 
