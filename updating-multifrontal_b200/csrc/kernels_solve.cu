@@ -169,7 +169,15 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_fwd(const int* __restrict__ 
     T acc[NR];
 #pragma unroll
     for (int c = 0; c < NR; c++) acc[c] = T(0);
-    // every block but the last, CH at a time as their flags come up
+    // every block but the last, CH at a time as their flags come up.  These
+    // bulk loads go by (row tid & 63, column group tid >> 6): a warp reads 32
+    // consecutive rows of a column (coalesced); the sums are handed to the
+    // (row, quarter) lanes once, after the loop.
+    const int rl2 = tid & (SB - 1), g2 = tid >> 6;
+    const T* Ar2 = A + row0 + rl2;
+    T acc2[NR];
+#pragma unroll
+    for (int c = 0; c < NR; c++) acc2[c] = T(0);
     for (int j0 = 0; j0 < jmax - 1; j0 += CH) {
       const int jc = min(CH, jmax - 1 - j0);
       __syncthreads();                        // ys of the previous round is consumed
@@ -182,18 +190,26 @@ __global__ void __launch_bounds__(SCT) k_solve_flow_fwd(const int* __restrict__ 
         ys[r][c] = col < d.n ? ldcg(Y + col + (int64_t)c * d.N) : T(0);
       }
       __syncthreads();
-      if (live) {
+      if (rl2 < rows) {
         for (int jj = 0; jj < jc; jj++) {
-          const int cb = (j0 + jj) * SB + 16 * g;
+          const int cb = (j0 + jj) * SB + 16 * g2;
           T l[16];
 #pragma unroll
-          for (int q = 0; q < 16; q++) l[q] = cb + q < d.n ? Ar[(int64_t)(cb + q) * d.ld] : T(0);
+          for (int q = 0; q < 16; q++) l[q] = cb + q < d.n ? Ar2[(int64_t)(cb + q) * d.ld] : T(0);
 #pragma unroll
           for (int q = 0; q < 16; q++)
 #pragma unroll
-            for (int c = 0; c < NR; c++) acc[c] = fma(l[q], ys[jj * SB + 16 * g + q][c], acc[c]);
+            for (int c = 0; c < NR; c++) acc2[c] = fma(l[q], ys[jj * SB + 16 * g2 + q][c], acc2[c]);
         }
       }
+    }
+    if (jmax > 1) {                           // hand the sums to the (row, quarter) lanes
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < NR; c++) ys[g2 * SB + rl2][c] = acc2[c];
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < NR; c++) acc[c] = ys[g * SB + rl][c];
     }
     // before the last wait: that block's L values, this row's quarter of
     // Dinv_R (lower triangular, column-major) and the right-hand side
