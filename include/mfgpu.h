@@ -298,7 +298,9 @@ enum mfgpu_kernel_class {
   MFGPU_KC_SOLVE = 4,     /* forward / backward sweeps                       */
   MFGPU_KC_APPLY = 5,     /* factored-operator application                   */
   MFGPU_KC_FRONT = 6,     /* fused partial factorization, one CTA per front  */
-  MFGPU_KC_COOP = 7,      /* cooperative per-level partial factorization     */
+  MFGPU_KC_COOP = 7,      /* per-level partial factorization on CUDA cores:
+                             cooperative kernel, panel kernels, and the
+                             tensor-core levels' sub-panels                   */
   MFGPU_KC_TC = 8,        /* tensor-core trailing updates (mixed path)       */
   MFGPU_KC_COUNT = 9
 };
